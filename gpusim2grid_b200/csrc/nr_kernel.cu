@@ -1,0 +1,567 @@
+// Persistent batched Newton–Raphson kernel for sm_100a.
+//
+// One CTA owns one batch row at a time and runs that row's whole Newton loop
+// without leaving the kernel: mismatch SpMV (FP64) → ‖F‖∞ → Jacobian fill →
+// sparse head LU (level-scheduled) → Schur update of the dense tail → dense
+// tail LU → triangular solves → polar voltage update (FP64).  A row leaves the
+// CTA as soon as it has converged, diverged or used its iteration budget, and
+// the CTA takes the next row from a global queue: rows retire individually
+// with no host round trip (the reference decides per round on the host,
+// src/_cpp/contingency/batch_pf_driver.cu:2691-2720).
+//
+// The arithmetic of every step follows the reference:
+//   mismatch  F = -[Re, Im](V∘conj(Y V) − Sbus)      acpf_nr_kernels.cu:493-557
+//   Jacobian  dS/dVa, dS/dVm (MATPOWER)              acpf_nr_kernels.cu:559-650
+//   update    Va += dθ on pvpq, then Vm += dVm on pq acpf_nr_kernels.cu:728-790
+//   norm      NaN-sticky ‖F‖∞                         acpf_nr_kernels.cu:1076-1128
+//   trips     Y −= {yff, ytt, yft, ytf} per branch    contingency_analysis_helper.cpp:23-84
+// The linear algebra (LU of J, solves) runs in T = double or float; the
+// mismatch, the norm and the voltages are always FP64.
+#include "nr_kernel.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+namespace gs2g {
+
+namespace {
+
+constexpr int BS = 256;        // threads per CTA
+constexpr int NWARP = BS / 32;
+constexpr int NB = 32;         // dense panel width
+constexpr int TM = 64;         // dense trailing-update tile (TM x TM)
+constexpr int MAX_EDITS = 64;  // Ybus edits per row held in shared memory
+
+template <typename T>
+struct DenseSmem {
+  static constexpr int kD = NB * (NB + 1);
+  static constexpr int kA = TM * (NB + 1);
+  static constexpr int kB = NB * TM;
+  static constexpr int bytes = (kD + kA + kB) * (int)sizeof(T);
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+struct RowEdits {
+  int n;
+  const int* k;
+  const double2* v;
+  __device__ __forceinline__ double2 apply(int kk, double2 y) const {
+    for (int e = 0; e < n; ++e)
+      if (k[e] == kk) y = csub(y, v[e]);
+    return y;
+  }
+};
+
+// NaN-sticky block max of |x| (a NaN anywhere makes the result NaN).
+__device__ double block_nanmax(double v, double* s_red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = (isnan(w) || isnan(v)) ? NAN : fmax(v, w);
+  }
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  double r = s_red[0];
+  for (int i = 1; i < NWARP; ++i) {
+    double w = s_red[i];
+    r = (isnan(w) || isnan(r)) ? NAN : fmax(r, w);
+  }
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Dense tail LU (no pivoting, in place, row-major with leading dimension ld).
+// Right-looking, NB-wide panels; the trailing update is a TM x TM tiled GEMM
+// with a 4x4 register tile per thread.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ void dense_trailing_update(T* __restrict__ C, const T* __restrict__ L, const T* __restrict__ U,
+                                      int m, int kb, int ld, T* sA, T* sB) {
+  const int tid = threadIdx.x;
+  const int tr = tid >> 4, tc = tid & 15;
+  for (int i0 = 0; i0 < m; i0 += TM) {
+    for (int j0 = 0; j0 < m; j0 += TM) {
+      for (int idx = tid; idx < TM * NB; idx += BS) {
+        const int r = idx / NB, c = idx % NB;
+        sA[r * (NB + 1) + c] = (i0 + r < m && c < kb) ? L[(int64_t)(i0 + r) * ld + c] : T(0);
+      }
+      for (int idx = tid; idx < NB * TM; idx += BS) {
+        const int r = idx / TM, c = idx % TM;
+        sB[r * TM + c] = (r < kb && j0 + c < m) ? U[(int64_t)r * ld + j0 + c] : T(0);
+      }
+      __syncthreads();
+      T acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+      for (int kk = 0; kk < kb; ++kk) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) av[i] = sA[(tr * 4 + i) * (NB + 1) + kk];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bv[j] = sB[kk * TM + tc * 4 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = i0 + tr * 4 + i;
+        if (r >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int c = j0 + tc * 4 + j;
+          if (c < m) C[(int64_t)r * ld + c] -= acc[i][j];
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
+  const T f = (T)floor_;
+  if (fabs(piv) < f) return piv < T(0) ? -f : f;
+  return piv;
+}
+
+template <typename T>
+__device__ void dense_lu(T* __restrict__ A, int n, int ld, T* sD, T* sA, T* sB, double pfloor) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k0 = 0; k0 < n; k0 += NB) {
+    const int kb = min(NB, n - k0);
+    for (int idx = tid; idx < kb * kb; idx += BS) {
+      const int r = idx / kb, c = idx % kb;
+      sD[r * (NB + 1) + c] = A[(int64_t)(k0 + r) * ld + k0 + c];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int j = 0; j < kb; ++j) {
+        T piv = clamp_pivot(sD[j * (NB + 1) + j], pfloor);
+        __syncwarp();
+        if (lane == j) sD[j * (NB + 1) + j] = piv;
+        if (lane > j && lane < kb) {
+          const T l = sD[lane * (NB + 1) + j] / piv;
+          sD[lane * (NB + 1) + j] = l;
+          for (int c = j + 1; c < kb; ++c) sD[lane * (NB + 1) + c] -= l * sD[j * (NB + 1) + c];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kb * kb; idx += BS) {
+      const int r = idx / kb, c = idx % kb;
+      A[(int64_t)(k0 + r) * ld + k0 + c] = sD[r * (NB + 1) + c];
+    }
+    const int m = n - k0 - kb;
+    if (m > 0) {
+      // L21 = A21 U11^{-1} (row-wise)
+      for (int r = tid; r < m; r += BS) {
+        T* row = A + (int64_t)(k0 + kb + r) * ld + k0;
+        T x[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) x[c] = c < kb ? row[c] : T(0);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+          if (c < kb) {
+            T v = x[c];
+#pragma unroll
+            for (int q = 0; q < c; ++q) v -= x[q] * sD[q * (NB + 1) + c];
+            x[c] = v / sD[c * (NB + 1) + c];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+          if (c < kb) row[c] = x[c];
+      }
+      // U12 = L11^{-1} A12 (column-wise, unit L)
+      for (int j = tid; j < m; j += BS) {
+        T* col = A + (int64_t)k0 * ld + k0 + kb + j;
+        T x[NB];
+#pragma unroll
+        for (int r = 0; r < NB; ++r) x[r] = r < kb ? col[(int64_t)r * ld] : T(0);
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+          if (r < kb) {
+            T v = x[r];
+#pragma unroll
+            for (int q = 0; q < r; ++q) v -= sD[r * (NB + 1) + q] * x[q];
+            x[r] = v;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < NB; ++r)
+          if (r < kb) col[(int64_t)r * ld] = x[r];
+      }
+      __syncthreads();
+      dense_trailing_update<T>(A + (int64_t)(k0 + kb) * ld + (k0 + kb), A + (int64_t)(k0 + kb) * ld + k0,
+                               A + (int64_t)k0 * ld + k0 + kb, m, kb, ld, sA, sB);
+    }
+    __syncthreads();
+  }
+}
+
+// Dense unit-lower forward solve y <- L^{-1} y and upper backward solve
+// y <- U^{-1} y on the tail (y is the tail part of the solve vector).
+template <typename T>
+__device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ y, T* s_blk) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int cb = min(32, n - c0);
+    if (warp == 0) {
+      T v = lane < cb ? y[c0 + lane] : T(0);
+      for (int c = 0; c < cb; ++c) {
+        const T yc = __shfl_sync(0xffffffffu, v, c);
+        if (lane > c && lane < cb) v -= A[(int64_t)(c0 + lane) * ld + c0 + c] * yc;
+      }
+      if (lane < cb) {
+        y[c0 + lane] = v;
+        s_blk[lane] = v;
+      }
+    }
+    __syncthreads();
+    for (int i = c0 + cb + tid; i < n; i += BS) {
+      const T* row = A + (int64_t)i * ld + c0;
+      T acc = y[i];
+      for (int c = 0; c < cb; ++c) acc -= row[c] * s_blk[c];
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+  const int nblk = (n + 31) / 32;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int c0 = bi * 32;
+    const int cb = min(32, n - c0);
+    if (warp == 0) {
+      T v = lane < cb ? y[c0 + lane] : T(0);
+      for (int c = cb - 1; c >= 0; --c) {
+        T xc = 0;
+        if (lane == c) {
+          v = v / A[(int64_t)(c0 + c) * ld + c0 + c];
+          xc = v;
+        }
+        xc = __shfl_sync(0xffffffffu, xc, c);
+        if (lane < c) v -= A[(int64_t)(c0 + lane) * ld + c0 + c] * xc;
+      }
+      if (lane < cb) {
+        y[c0 + lane] = v;
+        s_blk[lane] = v;
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < c0; i += BS) {
+      const T* row = A + (int64_t)i * ld + c0;
+      T acc = y[i];
+      for (int c = 0; c < cb; ++c) acc -= row[c] * s_blk[c];
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+__host__ __device__ __forceinline__ int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
+
+struct WsLayout {
+  int64_t V, I, F, HV, S, y, total;
+};
+
+template <typename T>
+__host__ __device__ WsLayout ws_layout(const DevPlan& P) {
+  WsLayout w;
+  int64_t o = 0;
+  w.V = o; o = align256(o + (int64_t)P.n_bus * 16);
+  w.I = o; o = align256(o + (int64_t)P.n_bus * 16);
+  w.F = o; o = align256(o + (int64_t)P.dim * 8);
+  w.HV = o; o = align256(o + (int64_t)P.n_hv * sizeof(T));
+  w.S = o; o = align256(o + (int64_t)P.nt * P.ld * sizeof(T));
+  w.y = o; o = align256(o + (int64_t)P.dim * sizeof(T));
+  w.total = o;
+  return w;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_row;
+  __shared__ int s_ne;
+  __shared__ int s_ek[MAX_EDITS];
+  __shared__ double2 s_ev[MAX_EDITS];
+  __shared__ double s_red[NWARP];
+  __shared__ T s_blk[32];
+  T* sD = reinterpret_cast<T*>(smem_raw);
+  T* sA = sD + DenseSmem<T>::kD;
+  T* sB = sA + DenseSmem<T>::kA;
+
+  const int tid = threadIdx.x;
+  const WsLayout L = ws_layout<T>(P);
+  char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
+  double2* V = reinterpret_cast<double2*>(ws + L.V);
+  double2* I = reinterpret_cast<double2*>(ws + L.I);
+  double* F = reinterpret_cast<double*>(ws + L.F);
+  T* HV = reinterpret_cast<T*>(ws + L.HV);
+  T* S = reinterpret_cast<T*>(ws + L.S);
+  T* y = reinterpret_cast<T*>(ws + L.y);
+  const double2* Y = reinterpret_cast<const double2*>(a.ybus);
+  const int n = P.n_bus;
+
+  for (;;) {
+    if (tid == 0) s_row = atomicAdd(a.queue, 1);
+    __syncthreads();
+    const int row = s_row;
+    if (row >= a.n_rows) return;
+    double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
+
+    if (a.row_skip != nullptr && a.row_skip[row]) {
+      for (int i = tid; i < n; i += BS) vout[i] = make_double2(NAN, NAN);
+      if (tid == 0) {
+        a.res_out[row] = NAN;
+        a.status_out[row] = ROW_NOT_SIMULATED;
+        a.iters_out[row] = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (tid == 0) {
+      int ne = 0;
+      if (a.edit_ptr != nullptr) {
+        const int e0 = a.edit_ptr[row], e1 = a.edit_ptr[row + 1];
+        ne = min(e1 - e0, MAX_EDITS);
+        for (int e = 0; e < ne; ++e) {
+          s_ek[e] = a.edit_k[e0 + e];
+          s_ev[e] = reinterpret_cast<const double2*>(a.edit_val)[e0 + e];
+        }
+      }
+      s_ne = ne;
+    }
+    const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
+    const double2* sb = reinterpret_cast<const double2*>(a.sbus) + (int64_t)row * a.sbus_stride;
+    for (int i = tid; i < n; i += BS) V[i] = v0[i];
+    __syncthreads();
+    const RowEdits ed{s_ne, s_ek, s_ev};
+
+    int it = 0, status = ROW_MAX_ITER;
+    double nrm = NAN;
+    for (;;) {
+      // ---- I = Y V (row-patched Ybus) ------------------------------------
+      for (int i = tid; i < n; i += BS) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int k = P.y_indptr[i]; k < P.y_indptr[i + 1]; ++k) {
+          const double2 yk = ed.apply(k, Y[k]);
+          const double2 vj = V[P.y_indices[k]];
+          acc.x = fma(yk.x, vj.x, fma(-yk.y, vj.y, acc.x));
+          acc.y = fma(yk.x, vj.y, fma(yk.y, vj.x, acc.y));
+        }
+        I[i] = acc;
+      }
+      __syncthreads();
+      // ---- F = -(V conj(I) - Sbus) at the P/Q rows, NaN-sticky inf-norm ---
+      double lmax = 0.0;
+      for (int i = tid; i < n; i += BS) {
+        const double2 s = csub(cmul(V[i], conj2(I[i])), sb[i]);
+        const int fp = P.fP[i], fq = P.fQ[i];
+        if (fp >= 0) {
+          F[fp] = -s.x;
+          const double ax = fabs(s.x);
+          lmax = (isnan(ax) || isnan(lmax)) ? NAN : fmax(lmax, ax);
+        }
+        if (fq >= 0) {
+          F[fq] = -s.y;
+          const double ay = fabs(s.y);
+          lmax = (isnan(ay) || isnan(lmax)) ? NAN : fmax(lmax, ay);
+        }
+      }
+      nrm = block_nanmax(lmax, s_red);
+      const bool finite = isfinite(nrm);
+      if (a.fixed_iters) {
+        if (it >= a.max_iter || !finite) {
+          status = !finite ? ROW_DIVERGED : (nrm < a.tol ? ROW_CONVERGED : ROW_MAX_ITER);
+          break;
+        }
+      } else {
+        if (!finite) { status = ROW_DIVERGED; break; }
+        if (nrm < a.tol) { status = ROW_CONVERGED; break; }
+        if (it >= a.max_iter) { status = ROW_MAX_ITER; break; }
+      }
+
+      // ---- zero the dense tail, then scatter J ------------------------------
+      {
+        const int64_t ns = (int64_t)P.nt * P.ld;
+        for (int64_t q = tid; q < ns; q += BS) S[q] = T(0);
+      }
+      __syncthreads();
+      for (int k = tid; k < P.nnz_y; k += BS) {
+        const int i = P.y_row[k], j = P.y_indices[k];
+        const double2 Vi = V[i], Ii = I[i];
+        const double2 yk = ed.apply(k, Y[k]);
+        double2 dVa, dVm;
+        if (i == j) {
+          const double2 t = cmul(Vi, conj2(csub(Ii, cmul(yk, Vi))));
+          dVa = make_double2(-t.y, t.x);
+          const double inv = 1.0 / hypot(Vi.x, Vi.y);
+          const double2 vn = make_double2(Vi.x * inv, Vi.y * inv);
+          dVm = cadd(cmul(Vi, conj2(cmul(yk, vn))), cmul(conj2(Ii), vn));
+        } else {
+          const double2 Vj = V[j];
+          const double2 t = cmul(Vi, conj2(cmul(yk, Vj)));
+          dVa = make_double2(t.y, -t.x);
+          const double inv = 1.0 / hypot(Vj.x, Vj.y);
+          const double2 vn = make_double2(Vj.x * inv, Vj.y * inv);
+          dVm = cmul(Vi, conj2(cmul(yk, vn)));
+        }
+        const double vals[4] = {dVa.x, dVm.x, dVa.y, dVm.y};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int dst = P.jmap[4 * k + q];
+          if (dst >= 0) HV[dst] = (T)vals[q];
+          else if (dst <= -2) S[-(dst + 2)] = (T)vals[q];
+        }
+      }
+      __syncthreads();
+
+      // ---- sparse head LU, level by level --------------------------------
+      for (int lv = 0; lv < P.n_levels; ++lv) {
+        const int t0 = P.lev_ptr[lv], t1 = P.lev_ptr[lv + 1];
+        for (int t = t0 + tid; t < t1; t += BS) {
+          const int out = P.task_out[t];
+          T acc = P.task_has_a[t] ? HV[out] : T(0);
+          const int q1 = P.task_pend[t];
+          for (int q = P.task_pbeg[t]; q < q1; ++q) acc -= HV[P.pair_l[q]] * HV[P.pair_u[q]];
+          if (out < P.p) acc = clamp_pivot(acc, a.pivot_floor);
+          HV[out] = acc;
+        }
+        __syncthreads();
+        for (int t = t0 + tid; t < t1; t += BS) {
+          const int dg = P.task_diag[t];
+          if (dg >= 0) HV[P.task_out[t]] /= HV[dg];
+        }
+        __syncthreads();
+      }
+
+      // ---- Schur update of the dense tail: warp per tail row ---------------
+      {
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int ti = warp; ti < P.nt; ti += NWARP) {
+          T* Srow = S + (int64_t)ti * P.ld;
+          for (int q = P.schur_ptr[ti]; q < P.schur_ptr[ti + 1]; ++q) {
+            const int s = P.schur_sn[q], ar = P.schur_a[q];
+            const int w = P.sn_w[s], t = P.sn_t[s];
+            const T* Lr = HV + P.sn_L[s] + ar * w;
+            const T* Ub = HV + P.sn_U[s];
+            const int* tx = P.tidx + P.sn_tidx[s];
+            for (int b = lane; b < t; b += 32) {
+              T acc = T(0);
+              for (int c = 0; c < w; ++c) acc += Lr[c] * Ub[c * t + b];
+              Srow[tx[b]] -= acc;
+            }
+            __syncwarp();
+          }
+        }
+      }
+      __syncthreads();
+
+      // ---- dense tail LU --------------------------------------------------
+      if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, sD, sA, sB, a.pivot_floor);
+
+      // ---- solves -----------------------------------------------------------
+      for (int i = tid; i < P.dim; i += BS) y[i] = (T)F[i];
+      __syncthreads();
+      for (int lv = 0; lv < P.n_levels; ++lv) {
+        for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+          const int i = P.lev_piv[q0];
+          T acc = y[i];
+          for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= HV[P.fw_pos[q]] * y[P.fw_col[q]];
+          y[i] = acc;
+        }
+        __syncthreads();
+      }
+      for (int ti = tid; ti < P.nt; ti += BS) {
+        const int i = P.p + ti;
+        T acc = y[i];
+        for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= HV[P.fw_pos[q]] * y[P.fw_col[q]];
+        y[i] = acc;
+      }
+      __syncthreads();
+      if (P.nt > 0) dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk);
+      for (int lv = P.n_levels - 1; lv >= 0; --lv) {
+        for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+          const int k = P.lev_piv[q0];
+          T acc = y[k];
+          for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) acc -= HV[P.bw_pos[q]] * y[P.bw_row[q]];
+          y[k] = acc / HV[k];
+        }
+        __syncthreads();
+      }
+
+      // ---- V update (FP64, polar) -----------------------------------------
+      for (int i = tid; i < n; i += BS) {
+        const int fp = P.fP[i], fq = P.fQ[i];
+        if (fp < 0 && fq < 0) continue;
+        const double dva = fp >= 0 ? (double)y[fp] : 0.0;
+        const double dvm = fq >= 0 ? (double)y[fq] : 0.0;
+        const double2 v = V[i];
+        const double vm = hypot(v.x, v.y) + dvm;
+        const double va = atan2(v.y, v.x) + dva;
+        double sn, cs;
+        sincos(va, &sn, &cs);
+        V[i] = make_double2(vm * cs, vm * sn);
+      }
+      __syncthreads();
+      ++it;
+    }
+
+    for (int i = tid; i < n; i += BS) vout[i] = V[i];
+    if (tid == 0) {
+      a.res_out[row] = nrm;
+      a.status_out[row] = status;
+      a.iters_out[row] = it;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+int smem_bytes() {
+  return DenseSmem<T>::bytes;
+}
+
+}  // namespace
+
+int64_t workspace_bytes(const DevPlan& P, int prec) {
+  return prec == 1 ? ws_layout<float>(P).total : ws_layout<double>(P).total;
+}
+
+int sweep_ctas(int prec, int device) {
+  int n_sm = 0;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
+  int per_sm = 0;
+  if (prec == 1)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<float>, BS, smem_bytes<float>());
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<double>, BS, smem_bytes<double>());
+  if (per_sm < 1) per_sm = 1;
+  return n_sm * per_sm;
+}
+
+int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0) return (int)cudaErrorInvalidValue;
+  if (prec == 1)
+    sweep_kernel<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
+  else
+    sweep_kernel<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(P, a);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace gs2g

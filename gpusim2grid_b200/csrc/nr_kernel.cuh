@@ -1,0 +1,87 @@
+// Device-side interface of the persistent batched Newton–Raphson kernel.
+// Plain structs of device pointers; no CUDA or torch types leak into the
+// C-ABI headers.
+#pragma once
+
+#include <cstdint>
+
+namespace gs2g {
+
+// Status codes of one batch row, the reference's RowStatus
+// (src/_cpp/contingency/row_status.hpp:33-42).
+enum RowStatusCode : int { ROW_CONVERGED = 0, ROW_MAX_ITER = 1, ROW_DIVERGED = 2, ROW_NOT_SIMULATED = 3 };
+
+// Device copy of a Plan (see plan.hpp); every pointer is device memory.
+struct DevPlan {
+  int n_bus, nnz_y, dim, p, nt, ld, n_hv, n_levels;
+  const int* y_indptr;
+  const int* y_indices;
+  const int* y_row;
+  const int* jmap;     // [4 * nnz_y]
+  const int* fP;       // [n_bus]
+  const int* fQ;       // [n_bus]
+  const int* lev_ptr;  // [n_levels + 1] into tasks
+  const int* task_out;
+  const int* task_diag;
+  const int* task_pbeg;
+  const int* task_pend;
+  const uint8_t* task_has_a;
+  const int* pair_l;
+  const int* pair_u;
+  const int* lev_piv_ptr;  // [n_levels + 1] into lev_piv
+  const int* lev_piv;      // head pivots by level
+  const int* sn_w;
+  const int* sn_t;
+  const int* sn_L;
+  const int* sn_U;
+  const int* sn_tidx;
+  const int* tidx;
+  const int* schur_ptr;  // [nt + 1]
+  const int* schur_sn;
+  const int* schur_a;
+  const int* fw_ptr;  // [dim + 1]
+  const int* fw_col;
+  const int* fw_pos;
+  const int* bw_ptr;  // [p + 1]
+  const int* bw_row;
+  const int* bw_pos;
+};
+
+// One launch = one sweep over a list of rows.
+struct SweepArgs {
+  int n_rows;
+  const double* ybus;     // [2 * nnz_y] interleaved complex base Ybus values
+  const double* v0;       // start voltage, complex, row r at v0 + 2 * r * v0_stride
+  int64_t v0_stride;      // in complex elements (0: shared)
+  const double* sbus;     // complex injections, row r at sbus + 2 * r * sbus_stride
+  int64_t sbus_stride;
+  const int* edit_ptr;    // [n_rows + 1] per-row Ybus edits (nullptr: none)
+  const int* edit_k;      // Ybus entry index
+  const double* edit_val; // complex delta to SUBTRACT
+  const int* row_skip;    // [n_rows] nonzero: NOT_SIMULATED (nullptr: none)
+  int max_iter;
+  double tol;
+  int fixed_iters;        // 1: exactly max_iter steps then the residual; 0: stop at tol
+  // outputs
+  double* v_out;          // [n_rows * n_bus] complex
+  double* res_out;        // [n_rows]
+  int* status_out;        // [n_rows]
+  int* iters_out;         // [n_rows]
+  // scheduling
+  int* queue;             // one int, zeroed before the launch
+  char* workspace;        // per-CTA scratch
+  int64_t ws_stride;      // bytes per CTA
+  double pivot_floor;     // static-pivot floor (|u_kk| below it is raised to it)
+};
+
+// Per-CTA workspace bytes for precision `prec` (0: fp64 LU, 1: fp32 LU).
+int64_t workspace_bytes(const DevPlan& P, int prec);
+
+// Launch the sweep on `stream` with `n_ctas` CTAs (<= 0: one wave at full
+// occupancy).  Returns the cudaError_t as int.
+int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream);
+
+// CTAs that fit at once for `prec` (for sizing the workspace).
+int sweep_ctas(int prec, int device);
+
+}  // namespace gs2g

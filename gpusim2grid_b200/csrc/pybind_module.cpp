@@ -1,0 +1,281 @@
+// pybind11 module _gs2g: a thin Python binding of the C-ABI in include/gs2g.h.
+// It converts numpy arrays to plain pointers and C status codes to Python
+// exceptions (GS2G_ERR_INVALID -> ValueError, others -> RuntimeError), the
+// error mapping of the reference's pybind11 module (src/_cpp/python_bindings.cpp).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/gs2g.h"
+
+namespace py = pybind11;
+
+namespace {
+
+using cplx = std::complex<double>;
+using IArr = py::array_t<int, py::array::c_style | py::array::forcecast>;
+using DArr = py::array_t<double, py::array::c_style | py::array::forcecast>;
+using CArr = py::array_t<cplx, py::array::c_style | py::array::forcecast>;
+
+void check(int rc) {
+  if (rc == GS2G_OK) return;
+  std::string msg = gs2g_last_error();
+  if (rc == GS2G_ERR_INVALID) throw py::value_error(msg);
+  throw std::runtime_error(msg);
+}
+
+gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
+                        int n_ctas) {
+  gs2g_run_opts o{};
+  o.max_iter = max_iter;
+  o.tol = tol;
+  o.fixed_iters = fixed_iters ? 1 : 0;
+  o.precision = precision;
+  o.start = start;
+  o.pivot_floor = pivot_floor;
+  o.n_ctas = n_ctas;
+  return o;
+}
+
+class Session {
+ public:
+  Session(int device, int n_bus, IArr indptr, IArr indices, CArr data, CArr vinit, CArr sbus, IArr pv, IArr pq,
+          int tail_policy)
+      : n_bus_(n_bus) {
+    if (indptr.size() != n_bus + 1) throw py::value_error("Ybus indptr must have n_bus + 1 entries");
+    if (indices.size() != data.size()) throw py::value_error("Ybus indices and data differ in length");
+    if (vinit.size() != n_bus || sbus.size() != n_bus) throw py::value_error("Vinit and Sbus must have n_bus entries");
+    if (indptr.at(n_bus) != indices.size()) throw py::value_error("Ybus indptr[-1] must equal nnz");
+    const double* dv = reinterpret_cast<const double*>(data.data());
+    int rc;
+    {
+      py::gil_scoped_release nogil;
+      rc = gs2g_session_create(device, n_bus, indptr.data(), indices.data(), dv,
+                               reinterpret_cast<const double*>(vinit.data()),
+                               reinterpret_cast<const double*>(sbus.data()), pv.data(), (int)pv.size(), pq.data(),
+                               (int)pq.size(), tail_policy, &s_);
+    }
+    check(rc);
+  }
+  ~Session() {
+    if (s_) gs2g_session_destroy(s_);
+  }
+  void close() {
+    if (s_) gs2g_session_destroy(s_);
+    s_ = nullptr;
+  }
+  gs2g_session* h() const {
+    if (!s_) throw std::runtime_error("session is closed");
+    return s_;
+  }
+
+  py::dict info() const {
+    gs2g_grid_info g{};
+    check(gs2g_grid_get_info(h(), &g));
+    py::dict d;
+    d["n_bus"] = g.n_bus;
+    d["nnz_y"] = g.nnz_y;
+    d["n_pvpq"] = g.n_pvpq;
+    d["n_pq"] = g.n_pq;
+    d["dim_j"] = g.dim_j;
+    d["nnz_j"] = g.nnz_j;
+    d["nnz_lu"] = g.nnz_lu;
+    d["head_dim"] = g.head_dim;
+    d["tail_dim"] = g.tail_dim;
+    d["tail_dim_exact"] = g.tail_dim_exact;
+    d["n_levels"] = g.n_levels;
+    d["n_supernodes"] = g.n_supernodes;
+    d["head_madds"] = g.head_madds;
+    d["schur_madds"] = g.schur_madds;
+    d["dense_madds"] = g.dense_madds;
+    d["plan_ms"] = g.plan_ms;
+    return d;
+  }
+
+  void set_branch_data(IArr f, IArr t, CArr yff, CArr yft, CArr ytf, CArr ytt) {
+    const int nb = (int)f.size();
+    if (t.size() != nb || yff.size() != nb || yft.size() != nb || ytf.size() != nb || ytt.size() != nb)
+      throw py::value_error("branch arrays differ in length");
+    auto d = [](const CArr& a) { return reinterpret_cast<const double*>(a.data()); };
+    check(gs2g_set_branch_data(h(), nb, f.data(), t.data(), d(yff), d(yft), d(ytf), d(ytt)));
+  }
+
+  void set_contingencies(IArr ptr, IArr ids) {
+    const int nr = (int)ptr.size() - 1;
+    if (nr < 0) throw py::value_error("ptr must have n_rows + 1 entries");
+    check(gs2g_set_contingencies(h(), nr, ptr.data(), ids.data()));
+  }
+
+  void clear_contingencies() { check(gs2g_set_contingencies(h(), 0, nullptr, nullptr)); }
+
+  void set_injections(DArr p, DArr q, double sn_mva) {
+    if (p.ndim() != 2 || q.ndim() != 2 || p.shape(1) != n_bus_ || q.shape(0) != p.shape(0) || q.shape(1) != n_bus_)
+      throw py::value_error("p_mw / q_mvar must both be (n_rows, n_bus)");
+    const int nr = (int)p.shape(0);
+    int rc;
+    {
+      py::gil_scoped_release nogil;
+      rc = gs2g_set_injections(h(), nr, p.data(), q.data(), sn_mva);
+    }
+    check(rc);
+  }
+
+  void clear_injections() { check(gs2g_set_injections(h(), 0, nullptr, nullptr, 1.0)); }
+
+  void set_start_rows(CArr v0) {
+    if (v0.ndim() != 2 || v0.shape(1) != n_bus_) throw py::value_error("start rows must be (n_rows, n_bus) complex");
+    check(gs2g_set_start_rows(h(), (int)v0.shape(0), reinterpret_cast<const double*>(v0.data())));
+  }
+
+  void set_start_rows_device(uintptr_t ptr, int n_rows) {
+    check(gs2g_set_start_rows_device(h(), n_rows, reinterpret_cast<const double*>(ptr)));
+  }
+
+  void set_sbus(CArr sbus) {
+    if (sbus.size() != n_bus_) throw py::value_error("Sbus must have n_bus entries");
+    check(gs2g_set_sbus(h(), reinterpret_cast<const double*>(sbus.data())));
+  }
+
+  void set_vinit(CArr v) {
+    if (v.size() != n_bus_) throw py::value_error("Vinit must have n_bus entries");
+    check(gs2g_set_vinit(h(), reinterpret_cast<const double*>(v.data())));
+  }
+
+  py::tuple solve_base(int max_iter, double tol, int precision, double pivot_floor) {
+    gs2g_run_opts o = make_opts(max_iter, tol, false, precision, GS2G_START_VINIT, pivot_floor, 1);
+    py::array_t<cplx> V(n_bus_);
+    int st = 0, it = 0;
+    double res = 0;
+    int rc;
+    {
+      cplx* vp = V.mutable_data();
+      py::gil_scoped_release nogil;
+      rc = gs2g_solve_base(h(), &o, reinterpret_cast<double*>(vp), &st, &it, &res);
+    }
+    check(rc);
+    return py::make_tuple(V, st, it, res);
+  }
+
+  double set_base_v(CArr v) {
+    if (v.size() != n_bus_) throw py::value_error("V must have n_bus entries");
+    double res = 0;
+    check(gs2g_set_base_v(h(), reinterpret_cast<const double*>(v.data()), &res));
+    return res;
+  }
+
+  void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas) {
+    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas);
+    int rc;
+    {
+      py::gil_scoped_release nogil;
+      rc = gs2g_run(h(), &o);
+    }
+    check(rc);
+  }
+
+  int n_rows() const { return gs2g_n_rows(h()); }
+
+  py::tuple results() const {
+    const int nr = gs2g_n_rows(h());
+    py::array_t<cplx> V({nr, n_bus_});
+    py::array_t<double> res(nr);
+    py::array_t<int> st(nr), it(nr);
+    int rc;
+    {
+      double* vp = reinterpret_cast<double*>(V.mutable_data());
+      double* rp = res.mutable_data();
+      int* sp = st.mutable_data();
+      int* ip = it.mutable_data();
+      py::gil_scoped_release nogil;
+      rc = gs2g_get_results(h(), vp, rp, sp, ip);
+    }
+    check(rc);
+    return py::make_tuple(V, res, st, it);
+  }
+
+  py::tuple device_results() const {
+    double *v = nullptr, *r = nullptr;
+    int *s = nullptr, *i = nullptr;
+    check(gs2g_get_device_results(h(), &v, &r, &s, &i));
+    return py::make_tuple((uintptr_t)v, (uintptr_t)r, (uintptr_t)s, (uintptr_t)i);
+  }
+
+  py::dict timings() const {
+    gs2g_timings t{};
+    check(gs2g_get_timings(h(), &t));
+    py::dict d;
+    d["plan_ms"] = t.plan_ms;
+    d["upload_ms"] = t.upload_ms;
+    d["kernel_ms"] = t.kernel_ms;
+    d["total_ms"] = t.total_ms;
+    d["total_iters"] = t.total_iters;
+    return d;
+  }
+
+  void sync() { check(gs2g_sync(h())); }
+
+ private:
+  gs2g_session* s_ = nullptr;
+  int n_bus_ = 0;
+};
+
+py::tuple acpf_nr(int device, int n_bus, IArr indptr, IArr indices, CArr data, CArr V, CArr sbus, IArr pv, IArr pq,
+                  int max_iter, double tol, int precision) {
+  if (V.size() != n_bus || sbus.size() != n_bus) throw py::value_error("V and Sbus must have n_bus entries");
+  py::array_t<cplx> out(n_bus);
+  std::memcpy(out.mutable_data(), V.data(), sizeof(cplx) * n_bus);
+  int conv = 0, it = 0;
+  double res = 0, ms = 0;
+  int rc;
+  {
+    double* op = reinterpret_cast<double*>(out.mutable_data());
+    py::gil_scoped_release nogil;
+    rc = gs2g_acpf_nr(device, n_bus, indptr.data(), indices.data(), reinterpret_cast<const double*>(data.data()), op,
+                      reinterpret_cast<const double*>(sbus.data()), pv.data(), (int)pv.size(), pq.data(),
+                      (int)pq.size(), max_iter, tol, precision, &conv, &it, &res, &ms);
+  }
+  check(rc);
+  return py::make_tuple(out, conv != 0, it, res, ms);
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_gs2g, m) {
+  m.doc() = "B200-native batched Newton-Raphson AC power flow (binding of include/gs2g.h)";
+  m.attr("PREC_FP64") = GS2G_PREC_FP64;
+  m.attr("PREC_MIXED") = GS2G_PREC_MIXED;
+  m.attr("START_VINIT") = GS2G_START_VINIT;
+  m.attr("START_BASE") = GS2G_START_BASE;
+  m.attr("START_ROWS") = GS2G_START_ROWS;
+  m.def("version", &gs2g_version);
+  m.def("max_edits_per_row", &gs2g_max_edits_per_row);
+  m.def("acpf_nr", &acpf_nr);
+  py::class_<Session>(m, "Session")
+      .def(py::init<int, int, IArr, IArr, CArr, CArr, CArr, IArr, IArr, int>(), py::arg("device"), py::arg("n_bus"),
+           py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),
+           py::arg("pq"), py::arg("tail_policy") = 1)
+      .def("close", &Session::close)
+      .def("info", &Session::info)
+      .def("set_branch_data", &Session::set_branch_data)
+      .def("set_contingencies", &Session::set_contingencies)
+      .def("clear_contingencies", &Session::clear_contingencies)
+      .def("set_injections", &Session::set_injections)
+      .def("clear_injections", &Session::clear_injections)
+      .def("set_start_rows", &Session::set_start_rows)
+      .def("set_start_rows_device", &Session::set_start_rows_device)
+      .def("set_sbus", &Session::set_sbus)
+      .def("set_vinit", &Session::set_vinit)
+      .def("solve_base", &Session::solve_base)
+      .def("set_base_v", &Session::set_base_v)
+      .def("run", &Session::run)
+      .def("n_rows", &Session::n_rows)
+      .def("results", &Session::results)
+      .def("device_results", &Session::device_results)
+      .def("timings", &Session::timings)
+      .def("sync", &Session::sync);
+}

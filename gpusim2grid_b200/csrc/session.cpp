@@ -1,0 +1,754 @@
+// Host side of the C-ABI (include/gs2g.h): sessions over one grid, batch-row
+// assembly (branch trips -> Ybus edit lists, islanding pre-check, injection
+// rows), device buffers and the launch of the persistent sweep kernel.
+//
+// Reference counterparts: the sessions of src/_cpp/contingency_analysis_session.cu,
+// injection_sweep_session.cu and scenario_sweep_session.cu, the branch-trip
+// deltas of contingency_analysis_helper.cpp:23-84 and the connectivity
+// pre-check of contingency_analysis_helper.cpp:634-651.
+#include "../../include/gs2g.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nr_kernel.cuh"
+#include "plan.hpp"
+
+namespace {
+
+thread_local std::string g_err;
+
+constexpr int kMaxEdits = 64;  // must match MAX_EDITS in nr_kernel.cu
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void ensure(size_t bytes) {
+    if (bytes <= n && p) return;
+    release();
+    ck(cudaMalloc(&p, bytes ? bytes : 16), "cudaMalloc");
+    n = bytes ? bytes : 16;
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct gs2g_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  gs2g::Plan plan;
+  gs2g::DevPlan dplan{};
+  std::vector<std::unique_ptr<DevBuf>> plan_bufs;
+  int n_bus = 0;
+  std::vector<double> ybus;  // canonical values, interleaved complex
+  std::vector<double> vinit, sbus, base_v;
+  bool has_base = false;
+  DevBuf d_ybus, d_vinit, d_sbus, d_basev;
+
+  // branch data
+  int n_branch = 0;
+  std::vector<int> br_from, br_to;
+  std::vector<double> yff, yft, ytf, ytt;
+  std::vector<int> k_ff, k_tt, k_ft, k_tf;  // Ybus entry of each branch term
+
+  // row definitions
+  int n_ctg = 0;
+  std::vector<int> ctg_ptr, ctg_ids;
+  int n_inj = 0;
+  std::vector<double> inj_sbus;  // [n_inj * n_bus] complex
+  int n_start = 0;
+  DevBuf d_v0rows;
+  bool rows_dirty = true;
+
+  // assembled rows on the device
+  int n_rows = 0;
+  bool rows_have_sbus = false, rows_have_edits = false, rows_have_skip = false;
+  DevBuf d_sbus_rows, d_edit_ptr, d_edit_k, d_edit_val, d_row_skip;
+  DevBuf d_v_out, d_res, d_status, d_iters;
+  DevBuf d_ws, d_queue;
+  // base-solve outputs (kept apart from the batch results)
+  DevBuf b_v, b_res, b_status, b_iters;
+
+  gs2g_timings tm{};
+  int last_rows_run = 0;
+};
+
+namespace {
+
+template <typename T>
+const T* upload_vec(gs2g_session* s, const std::vector<T>& v) {
+  auto b = std::make_unique<DevBuf>();
+  b->ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (!v.empty()) ck(cudaMemcpy(b->p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload plan");
+  const T* p = b->as<T>();
+  s->plan_bufs.push_back(std::move(b));
+  return p;
+}
+
+void upload_plan(gs2g_session* s) {
+  const gs2g::Plan& P = s->plan;
+  gs2g::DevPlan& D = s->dplan;
+  D.n_bus = P.n_bus;
+  D.nnz_y = P.nnz_y;
+  D.dim = P.dim;
+  D.p = P.p;
+  D.nt = P.nt;
+  D.ld = P.ld;
+  D.n_hv = P.n_hv;
+  D.n_levels = P.n_levels;
+  D.y_indptr = upload_vec(s, P.y_indptr);
+  D.y_indices = upload_vec(s, P.y_indices);
+  D.y_row = upload_vec(s, P.y_row);
+  D.jmap = upload_vec(s, P.jmap);
+  D.fP = upload_vec(s, P.fP);
+  D.fQ = upload_vec(s, P.fQ);
+  D.lev_ptr = upload_vec(s, P.lev_ptr);
+  D.task_out = upload_vec(s, P.task_out);
+  D.task_diag = upload_vec(s, P.task_diag);
+  D.task_pbeg = upload_vec(s, P.task_pbeg);
+  D.task_pend = upload_vec(s, P.task_pend);
+  D.task_has_a = upload_vec(s, P.task_has_a);
+  D.pair_l = upload_vec(s, P.pair_l);
+  D.pair_u = upload_vec(s, P.pair_u);
+  D.lev_piv_ptr = upload_vec(s, P.lev_piv_ptr);
+  D.lev_piv = upload_vec(s, P.lev_piv);
+  D.sn_w = upload_vec(s, P.sn_w);
+  D.sn_t = upload_vec(s, P.sn_t);
+  D.sn_L = upload_vec(s, P.sn_L);
+  D.sn_U = upload_vec(s, P.sn_U);
+  D.sn_tidx = upload_vec(s, P.sn_tidx);
+  D.tidx = upload_vec(s, P.tidx);
+  D.schur_ptr = upload_vec(s, P.schur_ptr);
+  D.schur_sn = upload_vec(s, P.schur_sn);
+  D.schur_a = upload_vec(s, P.schur_a);
+  D.fw_ptr = upload_vec(s, P.fw_ptr);
+  D.fw_col = upload_vec(s, P.fw_col);
+  D.fw_pos = upload_vec(s, P.fw_pos);
+  D.bw_ptr = upload_vec(s, P.bw_ptr);
+  D.bw_row = upload_vec(s, P.bw_row);
+  D.bw_pos = upload_vec(s, P.bw_pos);
+}
+
+// Ybus entry index of (i, j), -1 if not in the pattern.
+int ybus_find(const gs2g::Plan& P, int i, int j) {
+  const int* b = P.y_indices.data() + P.y_indptr[i];
+  const int* e = P.y_indices.data() + P.y_indptr[i + 1];
+  const int* it = std::lower_bound(b, e, j);
+  return (it != e && *it == j) ? int(it - P.y_indices.data()) : -1;
+}
+
+struct DSU {
+  std::vector<int> p;
+  explicit DSU(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
+  int f(int x) {
+    while (p[x] != x) x = p[x] = p[p[x]];
+    return x;
+  }
+  bool u(int a, int b) {
+    a = f(a);
+    b = f(b);
+    if (a == b) return false;
+    p[a] = b;
+    return true;
+  }
+};
+
+void assemble_rows(gs2g_session* s) {
+  if (!s->rows_dirty) return;
+  const int n = s->n_bus;
+  int nr = 0;
+  if (s->n_ctg > 0 && s->n_inj > 0 && s->n_ctg != s->n_inj)
+    throw std::invalid_argument("topology rows (" + std::to_string(s->n_ctg) + ") and injection rows (" +
+                                std::to_string(s->n_inj) + ") differ in number");
+  nr = std::max(s->n_ctg, s->n_inj);
+  s->n_rows = nr;
+  s->rows_have_sbus = s->n_inj > 0;
+  s->rows_have_edits = s->n_ctg > 0;
+  s->rows_have_skip = false;
+  if (nr == 0) {
+    s->rows_dirty = false;
+    return;
+  }
+  if (s->rows_have_sbus) {
+    s->d_sbus_rows.ensure(s->inj_sbus.size() * sizeof(double));
+    ck(cudaMemcpy(s->d_sbus_rows.p, s->inj_sbus.data(), s->inj_sbus.size() * sizeof(double), cudaMemcpyHostToDevice),
+       "upload sbus rows");
+  }
+  if (s->rows_have_edits) {
+    std::vector<int> eptr(nr + 1, 0), ek;
+    std::vector<double> ev;
+    std::vector<uint8_t> skip(nr, 0);
+    std::vector<int> uniq;
+    bool any_skip = false;
+    for (int r = 0; r < nr; ++r) {
+      uniq.assign(s->ctg_ids.begin() + s->ctg_ptr[r], s->ctg_ids.begin() + s->ctg_ptr[r + 1]);
+      std::sort(uniq.begin(), uniq.end());
+      uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+      if (!uniq.empty()) {
+        DSU d(n);
+        size_t ui = 0;
+        int comps = n;
+        for (int l = 0; l < s->n_branch; ++l) {
+          while (ui < uniq.size() && uniq[ui] < l) ++ui;
+          if (ui < uniq.size() && uniq[ui] == l) continue;
+          if (d.u(s->br_from[l], s->br_to[l])) --comps;
+        }
+        if (comps > 1) {
+          skip[r] = 1;
+          any_skip = true;
+          eptr[r + 1] = (int)ek.size();
+          continue;
+        }
+      }
+      std::map<int, std::complex<double>> acc;
+      for (int l : uniq) {
+        const double* v[4] = {&s->yff[2 * l], &s->ytt[2 * l], &s->yft[2 * l], &s->ytf[2 * l]};
+        const int kk[4] = {s->k_ff[l], s->k_tt[l], s->k_ft[l], s->k_tf[l]};
+        for (int q = 0; q < 4; ++q) acc[kk[q]] += std::complex<double>(v[q][0], v[q][1]);
+      }
+      if ((int)acc.size() > kMaxEdits)
+        throw std::invalid_argument("row " + std::to_string(r) + " trips too many branches (" +
+                                    std::to_string(acc.size()) + " Ybus edits > " + std::to_string(kMaxEdits) + ")");
+      for (auto& kv : acc) {
+        ek.push_back(kv.first);
+        ev.push_back(kv.second.real());
+        ev.push_back(kv.second.imag());
+      }
+      eptr[r + 1] = (int)ek.size();
+    }
+    s->d_edit_ptr.ensure(eptr.size() * sizeof(int));
+    ck(cudaMemcpy(s->d_edit_ptr.p, eptr.data(), eptr.size() * sizeof(int), cudaMemcpyHostToDevice), "upload edits");
+    s->d_edit_k.ensure(std::max<size_t>(ek.size(), 1) * sizeof(int));
+    s->d_edit_val.ensure(std::max<size_t>(ev.size(), 2) * sizeof(double));
+    if (!ek.empty()) {
+      ck(cudaMemcpy(s->d_edit_k.p, ek.data(), ek.size() * sizeof(int), cudaMemcpyHostToDevice), "upload edits");
+      ck(cudaMemcpy(s->d_edit_val.p, ev.data(), ev.size() * sizeof(double), cudaMemcpyHostToDevice), "upload edits");
+    }
+    if (any_skip) {
+      std::vector<int> sk(skip.begin(), skip.end());
+      s->d_row_skip.ensure(sk.size() * sizeof(int));
+      ck(cudaMemcpy(s->d_row_skip.p, sk.data(), sk.size() * sizeof(int), cudaMemcpyHostToDevice), "upload skip");
+      s->rows_have_skip = true;
+    }
+  }
+  s->rows_dirty = false;
+}
+
+struct OutBufs {
+  double* v;
+  double* res;
+  int* status;
+  int* iters;
+};
+
+float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
+             const double* sbus, int64_t sbus_stride, bool use_rows, const OutBufs& out, int n_ctas_req) {
+  if (o.precision != GS2G_PREC_FP64 && o.precision != GS2G_PREC_MIXED)
+    throw std::invalid_argument("precision must be GS2G_PREC_FP64 or GS2G_PREC_MIXED");
+  if (o.max_iter < 0) throw std::invalid_argument("max_iter must be >= 0");
+  int n_ctas = n_ctas_req > 0 ? n_ctas_req : gs2g::sweep_ctas(o.precision, s->device);
+  n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
+  const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
+  s->d_ws.ensure((size_t)wsb * n_ctas);
+  s->d_queue.ensure(sizeof(int));
+  gs2g::SweepArgs a{};
+  a.n_rows = n_rows;
+  a.ybus = s->d_ybus.as<double>();
+  a.v0 = v0;
+  a.v0_stride = v0_stride;
+  a.sbus = sbus;
+  a.sbus_stride = sbus_stride;
+  a.edit_ptr = use_rows && s->rows_have_edits ? s->d_edit_ptr.as<int>() : nullptr;
+  a.edit_k = use_rows && s->rows_have_edits ? s->d_edit_k.as<int>() : nullptr;
+  a.edit_val = use_rows && s->rows_have_edits ? s->d_edit_val.as<double>() : nullptr;
+  a.row_skip = use_rows && s->rows_have_skip ? s->d_row_skip.as<int>() : nullptr;
+  a.max_iter = o.max_iter;
+  a.tol = o.tol;
+  a.fixed_iters = o.fixed_iters;
+  a.v_out = out.v;
+  a.res_out = out.res;
+  a.status_out = out.status;
+  a.iters_out = out.iters;
+  a.queue = s->d_queue.as<int>();
+  a.workspace = s->d_ws.as<char>();
+  a.ws_stride = wsb;
+  a.pivot_floor = o.pivot_floor;
+  ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
+  ck(cudaEventRecord(s->ev0, s->stream), "event");
+  if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
+  ck(cudaEventRecord(s->ev1, s->stream), "event");
+  ck(cudaStreamSynchronize(s->stream), "sweep");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
+  return ms;
+}
+
+int fail(const std::exception& e) {
+  g_err = e.what();
+  if (dynamic_cast<const std::invalid_argument*>(&e)) return GS2G_ERR_INVALID;
+  if (dynamic_cast<const CudaError*>(&e)) return GS2G_ERR_CUDA;
+  return GS2G_ERR_RUNTIME;
+}
+
+#define GS2G_TRY try {
+#define GS2G_CATCH                                  \
+  return GS2G_OK;                                   \
+  }                                                 \
+  catch (const std::exception& e) { return fail(e); } \
+  catch (...) {                                     \
+    g_err = "unknown error";                        \
+    return GS2G_ERR_RUNTIME;                        \
+  }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (dev >= 0 && dev != prev) ck(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+void canonical_csr(int n, const int* indptr, const int* indices, const double* values, std::vector<int>& ip,
+                   std::vector<int>& ix, std::vector<double>& vals) {
+  if (indptr[0] != 0) throw std::invalid_argument("Ybus indptr[0] must be 0");
+  ip.assign(n + 1, 0);
+  ix.clear();
+  vals.clear();
+  std::vector<std::pair<int, std::complex<double>>> rowv;
+  for (int i = 0; i < n; ++i) {
+    if (indptr[i + 1] < indptr[i]) throw std::invalid_argument("Ybus indptr must be non-decreasing");
+    rowv.clear();
+    for (int k = indptr[i]; k < indptr[i + 1]; ++k) {
+      if (indices[k] < 0 || indices[k] >= n) throw std::invalid_argument("Ybus column index out of range");
+      rowv.emplace_back(indices[k], std::complex<double>(values[2 * k], values[2 * k + 1]));
+    }
+    std::sort(rowv.begin(), rowv.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t q = 0; q < rowv.size(); ++q) {
+      if (!ix.empty() && (int)ix.size() > ip[i] && ix.back() == rowv[q].first) {
+        vals[vals.size() - 2] += rowv[q].second.real();
+        vals[vals.size() - 1] += rowv[q].second.imag();
+      } else {
+        ix.push_back(rowv[q].first);
+        vals.push_back(rowv[q].second.real());
+        vals.push_back(rowv[q].second.imag());
+      }
+    }
+    ip[i + 1] = (int)ix.size();
+  }
+}
+
+gs2g_run_opts checked(const gs2g_run_opts* o) {
+  if (!o) throw std::invalid_argument("run options must not be NULL");
+  return *o;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gs2g_last_error(void) { return g_err.c_str(); }
+int gs2g_version(void) { return 100; }
+int gs2g_max_edits_per_row(void) { return kMaxEdits; }
+
+int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices,
+                        const double* ybus_values, const double* vinit, const double* sbus, const int* pv, int n_pv,
+                        const int* pq, int n_pq, int tail_policy, gs2g_session** out) {
+  GS2G_TRY
+  if (!out) throw std::invalid_argument("out must not be NULL");
+  *out = nullptr;
+  if (n_bus <= 0 || !ybus_indptr || !ybus_indices || !ybus_values || !vinit || !sbus)
+    throw std::invalid_argument("session_create: missing grid arrays");
+  if ((n_pv > 0 && !pv) || (n_pq > 0 && !pq) || n_pv < 0 || n_pq < 0)
+    throw std::invalid_argument("session_create: bad pv/pq");
+  auto s = std::make_unique<gs2g_session>();
+  if (device < 0) ck(cudaGetDevice(&device), "cudaGetDevice");
+  s->device = device;
+  DeviceGuard g(device);
+  s->n_bus = n_bus;
+  std::vector<int> ip, ix;
+  canonical_csr(n_bus, ybus_indptr, ybus_indices, ybus_values, ip, ix, s->ybus);
+  gs2g::TailOptions topt;
+  topt.policy = tail_policy;
+  s->plan = gs2g::build_plan(n_bus, ip.data(), ix.data(), pv, n_pv, pq, n_pq, topt);
+  s->tm.plan_ms = s->plan.build_ms;
+  s->vinit.assign(vinit, vinit + 2 * n_bus);
+  s->sbus.assign(sbus, sbus + 2 * n_bus);
+  ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  ck(cudaEventCreate(&s->ev0), "event");
+  ck(cudaEventCreate(&s->ev1), "event");
+  upload_plan(s.get());
+  s->d_ybus.ensure(s->ybus.size() * sizeof(double));
+  ck(cudaMemcpy(s->d_ybus.p, s->ybus.data(), s->ybus.size() * sizeof(double), cudaMemcpyHostToDevice), "upload Ybus");
+  s->d_vinit.ensure(2 * n_bus * sizeof(double));
+  ck(cudaMemcpy(s->d_vinit.p, vinit, 2 * n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Vinit");
+  s->d_sbus.ensure(2 * n_bus * sizeof(double));
+  ck(cudaMemcpy(s->d_sbus.p, sbus, 2 * n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Sbus");
+  *out = s.release();
+  GS2G_CATCH
+}
+
+int gs2g_session_destroy(gs2g_session* s) {
+  GS2G_TRY
+  if (!s) return GS2G_OK;
+  {
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+  }
+  GS2G_CATCH
+}
+
+int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out) {
+  GS2G_TRY
+  if (!s || !out) throw std::invalid_argument("NULL argument");
+  const gs2g::Plan& P = s->plan;
+  out->n_bus = P.n_bus;
+  out->nnz_y = P.nnz_y;
+  out->n_pvpq = P.n_pvpq;
+  out->n_pq = P.n_pq;
+  out->dim_j = P.dim;
+  out->nnz_j = P.nnz_j;
+  out->nnz_lu = P.nnz_lu;
+  out->head_dim = P.p;
+  out->tail_dim = P.nt;
+  out->tail_dim_exact = P.n_tail_exact;
+  out->n_levels = P.n_levels;
+  out->n_supernodes = P.n_sn;
+  out->head_madds = P.head_madds;
+  out->schur_madds = P.schur_madds;
+  out->dense_madds = P.dense_madds;
+  out->plan_ms = P.build_ms;
+  GS2G_CATCH
+}
+
+int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const int* to, const double* yff,
+                         const double* yft, const double* ytf, const double* ytt) {
+  GS2G_TRY
+  if (!s || n_branch < 0 || (n_branch > 0 && (!from || !to || !yff || !yft || !ytf || !ytt)))
+    throw std::invalid_argument("set_branch_data: bad arguments");
+  std::vector<int> kff(n_branch), ktt(n_branch), kft(n_branch), ktf(n_branch);
+  for (int l = 0; l < n_branch; ++l) {
+    const int f = from[l], t = to[l];
+    if (f < 0 || f >= s->n_bus || t < 0 || t >= s->n_bus || f == t)
+      throw std::invalid_argument("set_branch_data: branch " + std::to_string(l) + " has a bad endpoint");
+    kff[l] = ybus_find(s->plan, f, f);
+    ktt[l] = ybus_find(s->plan, t, t);
+    kft[l] = ybus_find(s->plan, f, t);
+    ktf[l] = ybus_find(s->plan, t, f);
+    if (kff[l] < 0 || ktt[l] < 0 || kft[l] < 0 || ktf[l] < 0)
+      throw std::invalid_argument("set_branch_data: branch " + std::to_string(l) + " is not in the Ybus pattern");
+  }
+  s->n_branch = n_branch;
+  s->br_from.assign(from, from + n_branch);
+  s->br_to.assign(to, to + n_branch);
+  s->yff.assign(yff, yff + 2 * n_branch);
+  s->yft.assign(yft, yft + 2 * n_branch);
+  s->ytf.assign(ytf, ytf + 2 * n_branch);
+  s->ytt.assign(ytt, ytt + 2 * n_branch);
+  s->k_ff.swap(kff);
+  s->k_tt.swap(ktt);
+  s->k_ft.swap(kft);
+  s->k_tf.swap(ktf);
+  s->rows_dirty = true;
+  GS2G_CATCH
+}
+
+int gs2g_set_contingencies(gs2g_session* s, int n_rows, const int* ptr, const int* ids) {
+  GS2G_TRY
+  if (!s || n_rows < 0) throw std::invalid_argument("set_contingencies: bad arguments");
+  if (n_rows > 0) {
+    if (!ptr || ptr[0] != 0) throw std::invalid_argument("set_contingencies: ptr[0] must be 0");
+    for (int r = 0; r < n_rows; ++r)
+      if (ptr[r + 1] < ptr[r]) throw std::invalid_argument("set_contingencies: ptr must be non-decreasing");
+    const int nnz = ptr[n_rows];
+    if (nnz > 0 && !ids) throw std::invalid_argument("set_contingencies: ids must not be NULL");
+    for (int q = 0; q < nnz; ++q)
+      if (ids[q] < 0 || ids[q] >= s->n_branch)
+        throw std::invalid_argument("set_contingencies: branch index " + std::to_string(ids[q]) +
+                                    " out of range (n_branches=" + std::to_string(s->n_branch) + ")");
+    s->ctg_ptr.assign(ptr, ptr + n_rows + 1);
+    s->ctg_ids.assign(ids, ids + nnz);
+  } else {
+    s->ctg_ptr.clear();
+    s->ctg_ids.clear();
+  }
+  s->n_ctg = n_rows;
+  s->rows_dirty = true;
+  GS2G_CATCH
+}
+
+int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const double* q_mvar, double sn_mva) {
+  GS2G_TRY
+  if (!s || n_rows < 0) throw std::invalid_argument("set_injections: bad arguments");
+  if (n_rows > 0) {
+    if (!p_mw || !q_mvar) throw std::invalid_argument("set_injections: p_mw / q_mvar must not be NULL");
+    if (!(sn_mva > 0)) throw std::invalid_argument("set_injections: sn_mva must be positive");
+    const int n = s->n_bus;
+    s->inj_sbus.resize((size_t)2 * n_rows * n);
+    const double inv = 1.0 / sn_mva;
+    for (size_t q = 0; q < (size_t)n_rows * n; ++q) {
+      s->inj_sbus[2 * q] = p_mw[q] * inv;
+      s->inj_sbus[2 * q + 1] = q_mvar[q] * inv;
+    }
+  } else {
+    s->inj_sbus.clear();
+  }
+  s->n_inj = n_rows;
+  s->rows_dirty = true;
+  GS2G_CATCH
+}
+
+int gs2g_set_start_rows(gs2g_session* s, int n_rows, const double* v0) {
+  GS2G_TRY
+  if (!s || n_rows < 0 || (n_rows > 0 && !v0)) throw std::invalid_argument("set_start_rows: bad arguments");
+  DeviceGuard g(s->device);
+  const size_t bytes = (size_t)n_rows * s->n_bus * 2 * sizeof(double);
+  s->d_v0rows.ensure(bytes);
+  if (bytes) ck(cudaMemcpy(s->d_v0rows.p, v0, bytes, cudaMemcpyHostToDevice), "upload start rows");
+  s->n_start = n_rows;
+  GS2G_CATCH
+}
+
+int gs2g_set_start_rows_device(gs2g_session* s, int n_rows, const double* v0_dev) {
+  GS2G_TRY
+  if (!s || n_rows < 0 || (n_rows > 0 && !v0_dev)) throw std::invalid_argument("set_start_rows_device: bad arguments");
+  DeviceGuard g(s->device);
+  const size_t bytes = (size_t)n_rows * s->n_bus * 2 * sizeof(double);
+  s->d_v0rows.ensure(bytes);
+  if (bytes) ck(cudaMemcpyAsync(s->d_v0rows.p, v0_dev, bytes, cudaMemcpyDeviceToDevice, s->stream), "copy start rows");
+  ck(cudaStreamSynchronize(s->stream), "copy start rows");
+  s->n_start = n_rows;
+  GS2G_CATCH
+}
+
+int gs2g_set_sbus(gs2g_session* s, const double* sbus) {
+  GS2G_TRY
+  if (!s || !sbus) throw std::invalid_argument("set_sbus: bad arguments");
+  DeviceGuard g(s->device);
+  s->sbus.assign(sbus, sbus + 2 * s->n_bus);
+  ck(cudaMemcpy(s->d_sbus.p, sbus, 2 * s->n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Sbus");
+  GS2G_CATCH
+}
+
+int gs2g_set_vinit(gs2g_session* s, const double* vinit) {
+  GS2G_TRY
+  if (!s || !vinit) throw std::invalid_argument("set_vinit: bad arguments");
+  DeviceGuard g(s->device);
+  s->vinit.assign(vinit, vinit + 2 * s->n_bus);
+  ck(cudaMemcpy(s->d_vinit.p, vinit, 2 * s->n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Vinit");
+  GS2G_CATCH
+}
+
+int gs2g_solve_base(gs2g_session* s, const gs2g_run_opts* o_, double* v_out, int* status, int* iters,
+                    double* residual) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  gs2g_run_opts o = checked(o_);
+  DeviceGuard g(s->device);
+  const int n = s->n_bus;
+  s->b_v.ensure(2 * n * sizeof(double));
+  s->b_res.ensure(sizeof(double));
+  s->b_status.ensure(sizeof(int));
+  s->b_iters.ensure(sizeof(int));
+  OutBufs ob{s->b_v.as<double>(), s->b_res.as<double>(), s->b_status.as<int>(), s->b_iters.as<int>()};
+  const float ms = launch(s, o, 1, s->d_vinit.as<double>(), 0, s->d_sbus.as<double>(), 0, false, ob, 1);
+  s->tm.kernel_ms = ms;
+  int st = 0, it = 0;
+  double res = 0;
+  s->base_v.resize(2 * n);
+  ck(cudaMemcpy(s->base_v.data(), s->b_v.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost), "read base V");
+  ck(cudaMemcpy(&st, s->b_status.p, sizeof(int), cudaMemcpyDeviceToHost), "read base status");
+  ck(cudaMemcpy(&it, s->b_iters.p, sizeof(int), cudaMemcpyDeviceToHost), "read base iters");
+  ck(cudaMemcpy(&res, s->b_res.p, sizeof(double), cudaMemcpyDeviceToHost), "read base residual");
+  s->d_basev.ensure(2 * n * sizeof(double));
+  ck(cudaMemcpy(s->d_basev.p, s->b_v.p, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice), "keep base V");
+  s->has_base = true;
+  if (v_out) std::memcpy(v_out, s->base_v.data(), 2 * n * sizeof(double));
+  if (status) *status = st;
+  if (iters) *iters = it;
+  if (residual) *residual = res;
+  GS2G_CATCH
+}
+
+int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual) {
+  GS2G_TRY
+  if (!s || !v) throw std::invalid_argument("set_base_v: bad arguments");
+  DeviceGuard g(s->device);
+  const int n = s->n_bus;
+  s->d_basev.ensure(2 * n * sizeof(double));
+  ck(cudaMemcpy(s->d_basev.p, v, 2 * n * sizeof(double), cudaMemcpyHostToDevice), "upload base V");
+  s->b_v.ensure(2 * n * sizeof(double));
+  s->b_res.ensure(sizeof(double));
+  s->b_status.ensure(sizeof(int));
+  s->b_iters.ensure(sizeof(int));
+  gs2g_run_opts o{};
+  o.max_iter = 0;
+  o.tol = 0;
+  o.fixed_iters = 1;
+  o.precision = GS2G_PREC_FP64;
+  OutBufs ob{s->b_v.as<double>(), s->b_res.as<double>(), s->b_status.as<int>(), s->b_iters.as<int>()};
+  launch(s, o, 1, s->d_basev.as<double>(), 0, s->d_sbus.as<double>(), 0, false, ob, 1);
+  double res = 0;
+  ck(cudaMemcpy(&res, s->b_res.p, sizeof(double), cudaMemcpyDeviceToHost), "read residual");
+  s->base_v.assign(v, v + 2 * n);
+  s->has_base = true;
+  if (residual) *residual = res;
+  GS2G_CATCH
+}
+
+int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  gs2g_run_opts o = checked(o_);
+  DeviceGuard g(s->device);
+  auto t0 = std::chrono::steady_clock::now();
+  assemble_rows(s);
+  s->tm.upload_ms = ms_since(t0);
+  const int nr = s->n_rows;
+  const int n = s->n_bus;
+  const double* v0 = s->d_vinit.as<double>();
+  int64_t v0s = 0;
+  if (o.start == GS2G_START_BASE) {
+    if (!s->has_base) throw std::runtime_error("start=BASE needs a base case (solve_base or set_base_v first)");
+    v0 = s->d_basev.as<double>();
+  } else if (o.start == GS2G_START_ROWS) {
+    if (s->n_start != nr)
+      throw std::invalid_argument("start=ROWS needs one start voltage per row (" + std::to_string(nr) + "), got " +
+                                  std::to_string(s->n_start));
+    v0 = s->d_v0rows.as<double>();
+    v0s = n;
+  } else if (o.start != GS2G_START_VINIT) {
+    throw std::invalid_argument("unknown start mode");
+  }
+  const double* sb = s->rows_have_sbus ? s->d_sbus_rows.as<double>() : s->d_sbus.as<double>();
+  const int64_t sbs = s->rows_have_sbus ? n : 0;
+  s->d_v_out.ensure((size_t)std::max(nr, 1) * n * 2 * sizeof(double));
+  s->d_res.ensure((size_t)std::max(nr, 1) * sizeof(double));
+  s->d_status.ensure((size_t)std::max(nr, 1) * sizeof(int));
+  s->d_iters.ensure((size_t)std::max(nr, 1) * sizeof(int));
+  OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>()};
+  s->tm.kernel_ms = launch(s, o, nr, v0, v0s, sb, sbs, true, ob, o.n_ctas);
+  s->last_rows_run = nr;
+  s->tm.total_ms = ms_since(t0);
+  s->tm.total_iters = -1;
+  GS2G_CATCH
+}
+
+int gs2g_n_rows(const gs2g_session* s) { return s ? s->last_rows_run : 0; }
+
+int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  DeviceGuard g(s->device);
+  const size_t nr = s->last_rows_run, n = s->n_bus;
+  if (v_out && nr)
+    ck(cudaMemcpy(v_out, s->d_v_out.p, nr * n * 2 * sizeof(double), cudaMemcpyDeviceToHost), "read V");
+  if (residuals && nr) ck(cudaMemcpy(residuals, s->d_res.p, nr * sizeof(double), cudaMemcpyDeviceToHost), "read res");
+  if (status && nr) ck(cudaMemcpy(status, s->d_status.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (iters && nr) ck(cudaMemcpy(iters, s->d_iters.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read iters");
+  GS2G_CATCH
+}
+
+int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  if (v) *v = s->d_v_out.as<double>();
+  if (residuals) *residuals = s->d_res.as<double>();
+  if (status) *status = s->d_status.as<int>();
+  if (iters) *iters = s->d_iters.as<int>();
+  GS2G_CATCH
+}
+
+int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out) {
+  GS2G_TRY
+  if (!s || !out) throw std::invalid_argument("NULL argument");
+  *out = s->tm;
+  if (s->last_rows_run > 0) {
+    DeviceGuard g(s->device);
+    std::vector<int> it(s->last_rows_run);
+    ck(cudaMemcpy(it.data(), s->d_iters.p, it.size() * sizeof(int), cudaMemcpyDeviceToHost), "read iters");
+    int64_t tot = 0;
+    for (int v : it) tot += v;
+    out->total_iters = tot;
+  }
+  GS2G_CATCH
+}
+
+int gs2g_sync(gs2g_session* s) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  DeviceGuard g(s->device);
+  ck(cudaStreamSynchronize(s->stream), "sync");
+  GS2G_CATCH
+}
+
+int gs2g_acpf_nr(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices, const double* ybus_values,
+                 double* v_inout, const double* sbus, const int* pv, int n_pv, const int* pq, int n_pq, int max_iter,
+                 double tol, int precision, int* converged, int* iters, double* residual, double* kernel_ms) {
+  gs2g_session* s = nullptr;
+  int rc = gs2g_session_create(device, n_bus, ybus_indptr, ybus_indices, ybus_values, v_inout, sbus, pv, n_pv, pq,
+                               n_pq, 1, &s);
+  if (rc) return rc;
+  gs2g_run_opts o{};
+  o.max_iter = max_iter;
+  o.tol = tol;
+  o.fixed_iters = 0;
+  o.precision = precision;
+  o.start = GS2G_START_VINIT;
+  int st = 0, it = 0;
+  double res = 0;
+  rc = gs2g_solve_base(s, &o, v_inout, &st, &it, &res);
+  if (rc == 0) {
+    if (converged) *converged = st == GS2G_ROW_CONVERGED ? 1 : 0;
+    if (iters) *iters = it;
+    if (residual) *residual = res;
+    if (kernel_ms) *kernel_ms = s->tm.kernel_ms;
+  }
+  std::string keep = g_err;
+  gs2g_session_destroy(s);
+  if (rc) g_err = keep;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+/*
+ * gs2g.h — C-ABI of the B200-native batched Newton–Raphson AC power flow.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (0 = success) and a thread-local last-error string.  No CUDA, torch or C++
+ * types cross this boundary.  Complex arrays are interleaved (re, im) doubles.
+ *
+ * The entry points replace the reference's pybind11 surface for its bare
+ * [pvpq | pq] Newton–Raphson path (file:line of the reference project):
+ *   gs2g_session_create      AcPfNrSession / ContingencyAnalysisSession /
+ *                            InjectionSweepSession / ScenarioSweepSession
+ *                            constructors in array-tuple mode
+ *                            (src/_cpp/python_bindings.cpp:1369, :1745, :2167, :2424)
+ *   gs2g_set_branch_data     ContingencyAnalysisSession.set_branch_data
+ *                            (src/gpusim2grid/contingency_analysis/gpu_facade.py:569)
+ *   gs2g_set_contingencies   build_contingencies / set_topology
+ *                            (src/_cpp/contingency_analysis_session.cu:188,
+ *                             src/_cpp/scenario_sweep_session.cu:1009)
+ *   gs2g_set_injections      InjectionSweepSession::set_injections
+ *                            (src/_cpp/injection_sweep_session.cu:144-169, :239-245)
+ *   gs2g_run                 ContingencyAnalysisSession::run / InjectionSweepSession::run /
+ *                            ScenarioSweepSession::run
+ *                            (src/_cpp/contingency_analysis_session.cu:394,
+ *                             src/_cpp/injection_sweep_session.cu:194,
+ *                             src/_cpp/scenario_sweep_session.cu:1267)
+ *   gs2g_get_*               V_results / last_residuals / get_row_status /
+ *                            get_row_iterations accessors
+ *                            (src/gpusim2grid/contingency_analysis/gpu_facade.py:1025, :1203)
+ *   gs2g_acpf_nr             acpf_nr_gpu (src/_cpp/python_bindings.cpp:1266-1285,
+ *                            src/_cpp/acpf_nr.hpp:27-40)
+ */
+#ifndef GS2G_H
+#define GS2G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS2G_OK 0
+#define GS2G_ERR_INVALID 1   /* bad argument (reference: ValueError / std::invalid_argument) */
+#define GS2G_ERR_RUNTIME 2   /* runtime failure (reference: RuntimeError) */
+#define GS2G_ERR_CUDA 3      /* a CUDA call failed */
+
+/* row status codes (src/_cpp/contingency/row_status.hpp:33-42) */
+#define GS2G_ROW_CONVERGED 0
+#define GS2G_ROW_MAX_ITER 1
+#define GS2G_ROW_DIVERGED 2
+#define GS2G_ROW_NOT_SIMULATED 3
+
+/* linear-algebra precision of the Newton step */
+#define GS2G_PREC_FP64 0  /* J, LU and solves in FP64 */
+#define GS2G_PREC_MIXED 1 /* J, LU and solves in FP32; mismatch, norm and V in FP64 */
+
+/* start voltage of the rows */
+#define GS2G_START_VINIT 0 /* the session's Vinit (flat start) for every row */
+#define GS2G_START_BASE 1  /* the converged base case, as the reference's batch sources */
+#define GS2G_START_ROWS 2  /* one start per row, given by gs2g_set_start_rows */
+
+typedef struct gs2g_session gs2g_session;
+
+typedef struct gs2g_grid_info {
+  int n_bus, nnz_y, n_pvpq, n_pq, dim_j;
+  int64_t nnz_j, nnz_lu;
+  int head_dim, tail_dim, tail_dim_exact, n_levels, n_supernodes;
+  int64_t head_madds, schur_madds, dense_madds;
+  double plan_ms;
+} gs2g_grid_info;
+
+typedef struct gs2g_run_opts {
+  int max_iter;       /* Newton steps allowed per row */
+  double tol;         /* ||F||inf threshold, per unit */
+  int fixed_iters;    /* 1: exactly max_iter steps, then the residual (the reference's
+                         chunked schedule); 0: stop each row at tol (continuous) */
+  int precision;      /* GS2G_PREC_* */
+  int start;          /* GS2G_START_* */
+  double pivot_floor; /* static-pivot floor, 0 disables */
+  int n_ctas;         /* persistent CTAs, <= 0 for one full wave */
+} gs2g_run_opts;
+
+typedef struct gs2g_timings {
+  double plan_ms;      /* symbolic analysis, once per session */
+  double upload_ms;    /* last host-to-device copy of row data (wall) */
+  double kernel_ms;    /* last sweep, CUDA events on the session stream */
+  double total_ms;     /* last gs2g_run, wall */
+  int64_t total_iters; /* sum of Newton steps over the rows of the last run */
+} gs2g_timings;
+
+const char* gs2g_last_error(void);
+int gs2g_version(void);
+int gs2g_max_edits_per_row(void);
+
+/* Session over one grid given as the reference's array tuple
+ * (Ybus CSR, Vinit, Sbus, pv, pq).  `device` < 0 means the current device. */
+int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices,
+                        const double* ybus_values, const double* vinit, const double* sbus,
+                        const int* pv, int n_pv, const int* pq, int n_pq, int tail_policy,
+                        gs2g_session** out);
+int gs2g_session_destroy(gs2g_session* s);
+int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
+
+/* π-model branch admittances, needed to trip branches. */
+int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const int* to,
+                         const double* yff, const double* yft, const double* ytf, const double* ytt);
+/* Batch rows as tripped-branch lists (CSR: row r trips ids[ptr[r]..ptr[r+1])).
+ * n_rows = 0 clears them.  With injections also set, rows combine both. */
+int gs2g_set_contingencies(gs2g_session* s, int n_rows, const int* ptr, const int* ids);
+/* Per-row injections in MW / MVAr, row-major [n_rows x n_bus]; Sbus = (p + jq)/sn_mva.
+ * n_rows = 0 clears them. */
+int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const double* q_mvar, double sn_mva);
+/* Per-row start voltages, complex [n_rows x n_bus] (used with GS2G_START_ROWS). */
+int gs2g_set_start_rows(gs2g_session* s, int n_rows, const double* v0);
+/* Same, from device memory already on the session's device. */
+int gs2g_set_start_rows_device(gs2g_session* s, int n_rows, const double* v0_dev);
+/* Replace the base injections (single-solve resolve). */
+int gs2g_set_sbus(gs2g_session* s, const double* sbus);
+/* Replace Vinit. */
+int gs2g_set_vinit(gs2g_session* s, const double* vinit);
+
+/* Solve the base case (no trips, base Sbus) from Vinit; keeps it as the
+ * GS2G_START_BASE start.  Fills status/iters/residual if not NULL. */
+int gs2g_solve_base(gs2g_session* s, const gs2g_run_opts* o, double* v_out, int* status, int* iters, double* residual);
+/* Validate a converged base V (the reference's init_from_n_powerflow path):
+ * returns the residual of V and stores it as the base start. */
+int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual);
+
+/* Run every row.  Results stay on the device until read. */
+int gs2g_run(gs2g_session* s, const gs2g_run_opts* o);
+int gs2g_n_rows(const gs2g_session* s);
+int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters);
+/* Device pointers of the last run's results (valid until the next run or destroy). */
+int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
+int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
+/* Synchronise the session stream. */
+int gs2g_sync(gs2g_session* s);
+
+/* acpf_nr_gpu: one solve from Vinit, V written back into `v_inout`.
+ * Returns the status through *converged (1/0), *iters and *residual. */
+int gs2g_acpf_nr(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices,
+                 const double* ybus_values, double* v_inout, const double* sbus,
+                 const int* pv, int n_pv, const int* pq, int n_pq, int max_iter, double tol,
+                 int precision, int* converged, int* iters, double* residual, double* kernel_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GS2G_H */
