@@ -1,0 +1,246 @@
+"""Batched sweeps on the GPU: ``ContingencyAnalysisGPU``, ``InjectionSweepGPU``
+and ``ScenarioSweepGPU`` (array-tuple mode).
+
+Facade signatures follow the reference:
+``src/gpusim2grid/contingency_analysis/gpu_facade.py:347-782`` (constructor,
+``set_branch_data`` :569, ``add_contingencies_by_branch_id`` :595, ``compute`` :762,
+``last_residuals`` :1025), ``src/gpusim2grid/injection_sweep/gpu_facade.py:220-546``
+(``set_injections`` :378, ``compute`` :515) and
+``src/gpusim2grid/scenario_sweep/gpu_facade.py:215-838`` (``set_topology`` :690,
+``get_disconnected`` :838).  Scheduling names and row statuses:
+``src/gpusim2grid/contingency_analysis/_scheduling.py:61-170``.
+
+Every row runs on the persistent kernel: a row is one CTA's whole Newton loop,
+and it leaves the GPU as soon as it is done (``scheduling='continuous'``) or
+after exactly ``nb_iter`` steps (``scheduling='chunked'``, the reference's
+default).  Rows start from the converged base case as the reference's batch
+sources do (``start='base'``), or from ``Vinit`` (``start='flat'``), or from
+per-row voltages (``set_start_voltages``).
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from ._common import (BatchTimings, RowStatus, default_tol, grid_arrays, make_session, resolve_precision,
+                      resolve_scheduling)
+from ._native import lib
+
+__all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU"]
+
+_START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS}
+
+
+def _ids_csr(rows):
+    ptr = np.zeros(len(rows) + 1, dtype=np.int32)
+    flat = []
+    for r, ids in enumerate(rows):
+        ids = [int(v) for v in (ids if ids is not None else [])]
+        flat.extend(ids)
+        ptr[r + 1] = len(flat)
+    return ptr, np.asarray(flat, dtype=np.int32)
+
+
+class _BatchSweep:
+    def __init__(self, grid, *, init_from_n_powerflow=True, precision="fp64", nb_iter=4, max_iter_base=10,
+                 tol_base=1e-8, device=None, scheduling=None, nb_iter_per_round=1, tol=None, start="base",
+                 **_ignored):
+        d = grid_arrays(grid)
+        self._d = d
+        self._prec = resolve_precision(precision)
+        self.nb_iter = int(nb_iter)
+        self.scheduling = resolve_scheduling("chunked" if scheduling is None else scheduling)
+        self.nb_iter_per_round = int(nb_iter_per_round)
+        if self.nb_iter_per_round < 1:
+            raise ValueError("nb_iter_per_round must be >= 1")
+        self.tol = default_tol() if tol is None else float(tol)
+        self._s = make_session(d, device)
+        if init_from_n_powerflow:
+            res = self._s.set_base_v(d["Vinit"])
+            if not (res < tol_base):
+                raise RuntimeError(f"init_from_n_powerflow: the base-case residual {res:.3e} is not below "
+                                   f"tol_base = {tol_base:.1e}")
+            self._base_iters = 0
+        else:
+            V, st, it, res = self._s.solve_base(int(max_iter_base), float(tol_base), self._prec, 0.0)
+            if st != RowStatus.CONVERGED:
+                raise RuntimeError(f"the base case did not converge (status {RowStatus(st).name}, "
+                                   f"residual {res:.3e})")
+            self._base_iters = it
+        self.start = start
+        self._n_branches = None
+        self._ran = False
+        self._timings = BatchTimings()
+
+    # -------------------------------------------------------------- options
+    @property
+    def start(self):
+        """'base' (the converged base case, default), 'flat' (``Vinit``) or
+        'rows' (``set_start_voltages``)."""
+        return self._start
+
+    @start.setter
+    def start(self, value):
+        if value not in _START:
+            raise ValueError(f"Unknown start {value!r}. Choose from: {list(_START)}")
+        self._start = value
+
+    # ----------------------------------------------------------------- data
+    def set_branch_data(self, branch_from, branch_to, yff_eff, yft_eff, ytf_eff, ytt_eff, bus_vn_kv=None,
+                        sn_mva=None):
+        """π-model branch admittances (explicit-array mode); needed to trip
+        branches.  ``bus_vn_kv`` / ``sn_mva`` are accepted for signature
+        parity (they only serve branch-flow post-processing)."""
+        c = lambda a: np.ascontiguousarray(a, dtype=np.complex128)
+        self._s.set_branch_data(np.ascontiguousarray(branch_from, dtype=np.int32),
+                                np.ascontiguousarray(branch_to, dtype=np.int32),
+                                c(yff_eff), c(yft_eff), c(ytf_eff), c(ytt_eff))
+        self._n_branches = len(branch_from)
+
+    def set_start_voltages(self, V0):
+        """Per-row start voltages (n_rows, n_bus) complex; switches ``start`` to 'rows'."""
+        V0 = np.ascontiguousarray(V0, dtype=np.complex128)
+        self._s.set_start_rows(V0)
+        self.start = "rows"
+
+    # ------------------------------------------------------------------ run
+    def _run(self, batch_size):
+        fixed = self.scheduling == "chunked"
+        n_ctas = max(int(batch_size), 0)
+        t0 = time.perf_counter()
+        self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False)
+        tm = self._s.timings()
+        self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
+                                     t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
+                                     t_kernel_ms=tm["kernel_ms"], t_total_ms=(time.perf_counter() - t0) * 1e3)
+        self._ran = True
+        self._host = None
+
+    def compute(self, batch_size=512):
+        """Solve every row.  Returns a DLPack capsule (n_rows, n_bus) complex128
+        aliasing device memory, valid until the next ``compute()``.
+        ``batch_size`` caps the rows in flight (one per CTA of the persistent
+        kernel)."""
+        self._run(batch_size)
+        return self._s.dlpack("v")
+
+    def _results(self):
+        if not self._ran:
+            raise RuntimeError("Call compute() first.")
+        if self._host is None:
+            self._host = self._s.results()
+        return self._host
+
+    def last_residuals(self):
+        """||F||inf per row of the last ``compute()``."""
+        return self._results()[1].copy()
+
+    def get_row_status(self):
+        return self._results()[2].copy()
+
+    def get_row_iterations(self):
+        return self._results()[3].copy()
+
+    @property
+    def V_results(self):
+        """(n_rows, n_bus) complex voltages of the last ``compute()`` (host copy)."""
+        return self._results()[0]
+
+    def converged(self, tol=None):
+        res = self.last_residuals()
+        return res < (self.tol if tol is None else tol)
+
+    def converged_n(self, tol=None):
+        return True
+
+    def results_dlpack(self, what="v"):
+        """DLPack capsule of 'v', 'residuals', 'status' or 'iters'."""
+        return self._s.dlpack(what)
+
+    @property
+    def timings(self):
+        return self._timings
+
+    @property
+    def n_bus(self):
+        return self._d["n_bus"]
+
+    @property
+    def n_branches(self):
+        return self._n_branches
+
+    @property
+    def session(self):
+        return self._s
+
+
+class ContingencyAnalysisGPU(_BatchSweep):
+    """Batch N-k contingency analysis: every row trips a set of branches from
+    the base case.  Rows whose trips island the grid are NOT_SIMULATED with NaN
+    voltages (``contingency_analysis_helper.cpp:634-651``)."""
+
+    def __init__(self, grid, **kw):
+        super().__init__(grid, **kw)
+        self._ctg = []
+
+    def add_contingencies_by_branch_id(self, branch_ids_per_ctg):
+        """One inner list per contingency (branch indices; a branch named twice
+        is tripped once).  Replaces previously given contingencies."""
+        if self._n_branches is None:
+            raise RuntimeError("set_branch_data() must be called before add_contingencies_by_branch_id()")
+        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_ctg]
+        ptr, ids = _ids_csr(rows)
+        self._s.set_contingencies(ptr, ids)
+        self._ctg = rows
+
+    def get_contingencies(self):
+        return [list(r) for r in self._ctg]
+
+    @property
+    def n_contingencies(self):
+        return len(self._ctg)
+
+
+class InjectionSweepGPU(_BatchSweep):
+    """One row per injection scenario on a fixed topology."""
+
+    def __init__(self, grid, **kw):
+        super().__init__(grid, **kw)
+        self._n_scen = 0
+
+    def set_injections(self, p_mw, q_mvar, sn_mva):
+        """Bus injections in MW / MVAr, (n_scenarios, n_bus); Sbus = (p + jq) / sn_mva
+        (``injection_sweep_session.cu:239-245``)."""
+        p = np.ascontiguousarray(p_mw, dtype=np.float64)
+        q = np.ascontiguousarray(q_mvar, dtype=np.float64)
+        if p.ndim != 2 or p.shape != q.shape or p.shape[1] != self.n_bus:
+            raise ValueError("p_mw and q_mvar must both be (n_scenarios, n_bus)")
+        self._s.set_injections(p, q, float(sn_mva))
+        self._n_scen = p.shape[0]
+
+    @property
+    def n_scenarios(self):
+        return self._n_scen
+
+
+class ScenarioSweepGPU(InjectionSweepGPU):
+    """Injections and topology per row: row r uses injection scenario r and
+    trips the branches of ``set_topology()[r]``."""
+
+    def __init__(self, grid, **kw):
+        super().__init__(grid, **kw)
+        self._topo = None
+
+    def set_topology(self, branch_ids_per_scenario):
+        if self._n_branches is None:
+            raise RuntimeError("set_branch_data() must be called before set_topology()")
+        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_scenario]
+        ptr, ids = _ids_csr(rows)
+        self._s.set_contingencies(ptr, ids)
+        self._topo = rows
+
+    def get_disconnected(self):
+        """(n_rows,) bool: rows whose topology islands the grid (never solved)."""
+        return self.get_row_status() == RowStatus.NOT_SIMULATED

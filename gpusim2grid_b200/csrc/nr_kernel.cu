@@ -148,16 +148,28 @@ __device__ void dense_lu(T* __restrict__ A, int n, int ld, T* sD, T* sA, T* sB, 
     }
     __syncthreads();
     if (warp == 0) {
-      for (int j = 0; j < kb; ++j) {
-        T piv = clamp_pivot(sD[j * (NB + 1) + j], pfloor);
-        __syncwarp();
-        if (lane == j) sD[j * (NB + 1) + j] = piv;
-        if (lane > j && lane < kb) {
-          const T l = sD[lane * (NB + 1) + j] / piv;
-          sD[lane * (NB + 1) + j] = l;
-          for (int c = j + 1; c < kb; ++c) sD[lane * (NB + 1) + c] -= l * sD[j * (NB + 1) + c];
+      // lane r holds row r of the diagonal block in registers; the pivot row
+      // is broadcast by shuffles (no shared-memory round trips per step)
+      T x[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) x[c] = (lane < kb && c < kb) ? sD[lane * (NB + 1) + c] : T(lane == c ? 1 : 0);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        T piv = clamp_pivot(__shfl_sync(0xffffffffu, x[j], j), pfloor);
+        if (lane == j) x[j] = piv;
+        const T l = x[j] / piv;
+        const bool below = lane > j;
+        if (below) x[j] = l;
+#pragma unroll
+        for (int c = j + 1; c < NB; ++c) {
+          const T u = __shfl_sync(0xffffffffu, x[c], j);
+          if (below) x[c] = fma(-l, u, x[c]);
         }
-        __syncwarp();
+      }
+      if (lane < kb) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+          if (c < kb) sD[lane * (NB + 1) + c] = x[c];
       }
     }
     __syncthreads();
@@ -221,10 +233,16 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int cb = min(32, n - c0);
     if (warp == 0) {
+      // lane r loads row r of the diagonal block up front (independent loads)
+      T arow[32];
+      const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c < lane) ? rp[c] : T(0);
       T v = lane < cb ? y[c0 + lane] : T(0);
-      for (int c = 0; c < cb; ++c) {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
         const T yc = __shfl_sync(0xffffffffu, v, c);
-        if (lane > c && lane < cb) v -= A[(int64_t)(c0 + lane) * ld + c0 + c] * yc;
+        v = fma(-arow[c], yc, v);
       }
       if (lane < cb) {
         y[c0 + lane] = v;
@@ -245,15 +263,17 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
     const int c0 = bi * 32;
     const int cb = min(32, n - c0);
     if (warp == 0) {
+      T arow[32];
+      const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c >= lane && c < cb) ? rp[c] : T(lane == c ? 1 : 0);
       T v = lane < cb ? y[c0 + lane] : T(0);
-      for (int c = cb - 1; c >= 0; --c) {
-        T xc = 0;
-        if (lane == c) {
-          v = v / A[(int64_t)(c0 + c) * ld + c0 + c];
-          xc = v;
-        }
+#pragma unroll
+      for (int c = 31; c >= 0; --c) {
+        T xc = v / arow[c];  // meaningful on lane c only
         xc = __shfl_sync(0xffffffffu, xc, c);
-        if (lane < c) v -= A[(int64_t)(c0 + lane) * ld + c0 + c] * xc;
+        if (lane == c) v = xc;
+        else if (lane < c) v = fma(-arow[c], xc, v);
       }
       if (lane < cb) {
         y[c0 + lane] = v;
@@ -270,6 +290,35 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
     __syncthreads();
   }
 }
+
+// Per-phase SM cycles, recorded by thread 0 of each CTA at the block-wide
+// barriers that separate the phases, summed over CTAs at exit.
+struct PhaseProf {
+  unsigned long long acc[N_PHASES];
+  long long t;
+  bool on;
+  __device__ void init(bool enabled) {
+    on = enabled;
+#pragma unroll
+    for (int q = 0; q < N_PHASES; ++q) acc[q] = 0;
+    t = clock64();
+  }
+  __device__ __forceinline__ void start() {
+    if (on) t = clock64();
+  }
+  __device__ __forceinline__ void mark(int ph) {
+    if (on) {
+      const long long now = clock64();
+      acc[ph] += (unsigned long long)(now - t);
+      t = now;
+    }
+  }
+  __device__ void flush(unsigned long long* out) {
+    if (!on) return;
+#pragma unroll
+    for (int q = 0; q < N_PHASES; ++q) atomicAdd(out + q, acc[q]);
+  }
+};
 
 __host__ __device__ __forceinline__ int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
 
@@ -292,7 +341,7 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepArgs a) {
+__global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const SweepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_row;
   __shared__ int s_ne;
@@ -315,12 +364,17 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
   T* y = reinterpret_cast<T*>(ws + L.y);
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const int n = P.n_bus;
+  PhaseProf prof;
+  prof.init(a.phase_cycles != nullptr && tid == 0);
 
   for (;;) {
     if (tid == 0) s_row = atomicAdd(a.queue, 1);
     __syncthreads();
     const int row = s_row;
-    if (row >= a.n_rows) return;
+    if (row >= a.n_rows) {
+      prof.flush(a.phase_cycles);
+      return;
+    }
     double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
 
     if (a.row_skip != nullptr && a.row_skip[row]) {
@@ -350,6 +404,7 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
     for (int i = tid; i < n; i += BS) V[i] = v0[i];
     __syncthreads();
     const RowEdits ed{s_ne, s_ek, s_ev};
+    prof.start();
 
     int it = 0, status = ROW_MAX_ITER;
     double nrm = NAN;
@@ -383,6 +438,7 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
         }
       }
       nrm = block_nanmax(lmax, s_red);
+      prof.mark(PH_MISMATCH);
       const bool finite = isfinite(nrm);
       if (a.fixed_iters) {
         if (it >= a.max_iter || !finite) {
@@ -430,10 +486,28 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
       }
       __syncthreads();
 
+      prof.mark(PH_FILL);
       // ---- sparse head LU, level by level --------------------------------
       for (int lv = 0; lv < P.n_levels; ++lv) {
-        const int t0 = P.lev_ptr[lv], t1 = P.lev_ptr[lv + 1];
-        for (int t = t0 + tid; t < t1; t += BS) {
+        const int t0 = P.lev_ptr[lv], tb = P.lev_big[lv], t1 = P.lev_ptr[lv + 1];
+        {
+          // long tasks: one warp each, products split over the lanes
+          const int lane = tid & 31, warp = tid >> 5;
+          for (int t = t0 + warp; t < tb; t += NWARP) {
+            const int out = P.task_out[t];
+            const int q1 = P.task_pend[t];
+            T part = T(0);
+            for (int q = P.task_pbeg[t] + lane; q < q1; q += 32) part += HV[P.pair_l[q]] * HV[P.pair_u[q]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (lane == 0) {
+              T acc = (P.task_has_a[t] ? HV[out] : T(0)) - part;
+              if (out < P.p) acc = clamp_pivot(acc, a.pivot_floor);
+              HV[out] = acc;
+            }
+          }
+        }
+        for (int t = tb + tid; t < t1; t += BS) {
           const int out = P.task_out[t];
           T acc = P.task_has_a[t] ? HV[out] : T(0);
           const int q1 = P.task_pend[t];
@@ -449,6 +523,7 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
         __syncthreads();
       }
 
+      prof.mark(PH_HEAD);
       // ---- Schur update of the dense tail: warp per tail row ---------------
       {
         const int lane = tid & 31, warp = tid >> 5;
@@ -471,9 +546,11 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
       }
       __syncthreads();
 
+      prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
       if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, sD, sA, sB, a.pivot_floor);
 
+      prof.mark(PH_DENSE);
       // ---- solves -----------------------------------------------------------
       for (int i = tid; i < P.dim; i += BS) y[i] = (T)F[i];
       __syncthreads();
@@ -504,6 +581,7 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
         __syncthreads();
       }
 
+      prof.mark(PH_SOLVE);
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
         const int fp = P.fP[i], fq = P.fQ[i];
@@ -518,6 +596,7 @@ __global__ void __launch_bounds__(BS) sweep_kernel(const DevPlan P, const SweepA
         V[i] = make_double2(vm * cs, vm * sn);
       }
       __syncthreads();
+      prof.mark(PH_UPDATE);
       ++it;
     }
 

@@ -21,6 +21,7 @@ struct DevPlan {
   const int* fP;       // [n_bus]
   const int* fQ;       // [n_bus]
   const int* lev_ptr;  // [n_levels + 1] into tasks
+  const int* lev_big;  // [n_levels]: tasks [lev_ptr[l], lev_big[l]) are long (warp per task)
   const int* task_out;
   const int* task_diag;
   const int* task_pbeg;
@@ -72,6 +73,21 @@ struct SweepArgs {
   char* workspace;        // per-CTA scratch
   int64_t ws_stride;      // bytes per CTA
   double pivot_floor;     // static-pivot floor (|u_kk| below it is raised to it)
+  // optional: per-phase SM cycles summed over CTAs (nullptr: not recorded)
+  unsigned long long* phase_cycles;  // [N_PHASES]
+};
+
+// Phases of one Newton iteration, as the reference's per-phase timings
+// (AcPfTimings, src/_cpp/timing_utils.hpp:131-215) split them.
+enum Phase : int {
+  PH_MISMATCH = 0,  // SpMV + mismatch + norm
+  PH_FILL = 1,      // zero the tail + Jacobian fill
+  PH_HEAD = 2,      // sparse head LU
+  PH_SCHUR = 3,     // Schur update of the tail
+  PH_DENSE = 4,     // dense tail LU
+  PH_SOLVE = 5,     // triangular solves
+  PH_UPDATE = 6,    // voltage update
+  N_PHASES = 7
 };
 
 // Per-CTA workspace bytes for precision `prec` (0: fp64 LU, 1: fp32 LU).

@@ -464,6 +464,31 @@ Plan build_plan(int n_bus, const int* ybus_indptr, const int* ybus_indices,
         end_task();
       }
     }
+    // long tasks first (a warp each on the device), longest first
+    {
+      const int t0 = P.lev_ptr.back(), t1 = (int)P.task_out.size();
+      std::vector<int> idx(t1 - t0);
+      std::iota(idx.begin(), idx.end(), t0);
+      auto len = [&](int t) { return P.task_pend[t] - P.task_pbeg[t]; };
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        const bool ba = len(a) >= Plan::kBigTask, bb = len(b) >= Plan::kBigTask;
+        if (ba != bb) return ba;
+        return ba ? len(a) > len(b) : false;
+      });
+      auto permute = [&](auto& v) {
+        auto tmp = v;
+        for (int q = 0; q < t1 - t0; ++q) v[t0 + q] = tmp[idx[q]];
+      };
+      permute(P.task_out);
+      permute(P.task_diag);
+      permute(P.task_pbeg);
+      permute(P.task_pend);
+      permute(P.task_has_a);
+      int nbig = 0;
+      for (int t = t0; t < t1; ++t)
+        if (len(t) >= Plan::kBigTask) ++nbig;
+      P.lev_big.push_back(t0 + nbig);
+    }
     P.lev_ptr.push_back((int)P.task_out.size());
   }
   P.head_madds = (int64_t)P.pair_l.size();

@@ -62,6 +62,10 @@ struct Plan {
   // head pivot levels: tasks of level l are [lev_ptr[l], lev_ptr[l+1])
   int n_levels = 0;
   std::vector<int> lev_ptr;
+  // within level l, tasks [lev_ptr[l], lev_big[l]) have at least kBigTask
+  // products (one warp each on the device), the rest one thread each
+  std::vector<int> lev_big;
+  static constexpr int kBigTask = 24;
   // head pivots by level (for the level-scheduled triangular solves)
   std::vector<int> lev_piv_ptr, lev_piv;
   // head tasks: out position in HV; has_a flag; diag position for L entries

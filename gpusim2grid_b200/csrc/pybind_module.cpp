@@ -17,6 +17,66 @@ namespace py = pybind11;
 
 namespace {
 
+// ---- DLPack export -----------------------------------------------------
+// The DLPack ABI (dlpack.h v0.8 layout), written out here: device buffers of
+// the session are exported zero-copy, as the reference's v_results_dlpack
+// (src/_cpp/dlpack_export.hpp:20-45).  The capsule aliases live device memory
+// and stays valid until the next run on the same session.
+struct DLDevice_ {
+  int32_t device_type;
+  int32_t device_id;
+};
+struct DLDataType_ {
+  uint8_t code;
+  uint8_t bits;
+  uint16_t lanes;
+};
+struct DLTensor_ {
+  void* data;
+  DLDevice_ device;
+  int32_t ndim;
+  DLDataType_ dtype;
+  int64_t* shape;
+  int64_t* strides;
+  uint64_t byte_offset;
+};
+struct DLManagedTensor_ {
+  DLTensor_ dl_tensor;
+  void* manager_ctx;
+  void (*deleter)(DLManagedTensor_*);
+};
+struct DLCtx {
+  int64_t shape[2];
+};
+enum : int32_t { kDLCUDA_ = 2 };
+enum : uint8_t { kDLInt_ = 0, kDLFloat_ = 2, kDLComplex_ = 5 };
+
+void dl_deleter(DLManagedTensor_* t) {
+  delete static_cast<DLCtx*>(t->manager_ctx);
+  delete t;
+}
+
+py::capsule make_dlpack(void* ptr, int device, int ndim, int64_t d0, int64_t d1, uint8_t code, uint8_t bits) {
+  auto* ctx = new DLCtx{{d0, d1}};
+  auto* t = new DLManagedTensor_{};
+  t->dl_tensor.data = ptr;
+  t->dl_tensor.device = {kDLCUDA_, device};
+  t->dl_tensor.ndim = ndim;
+  t->dl_tensor.dtype = {code, bits, 1};
+  t->dl_tensor.shape = ctx->shape;
+  t->dl_tensor.strides = nullptr;
+  t->dl_tensor.byte_offset = 0;
+  t->manager_ctx = ctx;
+  t->deleter = dl_deleter;
+  return py::capsule(t, "dltensor", [](PyObject* cap) {
+    // a consumed capsule is renamed "used_dltensor" and owned by its consumer
+    if (PyCapsule_IsValid(cap, "dltensor")) {
+      auto* m = static_cast<DLManagedTensor_*>(PyCapsule_GetPointer(cap, "dltensor"));
+      if (m && m->deleter) m->deleter(m);
+    }
+  });
+}
+
 using cplx = std::complex<double>;
 using IArr = py::array_t<int, py::array::c_style | py::array::forcecast>;
 using DArr = py::array_t<double, py::array::c_style | py::array::forcecast>;
@@ -30,7 +90,7 @@ void check(int rc) {
 }
 
 gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
-                        int n_ctas) {
+                        int n_ctas, bool profile = false) {
   gs2g_run_opts o{};
   o.max_iter = max_iter;
   o.tol = tol;
@@ -39,6 +99,7 @@ gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precisio
   o.start = start;
   o.pivot_floor = pivot_floor;
   o.n_ctas = n_ctas;
+  o.profile_phases = profile ? 1 : 0;
   return o;
 }
 
@@ -168,8 +229,9 @@ class Session {
     return res;
   }
 
-  void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas) {
-    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas);
+  void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas,
+           bool profile) {
+    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile);
     int rc;
     {
       py::gil_scoped_release nogil;
@@ -205,6 +267,22 @@ class Session {
     return py::make_tuple((uintptr_t)v, (uintptr_t)r, (uintptr_t)s, (uintptr_t)i);
   }
 
+  // DLPack capsules of the last run's device results: "v" (n_rows, n_bus)
+  // complex128, "residuals" (n_rows,) float64, "status"/"iters" (n_rows,) int32.
+  py::capsule dlpack(const std::string& what) const {
+    double *v = nullptr, *r = nullptr;
+    int *s = nullptr, *i = nullptr;
+    check(gs2g_get_device_results(h(), &v, &r, &s, &i));
+    const int nr = gs2g_n_rows(h());
+    int dev = 0;
+    check(gs2g_get_device(h(), &dev));
+    if (what == "v") return make_dlpack(v, dev, 2, nr, n_bus_, kDLComplex_, 128);
+    if (what == "residuals") return make_dlpack(r, dev, 1, nr, 0, kDLFloat_, 64);
+    if (what == "status") return make_dlpack(s, dev, 1, nr, 0, kDLInt_, 32);
+    if (what == "iters") return make_dlpack(i, dev, 1, nr, 0, kDLInt_, 32);
+    throw py::value_error("unknown result '" + what + "'");
+  }
+
   py::dict timings() const {
     gs2g_timings t{};
     check(gs2g_get_timings(h(), &t));
@@ -214,6 +292,13 @@ class Session {
     d["kernel_ms"] = t.kernel_ms;
     d["total_ms"] = t.total_ms;
     d["total_iters"] = t.total_iters;
+    py::list pc, ps;
+    for (int q = 0; q < GS2G_N_PHASES; ++q) {
+      pc.append(t.phase_cycles[q]);
+      ps.append(t.phase_share[q]);
+    }
+    d["phase_cycles"] = pc;
+    d["phase_share"] = ps;
     return d;
   }
 
@@ -243,9 +328,41 @@ py::tuple acpf_nr(int device, int n_bus, IArr indptr, IArr indices, CArr data, C
   return py::make_tuple(out, conv != 0, it, res, ms);
 }
 
+py::dict plan_info(int n_bus, IArr indptr, IArr indices, IArr pv, IArr pq, int tail_policy) {
+  if (indptr.size() != n_bus + 1) throw py::value_error("Ybus indptr must have n_bus + 1 entries");
+  gs2g_grid_info g{};
+  int rc;
+  {
+    py::gil_scoped_release nogil;
+    rc = gs2g_plan_info(n_bus, indptr.data(), indices.data(), pv.data(), (int)pv.size(), pq.data(), (int)pq.size(),
+                        tail_policy, &g);
+  }
+  check(rc);
+  py::dict d;
+  d["n_bus"] = g.n_bus;
+  d["nnz_y"] = g.nnz_y;
+  d["n_pvpq"] = g.n_pvpq;
+  d["n_pq"] = g.n_pq;
+  d["dim_j"] = g.dim_j;
+  d["nnz_j"] = g.nnz_j;
+  d["nnz_lu"] = g.nnz_lu;
+  d["head_dim"] = g.head_dim;
+  d["tail_dim"] = g.tail_dim;
+  d["tail_dim_exact"] = g.tail_dim_exact;
+  d["n_levels"] = g.n_levels;
+  d["n_supernodes"] = g.n_supernodes;
+  d["head_madds"] = g.head_madds;
+  d["schur_madds"] = g.schur_madds;
+  d["dense_madds"] = g.dense_madds;
+  d["plan_ms"] = g.plan_ms;
+  return d;
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_gs2g, m) {
+  m.def("plan_info", &plan_info, py::arg("n_bus"), py::arg("indptr"), py::arg("indices"), py::arg("pv"),
+        py::arg("pq"), py::arg("tail_policy") = 1);
   m.doc() = "B200-native batched Newton-Raphson AC power flow (binding of include/gs2g.h)";
   m.attr("PREC_FP64") = GS2G_PREC_FP64;
   m.attr("PREC_MIXED") = GS2G_PREC_MIXED;
@@ -272,10 +389,12 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("set_vinit", &Session::set_vinit)
       .def("solve_base", &Session::solve_base)
       .def("set_base_v", &Session::set_base_v)
-      .def("run", &Session::run)
+      .def("run", &Session::run, py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"), py::arg("precision"),
+           py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)
       .def("device_results", &Session::device_results)
+      .def("dlpack", &Session::dlpack)
       .def("timings", &Session::timings)
       .def("sync", &Session::sync);
 }

@@ -100,7 +100,7 @@ struct gs2g_session {
   bool rows_have_sbus = false, rows_have_edits = false, rows_have_skip = false;
   DevBuf d_sbus_rows, d_edit_ptr, d_edit_k, d_edit_val, d_row_skip;
   DevBuf d_v_out, d_res, d_status, d_iters;
-  DevBuf d_ws, d_queue;
+  DevBuf d_ws, d_queue, d_phase;
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
 
@@ -138,6 +138,7 @@ void upload_plan(gs2g_session* s) {
   D.fP = upload_vec(s, P.fP);
   D.fQ = upload_vec(s, P.fQ);
   D.lev_ptr = upload_vec(s, P.lev_ptr);
+  D.lev_big = upload_vec(s, P.lev_big);
   D.task_out = upload_vec(s, P.task_out);
   D.task_diag = upload_vec(s, P.task_diag);
   D.task_pbeg = upload_vec(s, P.task_pbeg);
@@ -308,6 +309,12 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
   a.pivot_floor = o.pivot_floor;
+  a.phase_cycles = nullptr;
+  if (o.profile_phases) {
+    s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
+    ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
+    a.phase_cycles = s->d_phase.as<unsigned long long>();
+  }
   ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
@@ -315,6 +322,17 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   ck(cudaStreamSynchronize(s->stream), "sweep");
   float ms = 0;
   ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
+  for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
+  if (o.profile_phases) {
+    unsigned long long c[gs2g::N_PHASES];
+    ck(cudaMemcpy(c, s->d_phase.p, sizeof(c), cudaMemcpyDeviceToHost), "read phases");
+    double tot = 0;
+    for (int q = 0; q < gs2g::N_PHASES; ++q) tot += (double)c[q];
+    for (int q = 0; q < gs2g::N_PHASES; ++q) {
+      s->tm.phase_cycles[q] = (double)c[q];
+      s->tm.phase_share[q] = tot > 0 ? c[q] / tot : 0;
+    }
+  }
   return ms;
 }
 
@@ -436,6 +454,43 @@ int gs2g_session_destroy(gs2g_session* s) {
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
   }
+  GS2G_CATCH
+}
+
+int gs2g_get_device(const gs2g_session* s, int* device) {
+  GS2G_TRY
+  if (!s || !device) throw std::invalid_argument("NULL argument");
+  *device = s->device;
+  GS2G_CATCH
+}
+
+int gs2g_plan_info(int n_bus, const int* ybus_indptr, const int* ybus_indices, const int* pv, int n_pv, const int* pq,
+                   int n_pq, int tail_policy, gs2g_grid_info* out) {
+  GS2G_TRY
+  if (n_bus <= 0 || !ybus_indptr || !ybus_indices || !out) throw std::invalid_argument("plan_info: bad arguments");
+  std::vector<int> ip, ix;
+  std::vector<double> vals;
+  std::vector<double> zeros(2 * (size_t)std::max(ybus_indptr[n_bus], 0), 0.0);
+  canonical_csr(n_bus, ybus_indptr, ybus_indices, zeros.data(), ip, ix, vals);
+  gs2g::TailOptions topt;
+  topt.policy = tail_policy;
+  const gs2g::Plan P = gs2g::build_plan(n_bus, ip.data(), ix.data(), pv, n_pv, pq, n_pq, topt);
+  out->n_bus = P.n_bus;
+  out->nnz_y = P.nnz_y;
+  out->n_pvpq = P.n_pvpq;
+  out->n_pq = P.n_pq;
+  out->dim_j = P.dim;
+  out->nnz_j = P.nnz_j;
+  out->nnz_lu = P.nnz_lu;
+  out->head_dim = P.p;
+  out->tail_dim = P.nt;
+  out->tail_dim_exact = P.n_tail_exact;
+  out->n_levels = P.n_levels;
+  out->n_supernodes = P.n_sn;
+  out->head_madds = P.head_madds;
+  out->schur_madds = P.schur_madds;
+  out->dense_madds = P.dense_madds;
+  out->plan_ms = P.build_ms;
   GS2G_CATCH
 }
 

@@ -77,7 +77,10 @@ typedef struct gs2g_run_opts {
   int start;          /* GS2G_START_* */
   double pivot_floor; /* static-pivot floor, 0 disables */
   int n_ctas;         /* persistent CTAs, <= 0 for one full wave */
+  int profile_phases; /* 1: record per-phase SM cycles (gs2g_timings.phase_*) */
 } gs2g_run_opts;
+
+#define GS2G_N_PHASES 7 /* mismatch, fill, head LU, Schur, dense LU, solves, update */
 
 typedef struct gs2g_timings {
   double plan_ms;      /* symbolic analysis, once per session */
@@ -85,6 +88,10 @@ typedef struct gs2g_timings {
   double kernel_ms;    /* last sweep, CUDA events on the session stream */
   double total_ms;     /* last gs2g_run, wall */
   int64_t total_iters; /* sum of Newton steps over the rows of the last run */
+  /* with profile_phases: SM cycles per phase summed over all CTAs, and each
+   * phase's share of their total */
+  double phase_cycles[GS2G_N_PHASES];
+  double phase_share[GS2G_N_PHASES];
 } gs2g_timings;
 
 const char* gs2g_last_error(void);
@@ -99,6 +106,13 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
                         gs2g_session** out);
 int gs2g_session_destroy(gs2g_session* s);
 int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
+int gs2g_get_device(const gs2g_session* s, int* device);
+
+/* Symbolic analysis only (host, no GPU needed): the statistics a session on
+ * this grid would have.  Counterpart of the reference's once-only ANALYSIS
+ * (src/_cpp/acpf_nr.cu:1466-1509, src/_cpp/own_lu/lu_plan.cpp:88-287). */
+int gs2g_plan_info(int n_bus, const int* ybus_indptr, const int* ybus_indices, const int* pv, int n_pv,
+                   const int* pq, int n_pq, int tail_policy, gs2g_grid_info* out);
 
 /* π-model branch admittances, needed to trip branches. */
 int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const int* to,

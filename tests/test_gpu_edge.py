@@ -1,0 +1,110 @@
+"""GPU edge cases: islanding, NaN rows, invariances, determinism, full-size
+properties (restated from the reference's test families)."""
+
+import numpy as np
+import pytest
+
+from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, RowStatus, ScenarioSweepGPU
+from gpusim2grid_b200.synthetic import injection_scenarios, n1_branches
+from oracle import nr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _ca(g, **kw):
+    kw.setdefault("init_from_n_powerflow", False)
+    kw.setdefault("nb_iter", 10)
+    kw.setdefault("scheduling", "continuous")
+    kw.setdefault("start", "flat")
+    ca = ContingencyAnalysisGPU(g.as_tuple(), **kw)
+    ca.set_branch_data(*g.branch_data())
+    return ca
+
+
+def test_islanded_row_is_nan_and_neighbours_unaffected(g118):
+    rows = n1_branches(g118)
+    bridge = int(np.setdiff1d(np.arange(g118.n_branch), rows)[0])
+    ca = _ca(g118)
+    ca.add_contingencies_by_branch_id([[int(rows[0])], [bridge], [int(rows[1])]])
+    ca.compute()
+    st = ca.get_row_status()
+    assert list(st) == [RowStatus.CONVERGED, RowStatus.NOT_SIMULATED, RowStatus.CONVERGED]
+    assert np.all(np.isnan(ca.V_results[1])) and np.isnan(ca.last_residuals()[1])
+    ca2 = _ca(g118)
+    ca2.add_contingencies_by_branch_id([[int(rows[0])], [int(rows[1])]])
+    ca2.compute()
+    np.testing.assert_array_equal(ca2.V_results, ca.V_results[[0, 2]])
+
+
+def test_nan_scenario_diverges_alone(g118):
+    p, q = injection_scenarios(g118, 4, seed=3)
+    p[2, g118.pq[0]] = np.nan
+    sw = InjectionSweepGPU(g118.as_tuple(), init_from_n_powerflow=False, nb_iter=10, scheduling="continuous",
+                           start="flat")
+    sw.set_injections(p, q, g118.sn_mva)
+    sw.compute()
+    st = sw.get_row_status()
+    assert st[2] == RowStatus.DIVERGED and np.isnan(sw.last_residuals()[2])
+    assert np.all(st[[0, 1, 3]] == RowStatus.CONVERGED)
+
+
+def test_batch_size_and_order_invariance(g118):
+    rows = [[int(b)] for b in n1_branches(g118)[:40]]
+    ca = _ca(g118)
+    ca.add_contingencies_by_branch_id(rows)
+    ca.compute(batch_size=512)
+    V_full = ca.V_results.copy()
+    ca.compute(batch_size=3)
+    np.testing.assert_array_equal(ca.V_results, V_full)  # bitwise: a row's arithmetic is independent of its CTA
+    perm = np.random.default_rng(1).permutation(len(rows))
+    ca.add_contingencies_by_branch_id([rows[i] for i in perm])
+    ca.compute()
+    np.testing.assert_array_equal(ca.V_results, V_full[perm])
+
+
+def test_duplicate_branch_ids_trip_once(g118):
+    b = int(n1_branches(g118)[3])
+    ca = _ca(g118)
+    ca.add_contingencies_by_branch_id([[b], [b, b]])
+    ca.compute()
+    np.testing.assert_array_equal(ca.V_results[0], ca.V_results[1])
+
+
+def test_unit_scale_injection_reproduces_base(g118):
+    """Injection rows equal to the base injections reproduce the base case
+    (reference test_injection_batch.py:169)."""
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vb, *_ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    P = np.tile(S.real * g118.sn_mva, (3, 1))
+    Q = np.tile(S.imag * g118.sn_mva, (3, 1))
+    sw = InjectionSweepGPU(g118.as_tuple(), init_from_n_powerflow=False, nb_iter=10, scheduling="continuous",
+                           start="flat")
+    sw.set_injections(P, Q, g118.sn_mva)
+    sw.compute()
+    assert np.abs(sw.V_results - Vb[None]).max() < 1e-9
+
+
+def test_out_of_range_branch_is_value_error(g118):
+    ca = _ca(g118)
+    with pytest.raises(ValueError):
+        ca.add_contingencies_by_branch_id([[g118.n_branch + 3]])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_injection_6500_full_size_properties(g6500, precision):
+    """Full-size 6500-bus injection sweep: every row converges and the
+    reported residual equals a host recompute of the mismatch."""
+    n = 256
+    p, q = injection_scenarios(g6500, n, seed=11)
+    sw = InjectionSweepGPU(g6500.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
+                           scheduling="continuous", start="flat")
+    sw.set_injections(p, q, g6500.sn_mva)
+    sw.compute()
+    st = sw.get_row_status()
+    assert np.all(st == RowStatus.CONVERGED)
+    Y, V0, S, _, _, pv, pq = g6500.as_tuple()
+    pvpq, pq_, _ = O.j_layout(g6500.n_bus, pv, pq)
+    for r in (0, 77, n - 1):
+        F = O.mismatch(Y, sw.V_results[r], (p[r] + 1j * q[r]) / g6500.sn_mva, pvpq, pq_)
+        assert abs(np.abs(F).max() - sw.last_residuals()[r]) < 1e-10
+        assert np.abs(F).max() < 1e-8

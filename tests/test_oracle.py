@@ -1,0 +1,93 @@
+"""CPU checks of the FP64 oracle (known-answer and invariance tests restated
+from the reference's test strategy) and of the committed golden vectors."""
+
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from gpusim2grid_b200.synthetic import build_ybus, n1_branches
+from oracle import nr_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "case118_golden.npz")
+
+
+def test_jacobian_matches_finite_differences(g118):
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    pvpq, pq_, d = O.j_layout(g118.n_bus, pv, pq)
+    rng = np.random.default_rng(0)
+    V = np.abs(V0) * (1 + 0.02 * rng.standard_normal(g118.n_bus)) * np.exp(1j * 0.05 * rng.standard_normal(g118.n_bus))
+    J = O.jacobian(Y, V, pvpq, pq_).toarray()
+    F0 = O.mismatch(Y, V, S, pvpq, pq_)
+    h = 1e-7
+    for col in rng.choice(d, 12, replace=False):
+        dx = np.zeros(d)
+        dx[col] = h
+        F1 = O.mismatch(Y, O.update_v(V, dx, pvpq, pq_), S, pvpq, pq_)
+        # F = -mismatch, so dF/dx = -J
+        np.testing.assert_allclose(-(F1 - F0) / h, J[:, col], atol=2e-4 * max(1, np.abs(J[:, col]).max()))
+
+
+def test_branch_trip_equals_rebuilt_ybus(g118):
+    rows = n1_branches(g118)[:5]
+    for b in rows:
+        Yt = O.trip_branches(g118.Ybus, [b, b], g118.branch_from, g118.branch_to,
+                             g118.yff, g118.yft, g118.ytf, g118.ytt)
+        keep = np.ones(g118.n_branch, dtype=bool)
+        keep[b] = False
+        *_, Yr = build_ybus(g118.n_bus, g118.branch_from[keep], g118.branch_to[keep], g118.r[keep],
+                            g118.x[keep], g118.b[keep], g118.tap[keep])
+        np.testing.assert_allclose((Yt - Yr).toarray(), 0, atol=1e-9)
+
+
+def test_base_solve_power_balance(g118):
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    V, st, it, res = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    assert st == O.CONVERGED and 2 <= it <= 10 and res < 1e-8
+    Sc = V * np.conj(Y @ V)   # independent recompute of the injections
+    mism = Sc - S
+    assert np.abs(mism.real[np.concatenate([pv, pq])]).max() < 1e-8
+    assert np.abs(mism.imag[pq]).max() < 1e-8
+    # one iteration is not converged (reference test_base_case.py:52-107)
+    _, st1, _, _ = O.nr_solve(Y, V0, S, pv, pq, 1, 1e-8)
+    assert st1 == O.MAX_ITER
+
+
+def test_nan_injection_diverges(g118):
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    S = S.copy()
+    S[pq[0]] = np.nan
+    _, st, _, res = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    assert st == O.DIVERGED and np.isnan(res)
+
+
+def test_islanding_detected(g118):
+    bridges = np.setdiff1d(np.arange(g118.n_branch), n1_branches(g118))
+    assert bridges.size > 0
+    assert O.islands(g118.n_bus, g118.branch_from, g118.branch_to, [int(bridges[0])])
+    assert not O.islands(g118.n_bus, g118.branch_from, g118.branch_to, [int(n1_branches(g118)[0])])
+
+
+def test_golden_vectors_reproduce(g118):
+    gd = np.load(GOLD)
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vb, st, it, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    np.testing.assert_allclose(Vb, gd["V_base"], atol=1e-12)
+    assert it == int(gd["base_iters"])
+    ptr, ids = gd["ctg_ptr"], gd["ctg_ids"]
+    ctg = [list(ids[ptr[r]:ptr[r + 1]]) for r in range(len(ptr) - 1)]
+    Vc, sc, ic, _ = O.contingency_sweep(Y, V0, S, pv, pq, ctg[:6] + ctg[-2:], g118.branch_from,
+                                        g118.branch_to, g118.yff, g118.yft, g118.ytf, g118.ytt, 10, 1e-8)
+    sel = list(range(6)) + [len(ctg) - 2, len(ctg) - 1]
+    np.testing.assert_allclose(np.nan_to_num(Vc), np.nan_to_num(gd["V_ctg"][sel]), atol=1e-12)
+    np.testing.assert_array_equal(sc, gd["status_ctg"][sel])
+    np.testing.assert_array_equal(ic, gd["iters_ctg"][sel])
+    assert gd["status_ctg"][-2] == O.NOT_SIMULATED
+
+
+def test_fixed_mode_runs_exact_steps(g118):
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vb, _, _, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    V, st, it, res = O.nr_solve(Y, Vb, S, pv, pq, 4, 1e-8, mode="fixed")
+    assert it == 4 and st == O.CONVERGED and res < 1e-8
