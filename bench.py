@@ -48,6 +48,8 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--strategy", choices=["adaptive", "refactor_every"], default="adaptive",
+                    help="linear-solve strategy of the measured arm (the FP64 comparison arm always refactors)")
     ap.add_argument("--cpu-sample-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
@@ -146,17 +148,22 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes_per_row_iter(info, w):
-    """Bytes one Newton iteration of one row must move at minimum (shared
-    structure amortised to zero): V read, outage edits, F write, J write and
-    read, LU factor write and read, rhs/x, dx read, V read-modify-write."""
+def algorithmic_bytes(info, w):
+    """Minimum bytes (shared structure amortised to zero) of one LU
+    factorization of one row (J write and read, factor write) and of one
+    Newton step of one row (V read, outage edits, F write, factor read by the
+    solves, rhs/x, dx read, V read-modify-write).  w = 8 (FP64) or 4 (FP32)."""
     n, d, nJ, nLU = info["n_bus"], info["dim_j"], info["nnz_j"], info["nnz_lu"]
-    return 16 * n + 16 * 4 + 8 * d + w * nJ * 2 + w * nLU * 2 + 16 * d + 8 * d + 32 * n
+    per_factor = w * nJ * 2 + w * nLU
+    per_iter = 16 * n + 16 * 4 + 8 * d + w * nLU + 16 * d + 8 * d + 32 * n
+    return per_factor, per_iter
 
 
-def flops_per_row_iter(info):
+def algorithmic_flops(info):
+    """FLOPs of one LU factorization (2 per madd) and of one Newton step
+    (two triangular solves + SpMV/Jacobian complex arithmetic)."""
     lu = info["head_madds"] + info["schur_madds"] + info["dense_madds"]
-    return 2 * lu + 4 * info["nnz_lu"] + 40 * info["nnz_y"]
+    return 2 * lu, 4 * info["nnz_lu"] + 40 * info["nnz_y"]
 
 
 # ---------------------------------------------------------------- our arm
@@ -178,12 +185,14 @@ def run_ours(args):
                                 nb_iter=MAX_ITER, scheduling="continuous", tol=TOL, start="flat", device=local)
     ca.set_branch_data(*g.branch_data())
     ca.add_contingencies_by_branch_id(rows)
+    ca.strategy = args.strategy
+    strat = lib.REFACTOR_ADAPTIVE if args.strategy == "adaptive" else lib.REFACTOR_EVERY
     s = ca.session
     info = s.info()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
-        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False)
+        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False, strat)
         return s.timings()["kernel_ms"]
 
     def barrier():
@@ -211,6 +220,7 @@ def run_ours(args):
     _, res, st, it = s.results()
     n_conv = int((st == RowStatus.CONVERGED).sum())
     total_iters = int(it.sum())
+    total_factors = int(s.factor_counts().sum())
     value = world * n_conv * args.steps / (total_ms / 1e3)
 
     # FP64 plain engine on the same rows (the metric's comparison arm)
@@ -225,10 +235,10 @@ def run_ours(args):
             fp64_ms.append(s.timings()["kernel_ms"])
         _, _, st64, _ = s.results()
         fp64_value = int((st64 == 0).sum()) / (np.mean(fp64_ms) / 1e3)
-        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False)
+        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False, strat)
 
     # phase split (one extra profiled run, not timed)
-    s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, True)
+    s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, True, strat)
     phases = dict(zip(["mismatch", "fill", "head_lu", "schur", "dense_lu", "solves", "update"],
                       [round(x, 4) for x in s.timings()["phase_share"]]))
 
@@ -248,12 +258,13 @@ def run_ours(args):
     d2h = V.nbytes + stt.nbytes + r.nbytes
 
     w = 4 if args.precision == "mixed" else 8
-    bpri = algorithmic_bytes_per_row_iter(info, w)
-    # units per launch: every Newton iteration plus the final mismatch evaluation of each row
-    achieved_gbs = bpri * total_iters / (total_ms / args.steps / 1e3) / 1e9
+    b_fact, b_iter = algorithmic_bytes(info, w)
+    launch_bytes = b_fact * total_factors + b_iter * total_iters
+    achieved_gbs = launch_bytes / (total_ms / args.steps / 1e3) / 1e9
     peak, peak_kind = _peaks()
-    fpri = flops_per_row_iter(info)
-    achieved_tflops = fpri * total_iters / (total_ms / args.steps / 1e3) / 1e12
+    f_fact, f_iter = algorithmic_flops(info)
+    launch_flops = f_fact * total_factors + f_iter * total_iters
+    achieved_tflops = launch_flops / (total_ms / args.steps / 1e3) / 1e12
     fma_peak = 71.4 if args.precision == "mixed" else 37.1
 
     line = {
@@ -264,17 +275,17 @@ def run_ours(args):
         "dtype": "f64 mismatch/V, f32 J/LU" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "grid": GRID, "rows": len(rows), "start": "flat",
-                   "precision": args.precision, "tol_pu": TOL, "max_iter": MAX_ITER,
+                   "precision": args.precision, "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
-        "rows_converged": n_conv, "newton_iters_total": total_iters,
+        "rows_converged": n_conv, "newton_iters_total": total_iters, "lu_factorizations_total": total_factors,
         "mean_iters": round(total_iters / max(len(rows), 1), 3),
         "fp64_flat_value": None if fp64_ms is None else round(fp64_value, 1),
         "speedup_vs_fp64_flat": None if fp64_ms is None else round(value / world / fp64_value, 3),
         "phase_share": phases,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": None,
-                     "note": f"peak {peak_kind}; algorithmic bytes {bpri} per row-iteration x "
-                             f"{total_iters} row-iterations per launch"},
+                     "note": f"peak {peak_kind}; algorithmic bytes per launch = {b_fact} per LU x "
+                             f"{total_factors} LUs + {b_iter} per Newton step x {total_iters} steps"},
         "fma_roofline": {"achieved": round(achieved_tflops, 3), "peak": fma_peak, "unit": "TFLOP/s",
                          "frac": round(achieved_tflops / fma_peak, 4),
                          "note": "FP64 (or FP32) FMA pipe; peak measured by a DFMA/FFMA loop on this pool"},

@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["nr_kernel.cu"]
 CPP_SOURCES = ["plan.cpp", "session.cpp"]
-HEADERS = ["nr_kernel.cuh", "plan.hpp"]
+HEADERS = ["nr_kernel.cuh", "plan.hpp", "dense_lu.cuh"]
 
 
 def _stale(target: Path, deps) -> bool:
@@ -57,7 +57,9 @@ def build(verbose: bool = False) -> None:
         obj = BUILD / (src + ".o")
         objs.append(obj)
         if _stale(obj, [CSRC / src] + hdrs):
-            jobs.append([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+            # GS2G_NVCC_DEFINES: build-time tunables, e.g. "-DGS2G_DENSE_KC=32"
+            extra = os.environ.get("GS2G_NVCC_DEFINES", "").split()
+            jobs.append([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", *extra,
                          "-Xptxas", "-v", "-c", str(CSRC / src), "-o", str(obj)])
     for src in CPP_SOURCES:
         obj = BUILD / (src + ".o")

@@ -31,6 +31,7 @@ from ._native import lib
 __all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU"]
 
 _START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS}
+_STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE}
 
 
 def _ids_csr(rows):
@@ -46,7 +47,7 @@ def _ids_csr(rows):
 class _BatchSweep:
     def __init__(self, grid, *, init_from_n_powerflow=True, precision="fp64", nb_iter=4, max_iter_base=10,
                  tol_base=1e-8, device=None, scheduling=None, nb_iter_per_round=1, tol=None, start="base",
-                 **_ignored):
+                 strategy="refactor_every", **_ignored):
         d = grid_arrays(grid)
         self._d = d
         self._prec = resolve_precision(precision)
@@ -70,6 +71,9 @@ class _BatchSweep:
                                    f"residual {res:.3e})")
             self._base_iters = it
         self.start = start
+        self.strategy = strategy
+        self.refactor_ratio = 0.3
+        self.max_reuse = 3
         self._n_branches = None
         self._ran = False
         self._timings = BatchTimings()
@@ -86,6 +90,21 @@ class _BatchSweep:
         if value not in _START:
             raise ValueError(f"Unknown start {value!r}. Choose from: {list(_START)}")
         self._start = value
+
+    @property
+    def strategy(self):
+        """Linear-solve strategy.  'refactor_every' (default): a new LU every
+        Newton step, the reference's 'direct_refactor_every'.  'adaptive':
+        keep the last LU while ||F||inf shrinks by ``refactor_ratio`` per step
+        (at most ``max_reuse`` steps), refactor otherwise; the FP64 mismatch
+        still converges every row to ``tol``."""
+        return self._strategy
+
+    @strategy.setter
+    def strategy(self, value):
+        if value not in _STRATEGY:
+            raise ValueError(f"Unknown strategy {value!r}. Choose from: {list(_STRATEGY)}")
+        self._strategy = value
 
     # ----------------------------------------------------------------- data
     def set_branch_data(self, branch_from, branch_to, yff_eff, yft_eff, ytf_eff, ytt_eff, bus_vn_kv=None,
@@ -110,7 +129,8 @@ class _BatchSweep:
         fixed = self.scheduling == "chunked"
         n_ctas = max(int(batch_size), 0)
         t0 = time.perf_counter()
-        self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False)
+        self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False,
+                    _STRATEGY[self._strategy], float(self.refactor_ratio), int(self.max_reuse))
         tm = self._s.timings()
         self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
                                      t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
@@ -142,6 +162,12 @@ class _BatchSweep:
 
     def get_row_iterations(self):
         return self._results()[3].copy()
+
+    def get_row_factorizations(self):
+        """LU factorizations each row of the last ``compute()`` performed."""
+        if not self._ran:
+            raise RuntimeError("Call compute() first.")
+        return self._s.factor_counts()
 
     @property
     def V_results(self):

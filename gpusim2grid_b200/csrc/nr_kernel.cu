@@ -21,6 +21,8 @@
 
 #include <cuda_runtime.h>
 
+#include "dense_lu.cuh"
+
 #include <cmath>
 #include <cstdint>
 
@@ -30,17 +32,8 @@ namespace {
 
 constexpr int BS = 256;        // threads per CTA
 constexpr int NWARP = BS / 32;
-constexpr int NB = 32;         // dense panel width
-constexpr int TM = 64;         // dense trailing-update tile (TM x TM)
 constexpr int MAX_EDITS = 64;  // Ybus edits per row held in shared memory
-
-template <typename T>
-struct DenseSmem {
-  static constexpr int kD = NB * (NB + 1);
-  static constexpr int kA = TM * (NB + 1);
-  static constexpr int kB = NB * TM;
-  static constexpr int bytes = (kD + kA + kB) * (int)sizeof(T);
-};
+static_assert(BS == dense::BS, "the dense LU assumes the sweep's CTA size");
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -78,151 +71,11 @@ __device__ double block_nanmax(double v, double* s_red) {
   return r;
 }
 
-// ---------------------------------------------------------------------------
-// Dense tail LU (no pivoting, in place, row-major with leading dimension ld).
-// Right-looking, NB-wide panels; the trailing update is a TM x TM tiled GEMM
-// with a 4x4 register tile per thread.
-// ---------------------------------------------------------------------------
-template <typename T>
-__device__ void dense_trailing_update(T* __restrict__ C, const T* __restrict__ L, const T* __restrict__ U,
-                                      int m, int kb, int ld, T* sA, T* sB) {
-  const int tid = threadIdx.x;
-  const int tr = tid >> 4, tc = tid & 15;
-  for (int i0 = 0; i0 < m; i0 += TM) {
-    for (int j0 = 0; j0 < m; j0 += TM) {
-      for (int idx = tid; idx < TM * NB; idx += BS) {
-        const int r = idx / NB, c = idx % NB;
-        sA[r * (NB + 1) + c] = (i0 + r < m && c < kb) ? L[(int64_t)(i0 + r) * ld + c] : T(0);
-      }
-      for (int idx = tid; idx < NB * TM; idx += BS) {
-        const int r = idx / TM, c = idx % TM;
-        sB[r * TM + c] = (r < kb && j0 + c < m) ? U[(int64_t)r * ld + j0 + c] : T(0);
-      }
-      __syncthreads();
-      T acc[4][4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-      for (int kk = 0; kk < kb; ++kk) {
-        T av[4], bv[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) av[i] = sA[(tr * 4 + i) * (NB + 1) + kk];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) bv[j] = sB[kk * TM + tc * 4 + j];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = i0 + tr * 4 + i;
-        if (r >= m) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int c = j0 + tc * 4 + j;
-          if (c < m) C[(int64_t)r * ld + c] -= acc[i][j];
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
 template <typename T>
 __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
   const T f = (T)floor_;
   if (fabs(piv) < f) return piv < T(0) ? -f : f;
   return piv;
-}
-
-template <typename T>
-__device__ void dense_lu(T* __restrict__ A, int n, int ld, T* sD, T* sA, T* sB, double pfloor) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    const int kb = min(NB, n - k0);
-    for (int idx = tid; idx < kb * kb; idx += BS) {
-      const int r = idx / kb, c = idx % kb;
-      sD[r * (NB + 1) + c] = A[(int64_t)(k0 + r) * ld + k0 + c];
-    }
-    __syncthreads();
-    if (warp == 0) {
-      // lane r holds row r of the diagonal block in registers; the pivot row
-      // is broadcast by shuffles (no shared-memory round trips per step)
-      T x[NB];
-#pragma unroll
-      for (int c = 0; c < NB; ++c) x[c] = (lane < kb && c < kb) ? sD[lane * (NB + 1) + c] : T(lane == c ? 1 : 0);
-#pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        T piv = clamp_pivot(__shfl_sync(0xffffffffu, x[j], j), pfloor);
-        if (lane == j) x[j] = piv;
-        const T l = x[j] / piv;
-        const bool below = lane > j;
-        if (below) x[j] = l;
-#pragma unroll
-        for (int c = j + 1; c < NB; ++c) {
-          const T u = __shfl_sync(0xffffffffu, x[c], j);
-          if (below) x[c] = fma(-l, u, x[c]);
-        }
-      }
-      if (lane < kb) {
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-          if (c < kb) sD[lane * (NB + 1) + c] = x[c];
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < kb * kb; idx += BS) {
-      const int r = idx / kb, c = idx % kb;
-      A[(int64_t)(k0 + r) * ld + k0 + c] = sD[r * (NB + 1) + c];
-    }
-    const int m = n - k0 - kb;
-    if (m > 0) {
-      // L21 = A21 U11^{-1} (row-wise)
-      for (int r = tid; r < m; r += BS) {
-        T* row = A + (int64_t)(k0 + kb + r) * ld + k0;
-        T x[NB];
-#pragma unroll
-        for (int c = 0; c < NB; ++c) x[c] = c < kb ? row[c] : T(0);
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-          if (c < kb) {
-            T v = x[c];
-#pragma unroll
-            for (int q = 0; q < c; ++q) v -= x[q] * sD[q * (NB + 1) + c];
-            x[c] = v / sD[c * (NB + 1) + c];
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-          if (c < kb) row[c] = x[c];
-      }
-      // U12 = L11^{-1} A12 (column-wise, unit L)
-      for (int j = tid; j < m; j += BS) {
-        T* col = A + (int64_t)k0 * ld + k0 + kb + j;
-        T x[NB];
-#pragma unroll
-        for (int r = 0; r < NB; ++r) x[r] = r < kb ? col[(int64_t)r * ld] : T(0);
-#pragma unroll
-        for (int r = 0; r < NB; ++r) {
-          if (r < kb) {
-            T v = x[r];
-#pragma unroll
-            for (int q = 0; q < r; ++q) v -= sD[r * (NB + 1) + q] * x[q];
-            x[r] = v;
-          }
-        }
-#pragma unroll
-        for (int r = 0; r < NB; ++r)
-          if (r < kb) col[(int64_t)r * ld] = x[r];
-      }
-      __syncthreads();
-      dense_trailing_update<T>(A + (int64_t)(k0 + kb) * ld + (k0 + kb), A + (int64_t)(k0 + kb) * ld + k0,
-                               A + (int64_t)k0 * ld + k0 + kb, m, kb, ld, sA, sB);
-    }
-    __syncthreads();
-  }
 }
 
 // Dense unit-lower forward solve y <- L^{-1} y and upper backward solve
@@ -341,7 +194,10 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const SweepArgs a) {
+#ifndef GS2G_MIN_CTAS_PER_SM
+#define GS2G_MIN_CTAS_PER_SM 2
+#endif
+__global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const DevPlan P, const SweepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_row;
   __shared__ int s_ne;
@@ -349,9 +205,7 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
   __shared__ double2 s_ev[MAX_EDITS];
   __shared__ double s_red[NWARP];
   __shared__ T s_blk[32];
-  T* sD = reinterpret_cast<T*>(smem_raw);
-  T* sA = sD + DenseSmem<T>::kD;
-  T* sB = sA + DenseSmem<T>::kA;
+  T* s_dense = reinterpret_cast<T*>(smem_raw);
 
   const int tid = threadIdx.x;
   const WsLayout L = ws_layout<T>(P);
@@ -407,6 +261,9 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
     prof.start();
 
     int it = 0, status = ROW_MAX_ITER;
+    bool have_factor = false;
+    int since_factor = 0, n_factor = 0;
+    double last_nrm = INFINITY;
     double nrm = NAN;
     for (;;) {
       // ---- I = Y V (row-patched Ybus) ------------------------------------
@@ -451,6 +308,19 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
         if (it >= a.max_iter) { status = ROW_MAX_ITER; break; }
       }
 
+      // ---- refactor, or reuse the factor of an earlier iterate ---------------
+      // Policy 0 refactors every step (Newton).  Policy 1 keeps the last LU
+      // while the mismatch contracts by at least refactor_ratio per step and
+      // for at most max_reuse steps (an inexact Newton / chord step: the FP64
+      // mismatch still drives the iterate to the same fixed point).  nrm is
+      // block-uniform, so the branch is taken by the whole CTA.
+      const bool refactor = !have_factor || a.refactor_policy == 0 || !(nrm <= a.refactor_ratio * last_nrm) ||
+                            since_factor >= a.max_reuse;
+      last_nrm = nrm;
+      if (refactor) {
+        have_factor = true;
+        since_factor = 0;
+        ++n_factor;
       // ---- zero the dense tail, then scatter J ------------------------------
       {
         const int64_t ns = (int64_t)P.nt * P.ld;
@@ -548,7 +418,9 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
 
       prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
-      if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, sD, sA, sB, a.pivot_floor);
+      if (P.nt > 0) dense::lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+      }  // refactor
+      ++since_factor;
 
       prof.mark(PH_DENSE);
       // ---- solves -----------------------------------------------------------
@@ -605,6 +477,7 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
       a.res_out[row] = nrm;
       a.status_out[row] = status;
       a.iters_out[row] = it;
+      if (a.factors_out != nullptr) a.factors_out[row] = n_factor;
     }
     __syncthreads();
   }
@@ -612,7 +485,7 @@ __global__ void __launch_bounds__(BS, 2) sweep_kernel(const DevPlan P, const Swe
 
 template <typename T>
 int smem_bytes() {
-  return DenseSmem<T>::bytes;
+  return dense::Smem<T>::bytes;
 }
 
 }  // namespace
@@ -621,9 +494,22 @@ int64_t workspace_bytes(const DevPlan& P, int prec) {
   return prec == 1 ? ws_layout<float>(P).total : ws_layout<double>(P).total;
 }
 
+namespace {
+// Dynamic shared memory above 48 KB needs an opt-in per kernel (per device
+// context); cheap and idempotent, so it is set before every query / launch.
+cudaError_t opt_in_smem() {
+  cudaError_t e = cudaFuncSetAttribute(sweep_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes<float>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(sweep_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              smem_bytes<double>());
+}
+}  // namespace
+
 int sweep_ctas(int prec, int device) {
   int n_sm = 0;
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
+  opt_in_smem();
   int per_sm = 0;
   if (prec == 1)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<float>, BS, smem_bytes<float>());
@@ -636,6 +522,8 @@ int sweep_ctas(int prec, int device) {
 int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n_ctas <= 0) return (int)cudaErrorInvalidValue;
+  const cudaError_t e = opt_in_smem();
+  if (e != cudaSuccess) return (int)e;
   if (prec == 1)
     sweep_kernel<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
   else

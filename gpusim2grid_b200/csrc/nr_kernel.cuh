@@ -63,6 +63,10 @@ struct SweepArgs {
   int max_iter;
   double tol;
   int fixed_iters;        // 1: exactly max_iter steps then the residual; 0: stop at tol
+  int refactor_policy;    // 0: refactor every step; 1: reuse the LU while ||F|| contracts
+  double refactor_ratio;  // policy 1: refactor when ||F_k|| > ratio * ||F_{k-1}||
+  int max_reuse;          // policy 1: refactor after this many steps on one LU
+  int* factors_out;       // [n_rows] LU factorizations per row (nullptr: not recorded)
   // outputs
   double* v_out;          // [n_rows * n_bus] complex
   double* res_out;        // [n_rows]

@@ -29,8 +29,8 @@ struct TailOptions {
   // head columns a cost model says are cheaper as dense work (default).
   int policy = 1;
   // cost-model weights: dense madds per unit of cost and scatter volume per unit
-  double dense_rate = 64.0 * 0.7;
-  double scatter_rate = 4.0;
+  double dense_rate = 40.0;
+  double scatter_rate = 1.0;
   // forced tail-row threshold (< 0: chosen by the cost model)
   int force_tau = -1;
 };

@@ -90,7 +90,8 @@ void check(int rc) {
 }
 
 gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
-                        int n_ctas, bool profile = false) {
+                        int n_ctas, bool profile = false, int refactor = 0, double refactor_ratio = 0.0,
+                        int max_reuse = 0) {
   gs2g_run_opts o{};
   o.max_iter = max_iter;
   o.tol = tol;
@@ -100,6 +101,9 @@ gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precisio
   o.pivot_floor = pivot_floor;
   o.n_ctas = n_ctas;
   o.profile_phases = profile ? 1 : 0;
+  o.refactor_policy = refactor;
+  o.refactor_ratio = refactor_ratio;
+  o.max_reuse = max_reuse;
   return o;
 }
 
@@ -230,8 +234,9 @@ class Session {
   }
 
   void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas,
-           bool profile) {
-    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile);
+           bool profile, int refactor, double refactor_ratio, int max_reuse) {
+    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
+                                refactor_ratio, max_reuse);
     int rc;
     {
       py::gil_scoped_release nogil;
@@ -258,6 +263,13 @@ class Session {
     }
     check(rc);
     return py::make_tuple(V, res, st, it);
+  }
+
+  py::array_t<int> factor_counts() const {
+    const int nr = gs2g_n_rows(h());
+    py::array_t<int> f(nr);
+    check(gs2g_get_factor_counts(h(), f.mutable_data()));
+    return f;
   }
 
   py::tuple device_results() const {
@@ -369,6 +381,8 @@ PYBIND11_MODULE(_gs2g, m) {
   m.attr("START_VINIT") = GS2G_START_VINIT;
   m.attr("START_BASE") = GS2G_START_BASE;
   m.attr("START_ROWS") = GS2G_START_ROWS;
+  m.attr("REFACTOR_EVERY") = GS2G_REFACTOR_EVERY;
+  m.attr("REFACTOR_ADAPTIVE") = GS2G_REFACTOR_ADAPTIVE;
   m.def("version", &gs2g_version);
   m.def("max_edits_per_row", &gs2g_max_edits_per_row);
   m.def("acpf_nr", &acpf_nr);
@@ -390,7 +404,9 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("solve_base", &Session::solve_base)
       .def("set_base_v", &Session::set_base_v)
       .def("run", &Session::run, py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"), py::arg("precision"),
-           py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false)
+           py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false,
+           py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0)
+      .def("factor_counts", &Session::factor_counts)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)
       .def("device_results", &Session::device_results)

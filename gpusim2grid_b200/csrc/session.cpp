@@ -99,7 +99,7 @@ struct gs2g_session {
   int n_rows = 0;
   bool rows_have_sbus = false, rows_have_edits = false, rows_have_skip = false;
   DevBuf d_sbus_rows, d_edit_ptr, d_edit_k, d_edit_val, d_row_skip;
-  DevBuf d_v_out, d_res, d_status, d_iters;
+  DevBuf d_v_out, d_res, d_status, d_iters, d_factors;
   DevBuf d_ws, d_queue, d_phase;
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -275,6 +275,7 @@ struct OutBufs {
   double* res;
   int* status;
   int* iters;
+  int* factors = nullptr;
 };
 
 float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
@@ -309,6 +310,12 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
   a.pivot_floor = o.pivot_floor;
+  if (o.refactor_policy != GS2G_REFACTOR_EVERY && o.refactor_policy != GS2G_REFACTOR_ADAPTIVE)
+    throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY or GS2G_REFACTOR_ADAPTIVE");
+  a.refactor_policy = o.refactor_policy;
+  a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
+  a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
+  a.factors_out = out.factors;
   a.phase_cycles = nullptr;
   if (o.profile_phases) {
     s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
@@ -722,7 +729,9 @@ int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
   s->d_res.ensure((size_t)std::max(nr, 1) * sizeof(double));
   s->d_status.ensure((size_t)std::max(nr, 1) * sizeof(int));
   s->d_iters.ensure((size_t)std::max(nr, 1) * sizeof(int));
-  OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>()};
+  s->d_factors.ensure((size_t)std::max(nr, 1) * sizeof(int));
+  OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>(),
+             s->d_factors.as<int>()};
   s->tm.kernel_ms = launch(s, o, nr, v0, v0s, sb, sbs, true, ob, o.n_ctas);
   s->last_rows_run = nr;
   s->tm.total_ms = ms_since(t0);
@@ -742,6 +751,16 @@ int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, in
   if (residuals && nr) ck(cudaMemcpy(residuals, s->d_res.p, nr * sizeof(double), cudaMemcpyDeviceToHost), "read res");
   if (status && nr) ck(cudaMemcpy(status, s->d_status.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read status");
   if (iters && nr) ck(cudaMemcpy(iters, s->d_iters.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read iters");
+  GS2G_CATCH
+}
+
+int gs2g_get_factor_counts(const gs2g_session* s, int* factors) {
+  GS2G_TRY
+  if (!s || !factors) throw std::invalid_argument("NULL argument");
+  DeviceGuard g(s->device);
+  if (s->last_rows_run)
+    ck(cudaMemcpy(factors, s->d_factors.p, (size_t)s->last_rows_run * sizeof(int), cudaMemcpyDeviceToHost),
+       "read factor counts");
   GS2G_CATCH
 }
 

@@ -78,7 +78,18 @@ typedef struct gs2g_run_opts {
   double pivot_floor; /* static-pivot floor, 0 disables */
   int n_ctas;         /* persistent CTAs, <= 0 for one full wave */
   int profile_phases; /* 1: record per-phase SM cycles (gs2g_timings.phase_*) */
+  /* GS2G_REFACTOR_EVERY: a new LU every Newton step (the reference's default
+   * 'direct_refactor_every' strategy).  GS2G_REFACTOR_ADAPTIVE: keep the last
+   * LU while ||F||inf shrinks by at least refactor_ratio per step, for at most
+   * max_reuse steps (the reference's 'direct_iter0_only' idea, made adaptive);
+   * the FP64 mismatch still converges every row to tol. */
+  int refactor_policy;
+  double refactor_ratio; /* adaptive: <= 0 selects 0.3 */
+  int max_reuse;         /* adaptive: <= 0 selects 3 */
 } gs2g_run_opts;
+
+#define GS2G_REFACTOR_EVERY 0
+#define GS2G_REFACTOR_ADAPTIVE 1
 
 #define GS2G_N_PHASES 7 /* mismatch, fill, head LU, Schur, dense LU, solves, update */
 
@@ -143,6 +154,8 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual);
 int gs2g_run(gs2g_session* s, const gs2g_run_opts* o);
 int gs2g_n_rows(const gs2g_session* s);
 int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters);
+/* LU factorizations each row of the last run performed. */
+int gs2g_get_factor_counts(const gs2g_session* s, int* factors);
 /* Device pointers of the last run's results (valid until the next run or destroy). */
 int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
 int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
