@@ -5,7 +5,7 @@ Produces, next to this file:
                                        + sm_100a CUDA kernels, static cudart
   _gs2g<EXT_SUFFIX>                    pybind11 binding of that C-ABI
 
-Run ``python -m gpusim2grid_b200._build`` (or ``__graft_entry__.build()``).
+Run ``python gpusim2grid_b200/_build.py`` (or ``__graft_entry__.build()``).
 nvcc cross-compiles for sm_100a without a GPU.  Rebuilds only what is stale.
 """
 

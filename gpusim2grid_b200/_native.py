@@ -11,7 +11,7 @@ try:
 except ImportError as e:  # pragma: no cover - exercised only on a broken install
     raise ImportError(
         "gpusim2grid_b200: the native library is not built "
-        "(run `python -m gpusim2grid_b200._build`): " + str(e)) from e
+        "(run `python gpusim2grid_b200/_build.py`): " + str(e)) from e
 
 from pathlib import Path
 
