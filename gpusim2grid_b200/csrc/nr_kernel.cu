@@ -25,6 +25,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 
 namespace gs2g {
 
@@ -529,6 +530,63 @@ int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
   else
     sweep_kernel<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(P, a);
   return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free sweep.  Its scratch -- the row-queue counter (first 256
+// bytes) and the per-CTA workspaces -- lives in this file-scope device array,
+// which every GPU that loads the library holds until the process exits.
+// Host code must not use the array's name as an address: on the host it is
+// a stand-in symbol.  The device address is looked up once per device with
+// cudaGetSymbolAddress (the first call on a device does it, so that first
+// call should come before any stream capture) and cached.  All calls share
+// the array, so calls that overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_sweep_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+char* g_scratch_ptr[kMaxDevices] = {};
+
+cudaError_t scratch_address(int device, char** out) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_ptr[device] = static_cast<char*>(p);
+  }
+  *out = g_scratch_ptr[device];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+int launch_sweep_static(const DevPlan& P, SweepArgs a, int prec, int device, void* stream, int* n_ctas_used) {
+  const int64_t ws = workspace_bytes(P, prec);
+  const int64_t room = kStaticScratchBytes - 256;
+  if (ws <= 0 || ws > room) return (int)cudaErrorInvalidValue;
+  char* base = nullptr;
+  cudaError_t e = scratch_address(device, &base);
+  if (e != cudaSuccess) return (int)e;
+  int n_ctas = sweep_ctas(prec, device);
+  const int64_t fit = room / ws;
+  if (n_ctas > fit) n_ctas = (int)fit;
+  if (n_ctas > a.n_rows) n_ctas = a.n_rows;
+  if (n_ctas < 1) n_ctas = 1;
+  a.queue = reinterpret_cast<int*>(base);
+  a.workspace = base + 256;
+  a.ws_stride = ws;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the queue must start at zero: the previous call left its final count there
+  e = cudaMemsetAsync(base, 0, sizeof(int), st);
+  if (e != cudaSuccess) return (int)e;
+  if (n_ctas_used) *n_ctas_used = n_ctas;
+  if (a.n_rows <= 0) return (int)cudaSuccess;
+  return launch_sweep(P, a, prec, n_ctas, stream);
 }
 
 }  // namespace gs2g

@@ -104,4 +104,15 @@ int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
 // CTAs that fit at once for `prec` (for sizing the workspace).
 int sweep_ctas(int prec, int device);
 
+// Size of the file-scope device array the allocation-free sweep uses as its
+// scratch (row queue + per-CTA workspaces).
+constexpr int64_t kStaticScratchBytes = int64_t(64) << 20;
+
+// Launch the sweep with its scratch in that static array instead of caller
+// memory: a.queue / a.workspace / a.ws_stride are filled in here.  `device`
+// must be the current device.  Returns a cudaError_t as int;
+// cudaErrorInvalidValue when one CTA's workspace does not fit the array.
+// *n_ctas_used receives the CTA count (bounded by what fits).
+int launch_sweep_static(const DevPlan& P, SweepArgs a, int prec, int device, void* stream, int* n_ctas_used);
+
 }  // namespace gs2g

@@ -138,6 +138,8 @@ class Session {
     if (!s_) throw std::runtime_error("session is closed");
     return s_;
   }
+  // the C-ABI handle, for callers that drive include/gs2g.h directly
+  uintptr_t handle() const { return reinterpret_cast<uintptr_t>(h()); }
 
   py::dict info() const {
     gs2g_grid_info g{};
@@ -391,6 +393,7 @@ PYBIND11_MODULE(_gs2g, m) {
            py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),
            py::arg("pq"), py::arg("tail_policy") = 1)
       .def("close", &Session::close)
+      .def("handle", &Session::handle)
       .def("info", &Session::info)
       .def("set_branch_data", &Session::set_branch_data)
       .def("set_contingencies", &Session::set_contingencies)

@@ -797,6 +797,52 @@ int gs2g_sync(gs2g_session* s) {
   GS2G_CATCH
 }
 
+int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, int64_t v0_stride,
+                          const double* sbus, int64_t sbus_stride, const gs2g_run_opts* o, double* v_out,
+                          double* residuals, int* status, int* iters, void* stream) {
+  // Allocation-free path: uses only device buffers the session set up at
+  // creation (plan, Ybus) and caller memory; the kernel's scratch is the
+  // library's static device array (launch_sweep_static).
+  GS2G_TRY
+  if (!s || !o) throw std::invalid_argument("run_rows_noalloc: NULL session or options");
+  if (n_rows < 0 || v0_stride < 0 || sbus_stride < 0) throw std::invalid_argument("run_rows_noalloc: negative size");
+  if (n_rows > 0 && (!v0 || !sbus || !v_out || !residuals || !status || !iters))
+    throw std::invalid_argument("run_rows_noalloc: NULL input or output");
+  if (o->precision != GS2G_PREC_FP64 && o->precision != GS2G_PREC_MIXED)
+    throw std::invalid_argument("precision must be GS2G_PREC_FP64 or GS2G_PREC_MIXED");
+  if (o->refactor_policy != GS2G_REFACTOR_EVERY && o->refactor_policy != GS2G_REFACTOR_ADAPTIVE)
+    throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY or GS2G_REFACTOR_ADAPTIVE");
+  if (o->max_iter < 0) throw std::invalid_argument("max_iter must be >= 0");
+  const int64_t ws = gs2g::workspace_bytes(s->dplan, o->precision);
+  if (ws + 256 > gs2g::kStaticScratchBytes)
+    throw std::invalid_argument("run_rows_noalloc: one row's workspace (" + std::to_string(ws) +
+                                " bytes) exceeds the static scratch (" +
+                                std::to_string(gs2g::kStaticScratchBytes) + " bytes); use gs2g_run");
+  DeviceGuard g(s->device);
+  gs2g::SweepArgs a{};
+  a.n_rows = n_rows;
+  a.ybus = s->d_ybus.as<double>();
+  a.v0 = v0;
+  a.v0_stride = v0_stride;
+  a.sbus = sbus;
+  a.sbus_stride = sbus_stride;
+  a.max_iter = o->max_iter;
+  a.tol = o->tol;
+  a.fixed_iters = o->fixed_iters;
+  a.refactor_policy = o->refactor_policy;
+  a.refactor_ratio = o->refactor_ratio > 0 ? o->refactor_ratio : 0.3;
+  a.max_reuse = o->max_reuse > 0 ? o->max_reuse : 3;
+  a.v_out = v_out;
+  a.res_out = residuals;
+  a.status_out = status;
+  a.iters_out = iters;
+  a.pivot_floor = o->pivot_floor;
+  int used = 0;
+  ck((cudaError_t)gs2g::launch_sweep_static(s->dplan, a, o->precision, s->device, stream, &used),
+     "allocation-free sweep launch");
+  GS2G_CATCH
+}
+
 int gs2g_acpf_nr(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices, const double* ybus_values,
                  double* v_inout, const double* sbus, const int* pv, int n_pv, const int* pq, int n_pq, int max_iter,
                  double tol, int precision, int* converged, int* iters, double* residual, double* kernel_ms) {

@@ -162,6 +162,29 @@ int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
 /* Synchronise the session stream. */
 int gs2g_sync(gs2g_session* s);
 
+/* Allocation-free batch solve.  No counterpart in the reference: this entry
+ * point exists for callers that must not allocate device memory while they
+ * solve -- e.g. code running under a framework's memory pool or arena that
+ * forbids cudaMalloc/cudaFree in its hot path, or real-time code that cannot
+ * afford an allocation's implicit synchronisation.  It runs the same sweep
+ * kernel as gs2g_run on rows that differ by start voltage and injections (no
+ * branch trips), with every input and output in caller-provided device
+ * memory, and keeps the kernel's scratch (the row queue and per-row
+ * workspaces, max 64 MiB in total) in a static device array the library
+ * holds on each GPU that loads it.  It calls no cudaMalloc, cudaFree or
+ * allocating library routine.
+ *   v0 / sbus: complex rows (interleaved doubles) with strides in complex
+ *   elements (0: one row shared by all).  Outputs as gs2g_get_device_results.
+ *   Grids whose per-row workspace exceeds the static scratch are rejected
+ *   (GS2G_ERR_INVALID); fewer rows run at once when fewer workspaces fit.
+ *   The first call on a device looks up the array's device address (make it
+ *   before any stream capture).  Every call shares the array: calls that
+ *   overlap on the GPU race.  Returns once the work is enqueued on `stream`
+ *   (NULL = default stream); synchronise it before reading the outputs. */
+int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, int64_t v0_stride,
+                          const double* sbus, int64_t sbus_stride, const gs2g_run_opts* o, double* v_out,
+                          double* residuals, int* status, int* iters, void* stream);
+
 /* acpf_nr_gpu: one solve from Vinit, V written back into `v_inout`.
  * Returns the status through *converged (1/0), *iters and *residual. */
 int gs2g_acpf_nr(int device, int n_bus, const int* ybus_indptr, const int* ybus_indices,
