@@ -2,15 +2,22 @@
 
 Workload (one "step"): the full N-1 contingency sweep of the seeded synthetic
 2000-bus grid (3200 branches, 400 PV buses, 1500 loads): every single-branch
-outage that keeps the grid connected (2847 rows for seed 0), flat start,
-||F||inf < 1e-8 pu, at most 10 Newton steps per row, one symbolic analysis
-shared by every row.
+outage that keeps the grid connected (2847 rows for seed 0), ||F||inf < 1e-8
+pu, at most 10 Newton steps per row, one symbolic analysis shared by every
+row.  Default arm (``--start learned``): each row starts from the voltages
+the warm-start MLP predicts for it (features -> BF16 MLP on tcgen05 -> V0,
+on the device), then the mixed-precision sweep converges it; the network is
+trained before the run (untimed, reported under ``training``) on 100k
+GPU-solved synthetic operating points.  The comparison arm is the same rows
+solved by plain FP64 Newton from a flat start (``fp64_flat_value``).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--start learned|flat] [--precision mixed|fp64]
 
-`value`  : rows converged per second, device time of the sweep kernel (CUDA
-           events on the session stream), inputs resident in HBM, L2 flushed
-           (256 MiB write) before every timed step.
+`value`  : rows converged per second; device time per step = CUDA events
+           around features + MLP + V0 (torch's stream) + the sweep kernel
+           (CUDA events on the session stream); inputs resident in HBM; L2
+           flushed (256 MiB write) before every timed step.
 `e2e`    : the same metric through the public facade with host buffers
            (contingency lists in, voltages + statuses + residuals out).
 --impl reference: the CPU restatement of the reference's Newton–Raphson
@@ -39,6 +46,7 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "n1_sweep_case2000_synth"
 GRID = "case2000_synth"
 MAX_ITER, TOL = 10, 1e-8
+METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
 
 
 def _args():
@@ -53,6 +61,11 @@ def _args():
     ap.add_argument("--cpu-sample-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
+    ap.add_argument("--start", choices=["learned", "flat"], default="learned",
+                    help="learned: MLP warm start (trained untimed before the run); flat: Vinit")
+    ap.add_argument("--train-rows", type=int, default=100000)
+    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--hidden", type=int, default=1024)
     return ap.parse_args()
 
 
@@ -167,19 +180,28 @@ def algorithmic_flops(info):
 
 
 # ---------------------------------------------------------------- our arm
+def _train_learned(g, args, device):
+    from gpusim2grid_b200.warmstart import LearnedStart
+    ls = LearnedStart(g, hidden=args.hidden, layers=2, device=device, seed=0)
+    rep = ls.train(n_rows=args.train_rows, epochs=args.train_epochs, batch=1024, lr=1e-3, lr_decay=0.8, seed=1)
+    return ls, rep
+
+
 def run_ours(args):
     import torch
     rank, world, local = _dist()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from gpusim2grid_b200 import ContingencyAnalysisGPU, RowStatus
     from gpusim2grid_b200._native import lib
 
     g, rows = _workload()
     if args.rows > 0:
         rows = rows[:args.rows]
+    n = len(rows)
+    learned = args.start == "learned"
     prec = lib.PREC_MIXED if args.precision == "mixed" else lib.PREC_FP64
     ca = ContingencyAnalysisGPU(g.as_tuple(), init_from_n_powerflow=False, precision=args.precision,
                                 nb_iter=MAX_ITER, scheduling="continuous", tol=TOL, start="flat", device=local)
@@ -191,9 +213,39 @@ def run_ours(args):
     info = s.info()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    train = None
+    ls = None
+    ratio, reuse = 0.0, 0
+    if learned:
+        t0 = time.perf_counter()
+        ls, rep = _train_learned(g, args, local)
+        train = {"rows": rep["n_rows"], "epochs": args.train_epochs, "hidden": args.hidden, "layers": 2,
+                 "t_generate_solve_s": round(rep["t_rows_s"] + rep["t_solve_s"], 2),
+                 "t_fit_s": round(rep["t_fit_s"], 2), "t_total_s": round(time.perf_counter() - t0, 2),
+                 "loss_first_last": [round(rep["loss"][0], 5), round(rep["loss"][-1], 5)],
+                 "val_mse": round(rep["val"][-1], 5) if rep["val"] else None,
+                 "note": "untimed: training rows are seeded synthetic operating points (load scaling and single "
+                         "outages) solved by this engine in FP64; the timed rows (base injections, every "
+                         "outage) are not among them"}
+        ca.set_learned_start(ls)
+        ratio, reuse = ca._learned_opts
+        ptr, ids = _ids(rows)
+    start_mode = lib.START_ROWS if learned else lib.START_VINIT
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
     def step():
-        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False, strat)
-        return s.timings()["kernel_ms"]
+        """Device ms of one pass: [features -> MLP -> V0 (torch's stream)] + sweep kernel (session stream)."""
+        pre_ms = 0.0
+        if learned:
+            buf = s.start_rows_buffer(n)
+            ev0.record()
+            ls.start_voltages(None, (ptr, ids), n, out_ptr=buf)
+            ev1.record()
+            ev1.synchronize()
+            pre_ms = ev0.elapsed_time(ev1)
+        s.run(MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, False, strat, ratio, reuse, learned)
+        return pre_ms, s.timings()["kernel_ms"]
 
     def barrier():
         torch.cuda.synchronize()
@@ -205,44 +257,58 @@ def run_ours(args):
     clk = ClockSampler(local)
     clk.start()
     barrier()
-    ms = []
+    pre, ker = [], []
     for _ in range(args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        ms.append(step())
+        a_, b_ = step()
+        pre.append(a_)
+        ker.append(b_)
     barrier()
     clocks = clk.stop()
-    total_ms = float(np.sum(ms))
+    total_ms = float(np.sum(pre) + np.sum(ker))
     if world > 1:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    _, res, st, it = s.results()
+    V_w, res, st, it = s.results()
     n_conv = int((st == RowStatus.CONVERGED).sum())
     total_iters = int(it.sum())
     total_factors = int(s.factor_counts().sum())
+    n_rescued = int(s.timings()["n_rescued"])
     value = world * n_conv * args.steps / (total_ms / 1e3)
+    iters_hist = {int(k): int(v) for k, v in zip(*np.unique(it, return_counts=True))}
 
-    # FP64 plain engine on the same rows (the metric's comparison arm)
-    fp64_ms = None
-    if args.precision != "fp64":
-        s.run(MAX_ITER, TOL, False, lib.PREC_FP64, lib.START_VINIT, 0.0, 0, False)
-        fp64_ms = []
+    # comparison arms on the same rows: plain FP64 NR from flat (the metric's
+    # denominator) and mixed precision from flat
+    def flat_arm(p_, strat_):
+        s.run(MAX_ITER, TOL, False, p_, lib.START_VINIT, 0.0, 0, False, strat_)
+        ms_ = []
         for _ in range(max(1, min(args.steps, 3))):
             flush.fill_(1.0)
             torch.cuda.synchronize()
-            s.run(MAX_ITER, TOL, False, lib.PREC_FP64, lib.START_VINIT, 0.0, 0, False)
-            fp64_ms.append(s.timings()["kernel_ms"])
-        _, _, st64, _ = s.results()
-        fp64_value = int((st64 == 0).sum()) / (np.mean(fp64_ms) / 1e3)
-        s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, False, strat)
+            s.run(MAX_ITER, TOL, False, p_, lib.START_VINIT, 0.0, 0, False, strat_)
+            ms_.append(s.timings()["kernel_ms"])
+        V_, _, st_, it_ = s.results()
+        return int((st_ == 0).sum()) / (np.mean(ms_) / 1e3), V_, st_, it_
 
-    # phase split (one extra profiled run, not timed)
-    s.run(MAX_ITER, TOL, False, prec, lib.START_VINIT, 0.0, 0, True, strat)
+    fp64_value, V64, st64, it64 = flat_arm(lib.PREC_FP64, lib.REFACTOR_EVERY)
+    ok = (st == 0) & (st64 == 0)
+    agree = float(np.abs(V_w[ok] - V64[ok]).max()) if ok.any() else None
+    mixed_flat_value = None
+    if learned and args.precision == "mixed":
+        mixed_flat_value, _, _, it_mf = flat_arm(lib.PREC_MIXED, lib.REFACTOR_ADAPTIVE)
+
+    # phase split of the measured arm (one extra profiled run, not timed)
+    if learned:
+        ls.start_voltages(None, (ptr, ids), n, out_ptr=s.start_rows_buffer(n))
+        torch.cuda.synchronize()
+    s.run(MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, True, strat, ratio, reuse, learned)
     phases = dict(zip(["mismatch", "fill", "head_lu", "schur", "dense_lu", "solves", "update"],
                       [round(x, 4) for x in s.timings()["phase_share"]]))
 
     # end to end through the facade, host buffers in and out
+    ca.start = "learned" if learned else "flat"
     e2e_s = []
     for _ in range(args.steps):
         torch.cuda.synchronize()
@@ -254,44 +320,52 @@ def run_ours(args):
         r = ca.last_residuals()
         e2e_s.append(time.perf_counter() - t0)
     e2e_value = world * int((stt == 0).sum()) / float(np.mean(e2e_s))
-    h2d = 4 * (len(rows) + 1) + 4 * sum(len(r_) for r_ in rows)
+    n_ids = sum(len(r_) for r_ in rows)
+    h2d = 4 * (n + 1) + 4 * n_ids + (16 * n_ids if learned else 0)
     d2h = V.nbytes + stt.nbytes + r.nbytes
 
     w = 4 if args.precision == "mixed" else 8
     b_fact, b_iter = algorithmic_bytes(info, w)
     launch_bytes = b_fact * total_factors + b_iter * total_iters
-    achieved_gbs = launch_bytes / (total_ms / args.steps / 1e3) / 1e9
+    kernel_ms = float(np.mean(ker))
+    achieved_gbs = launch_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
     f_fact, f_iter = algorithmic_flops(info)
     launch_flops = f_fact * total_factors + f_iter * total_iters
-    achieved_tflops = launch_flops / (total_ms / args.steps / 1e3) / 1e12
+    achieved_tflops = launch_flops / (kernel_ms / 1e3) / 1e12
     fma_peak = 71.4 if args.precision == "mixed" else 37.1
+    per_step_launches = 1 + (ls.launches_per_call(n) if learned else 0)
 
     line = {
-        "metric": "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu",
+        "metric": METRIC,
         "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 mismatch/V, f32 J/LU" if args.precision == "mixed" else "f64",
+        "dtype": "f64 mismatch/V, f32 J/LU, bf16 MLP" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": WORKLOAD, "grid": GRID, "rows": len(rows), "start": "flat",
+        "config": {"workload": WORKLOAD, "grid": GRID, "rows": n, "start": args.start,
                    "precision": args.precision, "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
-        "rows_converged": n_conv, "newton_iters_total": total_iters, "lu_factorizations_total": total_factors,
-        "mean_iters": round(total_iters / max(len(rows), 1), 3),
-        "fp64_flat_value": None if fp64_ms is None else round(fp64_value, 1),
-        "speedup_vs_fp64_flat": None if fp64_ms is None else round(value / world / fp64_value, 3),
+        "rows_converged": n_conv, "rows_rescued": n_rescued, "newton_iters_total": total_iters,
+        "lu_factorizations_total": total_factors, "mean_iters": round(total_iters / max(n, 1), 3),
+        "iters_hist": iters_hist,
+        "ms_split": {"features_mlp_v0": round(float(np.mean(pre)), 4), "sweep_kernel": round(kernel_ms, 4)},
+        "fp64_flat_value": round(fp64_value, 1),
+        "speedup_vs_fp64_flat": round(value / world / fp64_value, 3),
+        "mixed_flat_value": None if mixed_flat_value is None else round(mixed_flat_value, 1),
+        "agreement_with_fp64": {"max_abs_dv_pu": agree, "rows_compared": int(ok.sum())},
+        "training": train,
         "phase_share": phases,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": None,
-                     "note": f"peak {peak_kind}; algorithmic bytes per launch = {b_fact} per LU x "
+                     "note": f"sweep kernel; peak {peak_kind}; algorithmic bytes per launch = {b_fact} per LU x "
                              f"{total_factors} LUs + {b_iter} per Newton step x {total_iters} steps"},
         "fma_roofline": {"achieved": round(achieved_tflops, 3), "peak": fma_peak, "unit": "TFLOP/s",
                          "frac": round(achieved_tflops / fma_peak, 4),
                          "note": "FP64 (or FP32) FMA pipe; peak measured by a DFMA/FFMA loop on this pool"},
         "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * per_step_launches,
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -303,6 +377,12 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def _ids(rows):
+    ptr = np.zeros(len(rows) + 1, dtype=np.int32)
+    ptr[1:] = np.cumsum([len(r) for r in rows])
+    return ptr, np.fromiter((b for r in rows for b in r), dtype=np.int32, count=int(ptr[-1]))
 
 
 # ---------------------------------------------------------------- reference arm
@@ -321,7 +401,7 @@ def run_reference(args):
     value = float(np.mean(vals))
     print(json.dumps({
         "impl": "reference",
-        "metric": "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu",
+        "metric": METRIC,
         "value": round(value, 2), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, no dataset)",

@@ -28,7 +28,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["nr_kernel.cu"]
+CU_SOURCES = ["nr_kernel.cu", "mlp_kernels.cu"]
 CPP_SOURCES = ["plan.cpp", "session.cpp"]
 HEADERS = ["nr_kernel.cuh", "plan.hpp", "dense_lu.cuh"]
 

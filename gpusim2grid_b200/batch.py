@@ -15,7 +15,10 @@ and it leaves the GPU as soon as it is done (``scheduling='continuous'``) or
 after exactly ``nb_iter`` steps (``scheduling='chunked'``, the reference's
 default).  Rows start from the converged base case as the reference's batch
 sources do (``start='base'``), or from ``Vinit`` (``start='flat'``), or from
-per-row voltages (``set_start_voltages``).
+per-row voltages (``set_start_voltages``), or from voltages a trained
+network predicts for each row (``set_learned_start``, ``start='learned'``;
+see ``warmstart.py``).  Rows given a start of their own that fail from it
+restart once from ``Vinit`` inside the same launch.
 """
 
 from __future__ import annotations
@@ -30,7 +33,7 @@ from ._native import lib
 
 __all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU"]
 
-_START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS}
+_START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS, "learned": lib.START_ROWS}
 _STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE}
 
 
@@ -74,6 +77,8 @@ class _BatchSweep:
         self.strategy = strategy
         self.refactor_ratio = 0.3
         self.max_reuse = 3
+        self._learned = None
+        self._warm = {}
         self._n_branches = None
         self._ran = False
         self._timings = BatchTimings()
@@ -81,15 +86,40 @@ class _BatchSweep:
     # -------------------------------------------------------------- options
     @property
     def start(self):
-        """'base' (the converged base case, default), 'flat' (``Vinit``) or
-        'rows' (``set_start_voltages``)."""
+        """'base' (the converged base case, default), 'flat' (``Vinit``),
+        'rows' (``set_start_voltages``) or 'learned' (``set_learned_start``)."""
         return self._start
 
     @start.setter
     def start(self, value):
         if value not in _START:
             raise ValueError(f"Unknown start {value!r}. Choose from: {list(_START)}")
+        if value == "learned" and getattr(self, "_learned", None) is None:
+            raise ValueError("start='learned' needs set_learned_start() first")
         self._start = value
+
+    def set_learned_start(self, learned, refactor_ratio=0.5, max_reuse=6):
+        """Start every row from the voltages ``learned`` (a trained
+        ``warmstart.LearnedStart`` of this grid) predicts for it, on the
+        device, at every ``compute()``; switches ``start`` to 'learned'.
+        A good start leaves only the fast-contracting end of Newton's
+        iteration, so the adaptive strategy may keep one LU longer:
+        ``refactor_ratio`` / ``max_reuse`` apply to learned runs."""
+        if learned.grid.n_bus != self.n_bus:
+            raise ValueError("the learned start belongs to a grid of another size")
+        self._learned = learned
+        self._learned_opts = (float(refactor_ratio), int(max_reuse))
+        self.start = "learned"
+
+    def _row_defs(self):
+        """(sbus_rows or None, trips CSR or None, n_rows) of the current rows."""
+        raise NotImplementedError
+
+    @property
+    def warm_report(self):
+        """Timings of the last learned start: predict_ms (features, network
+        and V0 on the device, wall), n_rescued (rows restarted from Vinit)."""
+        return dict(self._warm)
 
     @property
     def strategy(self):
@@ -129,9 +159,23 @@ class _BatchSweep:
         fixed = self.scheduling == "chunked"
         n_ctas = max(int(batch_size), 0)
         t0 = time.perf_counter()
+        ratio, reuse = float(self.refactor_ratio), int(self.max_reuse)
+        rescue = self._start in ("rows", "learned")
+        if self._start == "learned":
+            import torch
+            sbus, trips, n = self._row_defs()
+            # V0 is written in place into the session's start-row buffer on
+            # torch's stream, which must be done before the session's launch
+            self._learned.start_voltages(sbus, trips, n, out_ptr=self._s.start_rows_buffer(n))
+            torch.cuda.current_stream().synchronize()
+            self._learned.net.check()
+            self._warm = dict(predict_ms=(time.perf_counter() - t0) * 1e3)
+            ratio, reuse = self._learned_opts
         self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False,
-                    _STRATEGY[self._strategy], float(self.refactor_ratio), int(self.max_reuse))
+                    _STRATEGY[self._strategy], ratio, reuse, rescue)
         tm = self._s.timings()
+        if self._start == "learned":
+            self._warm["n_rescued"] = int(tm["n_rescued"])
         self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
                                      t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
                                      t_kernel_ms=tm["kernel_ms"], t_total_ms=(time.perf_counter() - t0) * 1e3)
@@ -224,6 +268,9 @@ class ContingencyAnalysisGPU(_BatchSweep):
     def get_contingencies(self):
         return [list(r) for r in self._ctg]
 
+    def _row_defs(self):
+        return None, self._ctg, len(self._ctg)
+
     @property
     def n_contingencies(self):
         return len(self._ctg)
@@ -235,6 +282,7 @@ class InjectionSweepGPU(_BatchSweep):
     def __init__(self, grid, **kw):
         super().__init__(grid, **kw)
         self._n_scen = 0
+        self._inj = None
 
     def set_injections(self, p_mw, q_mvar, sn_mva):
         """Bus injections in MW / MVAr, (n_scenarios, n_bus); Sbus = (p + jq) / sn_mva
@@ -245,6 +293,13 @@ class InjectionSweepGPU(_BatchSweep):
             raise ValueError("p_mw and q_mvar must both be (n_scenarios, n_bus)")
         self._s.set_injections(p, q, float(sn_mva))
         self._n_scen = p.shape[0]
+        self._inj = (p, q, float(sn_mva))
+
+    def _row_defs(self):
+        if self._inj is None:
+            raise RuntimeError("set_injections() must be called before compute()")
+        p, q, sn = self._inj
+        return (p + 1j * q) / sn, None, self._n_scen
 
     @property
     def n_scenarios(self):
@@ -266,6 +321,12 @@ class ScenarioSweepGPU(InjectionSweepGPU):
         ptr, ids = _ids_csr(rows)
         self._s.set_contingencies(ptr, ids)
         self._topo = rows
+
+    def _row_defs(self):
+        if self._inj is None:
+            raise RuntimeError("set_injections() must be called before compute()")
+        p, q, sn = self._inj
+        return (p + 1j * q) / sn, self._topo, self._n_scen
 
     def get_disconnected(self):
         """(n_rows,) bool: rows whose topology islands the grid (never solved)."""

@@ -261,11 +261,16 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
     const RowEdits ed{s_ne, s_ek, s_ev};
     prof.start();
 
-    int it = 0, status = ROW_MAX_ITER;
-    bool have_factor = false;
-    int since_factor = 0, n_factor = 0;
-    double last_nrm = INFINITY;
+    int it_total = 0, status = ROW_MAX_ITER, n_factor = 0;
     double nrm = NAN;
+    // attempt 0 starts from the row's own start voltage; with a rescue
+    // voltage, a row that ends unconverged there gets one more attempt from
+    // it, with a fresh Newton budget (iterations and factorizations add up)
+    for (int attempt = 0;; ++attempt) {
+    int it = 0;
+    bool have_factor = false;
+    int since_factor = 0;
+    double last_nrm = INFINITY;
     for (;;) {
       // ---- I = Y V (row-patched Ybus) ------------------------------------
       for (int i = tid; i < n; i += BS) {
@@ -472,12 +477,20 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       prof.mark(PH_UPDATE);
       ++it;
     }
+    it_total += it;
+    // status and attempt are block-uniform: the whole CTA restarts or leaves
+    if (status == ROW_CONVERGED || a.fixed_iters || a.rescue_v0 == nullptr || attempt > 0) break;
+    const double2* rv = reinterpret_cast<const double2*>(a.rescue_v0);
+    for (int i = tid; i < n; i += BS) V[i] = rv[i];
+    if (tid == 0 && a.n_rescued != nullptr) atomicAdd(a.n_rescued, 1);
+    __syncthreads();
+    }  // attempts
 
     for (int i = tid; i < n; i += BS) vout[i] = V[i];
     if (tid == 0) {
       a.res_out[row] = nrm;
       a.status_out[row] = status;
-      a.iters_out[row] = it;
+      a.iters_out[row] = it_total;
       if (a.factors_out != nullptr) a.factors_out[row] = n_factor;
     }
     __syncthreads();

@@ -67,6 +67,11 @@ struct SweepArgs {
   double refactor_ratio;  // policy 1: refactor when ||F_k|| > ratio * ||F_{k-1}||
   int max_reuse;          // policy 1: refactor after this many steps on one LU
   int* factors_out;       // [n_rows] LU factorizations per row (nullptr: not recorded)
+  // rescue: a row that ends unconverged (continuous schedule) restarts once
+  // from this complex [n_bus] voltage (nullptr: no rescue); n_rescued counts
+  // the restarts (nullptr: not counted)
+  const double* rescue_v0;
+  int* n_rescued;
   // outputs
   double* v_out;          // [n_rows * n_bus] complex
   double* res_out;        // [n_rows]

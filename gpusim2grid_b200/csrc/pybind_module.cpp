@@ -91,7 +91,7 @@ void check(int rc) {
 
 gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
                         int n_ctas, bool profile = false, int refactor = 0, double refactor_ratio = 0.0,
-                        int max_reuse = 0) {
+                        int max_reuse = 0, bool rescue = false) {
   gs2g_run_opts o{};
   o.max_iter = max_iter;
   o.tol = tol;
@@ -104,6 +104,7 @@ gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precisio
   o.refactor_policy = refactor;
   o.refactor_ratio = refactor_ratio;
   o.max_reuse = max_reuse;
+  o.rescue = rescue ? 1 : 0;
   return o;
 }
 
@@ -203,6 +204,12 @@ class Session {
     check(gs2g_set_start_rows_device(h(), n_rows, reinterpret_cast<const double*>(ptr)));
   }
 
+  uintptr_t start_rows_buffer(int n_rows) {
+    double* p = nullptr;
+    check(gs2g_start_rows_buffer(h(), n_rows, &p));
+    return reinterpret_cast<uintptr_t>(p);
+  }
+
   void set_sbus(CArr sbus) {
     if (sbus.size() != n_bus_) throw py::value_error("Sbus must have n_bus entries");
     check(gs2g_set_sbus(h(), reinterpret_cast<const double*>(sbus.data())));
@@ -236,9 +243,9 @@ class Session {
   }
 
   void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas,
-           bool profile, int refactor, double refactor_ratio, int max_reuse) {
+           bool profile, int refactor, double refactor_ratio, int max_reuse, bool rescue) {
     gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                                refactor_ratio, max_reuse);
+                                refactor_ratio, max_reuse, rescue);
     int rc;
     {
       py::gil_scoped_release nogil;
@@ -313,6 +320,7 @@ class Session {
     }
     d["phase_cycles"] = pc;
     d["phase_share"] = ps;
+    d["n_rescued"] = t.n_rescued;
     return d;
   }
 
@@ -372,6 +380,55 @@ py::dict plan_info(int n_bus, IArr indptr, IArr indices, IArr pv, IArr pq, int t
   return d;
 }
 
+// ---- warm-start MLP: raw device pointers (integers) from the caller's tensors
+template <class T>
+T* P(uintptr_t p) {
+  return reinterpret_cast<T*>(p);
+}
+void* S(uintptr_t stream) { return reinterpret_cast<void*>(stream); }
+
+void bind_mlp(py::module_& m) {
+  auto mm = m.def_submodule("mlp", "warm-start MLP device routines (include/gs2g.h, gs2g_mlp_*)");
+  mm.def("gemm_tn_bf16", [](uintptr_t A, int lda, uintptr_t B, int ldb, uintptr_t D, int ldd, int M, int N, int K,
+                            bool accumulate, uintptr_t err, uintptr_t stream) {
+    check(gs2g_mlp_gemm_tn_bf16(P<void>(A), lda, P<void>(B), ldb, P<float>(D), ldd, M, N, K, accumulate ? 1 : 0,
+                                P<int>(err), S(stream)));
+  });
+  mm.def("bias_act", [](uintptr_t pre, int ldp, uintptr_t bias, uintptr_t act, int lda, int rows, int cols, bool gelu,
+                        uintptr_t stream) {
+    check(gs2g_mlp_bias_act(P<float>(pre), ldp, P<float>(bias), P<void>(act), lda, rows, cols, gelu ? 1 : 0,
+                            S(stream)));
+  });
+  mm.def("gelu_bwd", [](uintptr_t dact, int ldg, uintptr_t pre, int ldp, uintptr_t dpre, int ldo, int rows, int cols,
+                        uintptr_t stream) {
+    check(gs2g_mlp_gelu_bwd(P<float>(dact), ldg, P<float>(pre), ldp, P<void>(dpre), ldo, rows, cols, S(stream)));
+  });
+  mm.def("mse_grad", [](uintptr_t y, uintptr_t t, int ld, uintptr_t dy, int rows, int cols, int cols_valid,
+                        float scale, uintptr_t loss, uintptr_t stream) {
+    check(gs2g_mlp_mse_grad(P<float>(y), P<float>(t), ld, P<void>(dy), rows, cols, cols_valid, scale, P<float>(loss),
+                            S(stream)));
+  });
+  mm.def("colsum_bf16", [](uintptr_t x, int ld, int rows, int cols, uintptr_t out, uintptr_t stream) {
+    check(gs2g_mlp_colsum_bf16(P<void>(x), ld, rows, cols, P<float>(out), S(stream)));
+  });
+  mm.def("transpose_bf16", [](uintptr_t in, int ldi, uintptr_t out, int ldo, int rows, int cols, uintptr_t stream) {
+    check(gs2g_mlp_transpose_bf16(P<void>(in), ldi, P<void>(out), ldo, rows, cols, S(stream)));
+  });
+  mm.def("to_bf16", [](uintptr_t in, uintptr_t out, int64_t n, uintptr_t stream) {
+    check(gs2g_mlp_to_bf16(P<float>(in), P<void>(out), n, S(stream)));
+  });
+  mm.def("adam", [](uintptr_t w, uintptr_t g, uintptr_t mo, uintptr_t v, uintptr_t wb, int64_t n, float lr,
+                    float b1, float b2, float eps, int step, float wd, uintptr_t stream) {
+    check(gs2g_mlp_adam(P<float>(w), P<float>(g), P<float>(mo), P<float>(v), P<void>(wb), n, lr, b1, b2, eps, step,
+                        wd, S(stream)));
+  });
+  mm.def("start_voltages", [](uintptr_t y, int ldy, uintptr_t ymean, uintptr_t ystd, uintptr_t ia, uintptr_t im,
+                              uintptr_t vinit, int n_bus, uintptr_t v0, int rows, uintptr_t stream) {
+    check(gs2g_mlp_start_voltages(P<float>(y), ldy, P<float>(ymean), P<float>(ystd), P<int>(ia), P<int>(im),
+                                  P<double>(vinit), n_bus, P<double>(v0), rows, S(stream)));
+  });
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_gs2g, m) {
@@ -388,6 +445,7 @@ PYBIND11_MODULE(_gs2g, m) {
   m.def("version", &gs2g_version);
   m.def("max_edits_per_row", &gs2g_max_edits_per_row);
   m.def("acpf_nr", &acpf_nr);
+  bind_mlp(m);
   py::class_<Session>(m, "Session")
       .def(py::init<int, int, IArr, IArr, CArr, CArr, CArr, IArr, IArr, int>(), py::arg("device"), py::arg("n_bus"),
            py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),
@@ -402,13 +460,15 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("clear_injections", &Session::clear_injections)
       .def("set_start_rows", &Session::set_start_rows)
       .def("set_start_rows_device", &Session::set_start_rows_device)
+      .def("start_rows_buffer", &Session::start_rows_buffer)
       .def("set_sbus", &Session::set_sbus)
       .def("set_vinit", &Session::set_vinit)
       .def("solve_base", &Session::solve_base)
       .def("set_base_v", &Session::set_base_v)
       .def("run", &Session::run, py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"), py::arg("precision"),
            py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false,
-           py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0)
+           py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
+           py::arg("rescue") = false)
       .def("factor_counts", &Session::factor_counts)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)

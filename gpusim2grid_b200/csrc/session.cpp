@@ -287,7 +287,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
   s->d_ws.ensure((size_t)wsb * n_ctas);
-  s->d_queue.ensure(sizeof(int));
+  s->d_queue.ensure(2 * sizeof(int));  // [0] row queue, [1] rescue count
   gs2g::SweepArgs a{};
   a.n_rows = n_rows;
   a.ybus = s->d_ybus.as<double>();
@@ -316,13 +316,16 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
   a.factors_out = out.factors;
+  const bool rescue = o.rescue != 0 && v0_stride != 0 && !o.fixed_iters;
+  a.rescue_v0 = rescue ? s->d_vinit.as<double>() : nullptr;
+  a.n_rescued = s->d_queue.as<int>() + 1;
   a.phase_cycles = nullptr;
   if (o.profile_phases) {
     s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
     ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
     a.phase_cycles = s->d_phase.as<unsigned long long>();
   }
-  ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");
@@ -330,6 +333,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   float ms = 0;
   ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
   for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
+  ck(cudaMemcpy(&s->tm.n_rescued, s->d_queue.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost), "rescue count");
   if (o.profile_phases) {
     unsigned long long c[gs2g::N_PHASES];
     ck(cudaMemcpy(c, s->d_phase.p, sizeof(c), cudaMemcpyDeviceToHost), "read phases");
@@ -342,6 +346,15 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   }
   return ms;
 }
+
+}  // namespace
+
+namespace gs2g {
+// last-error text for the MLP entry points (mlp_kernels.cu)
+void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
+}  // namespace gs2g
+
+namespace {
 
 int fail(const std::exception& e) {
   g_err = e.what();
@@ -624,6 +637,16 @@ int gs2g_set_start_rows_device(gs2g_session* s, int n_rows, const double* v0_dev
   GS2G_CATCH
 }
 
+int gs2g_start_rows_buffer(gs2g_session* s, int n_rows, double** v0_dev) {
+  GS2G_TRY
+  if (!s || n_rows < 0 || !v0_dev) throw std::invalid_argument("start_rows_buffer: bad arguments");
+  DeviceGuard g(s->device);
+  s->d_v0rows.ensure((size_t)std::max(n_rows, 1) * s->n_bus * 2 * sizeof(double));
+  s->n_start = n_rows;
+  *v0_dev = s->d_v0rows.as<double>();
+  GS2G_CATCH
+}
+
 int gs2g_set_sbus(gs2g_session* s, const double* sbus) {
   GS2G_TRY
   if (!s || !sbus) throw std::invalid_argument("set_sbus: bad arguments");
@@ -837,6 +860,7 @@ int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, i
   a.status_out = status;
   a.iters_out = iters;
   a.pivot_floor = o->pivot_floor;
+  if (o->rescue != 0 && v0_stride != 0 && !o->fixed_iters) a.rescue_v0 = s->d_vinit.as<double>();
   int used = 0;
   ck((cudaError_t)gs2g::launch_sweep_static(s->dplan, a, o->precision, s->device, stream, &used),
      "allocation-free sweep launch");

@@ -86,6 +86,12 @@ typedef struct gs2g_run_opts {
   int refactor_policy;
   double refactor_ratio; /* adaptive: <= 0 selects 0.3 */
   int max_reuse;         /* adaptive: <= 0 selects 3 */
+  /* 1: with GS2G_START_ROWS and the continuous schedule, a row that ends
+   * unconverged (MAX_ITER or DIVERGED) from its given start restarts once
+   * from Vinit inside the same launch, with a fresh max_iter budget; its
+   * iteration and factorization counts include both attempts.  Guards a
+   * learned or otherwise predicted start against a bad prediction. */
+  int rescue;
 } gs2g_run_opts;
 
 #define GS2G_REFACTOR_EVERY 0
@@ -103,6 +109,7 @@ typedef struct gs2g_timings {
    * phase's share of their total */
   double phase_cycles[GS2G_N_PHASES];
   double phase_share[GS2G_N_PHASES];
+  int n_rescued; /* rows of the last run restarted from Vinit (gs2g_run_opts.rescue) */
 } gs2g_timings;
 
 const char* gs2g_last_error(void);
@@ -138,6 +145,13 @@ int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const d
 int gs2g_set_start_rows(gs2g_session* s, int n_rows, const double* v0);
 /* Same, from device memory already on the session's device. */
 int gs2g_set_start_rows_device(gs2g_session* s, int n_rows, const double* v0_dev);
+/* The session's own start-row buffer, complex [n_rows x n_bus] on its
+ * device, for callers that compute start voltages on the GPU and write them
+ * in place (no copy).  Sizes the buffer and records n_rows start rows; its
+ * contents are used by the next GS2G_START_ROWS run, so the caller's writes
+ * must be complete (its stream synchronised) before gs2g_run.  Valid until
+ * the next call that sets start rows or destroy. */
+int gs2g_start_rows_buffer(gs2g_session* s, int n_rows, double** v0_dev);
 /* Replace the base injections (single-solve resolve). */
 int gs2g_set_sbus(gs2g_session* s, const double* sbus);
 /* Replace Vinit. */
@@ -180,10 +194,55 @@ int gs2g_sync(gs2g_session* s);
  *   The first call on a device looks up the array's device address (make it
  *   before any stream capture).  Every call shares the array: calls that
  *   overlap on the GPU race.  Returns once the work is enqueued on `stream`
- *   (NULL = default stream); synchronise it before reading the outputs. */
+ *   (NULL = default stream); synchronise it before reading the outputs.
+ *   The rescue option restarts from the session's Vinit; its count is not
+ *   recorded (gs2g_timings is not touched). */
 int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, int64_t v0_stride,
                           const double* sbus, int64_t sbus_stride, const gs2g_run_opts* o, double* v_out,
                           double* residuals, int* status, int* iters, void* stream);
+
+/* ---- Warm-start MLP building blocks ------------------------------------
+ * The learned start voltage (the reference's ScenarioSweepGPU warm_start
+ * slot, src/gpusim2grid/scenario_sweep/gpu_facade.py, which takes any
+ * per-row V0) is produced by an MLP trained and evaluated with these device
+ * routines.  All pointers are device memory on the current device; `stream`
+ * NULL = default stream; each call only enqueues work.  bf16 arrays are
+ * passed as void*.  Row-major matrices, `ld*` in elements.
+ *
+ * D[M x N] (fp32) = A[M x K] . B[N x K]^T (+ D when accumulate), A, B bf16,
+ * on tcgen05 tensor cores.  M, N multiples of 128, K of 64; lda, ldb
+ * multiples of 8, ldd of 4; 16-byte aligned bases.  *err is set to 1 if a
+ * bounded wait inside the kernel ran out (the tile is then not written). */
+int gs2g_mlp_gemm_tn_bf16(const void* A, int lda, const void* B, int ldb, float* D, int ldd, int M, int N, int K,
+                          int accumulate, int* err, void* stream);
+/* pre += bias (per column); act = bf16(gelu(pre)) (exact erf GELU) or
+ * bf16(pre) when gelu = 0; act may be NULL. */
+int gs2g_mlp_bias_act(float* pre, int ldp, const float* bias, void* act_bf16, int lda, int rows, int cols, int gelu,
+                      void* stream);
+/* dpre = bf16(dact * gelu'(pre)) */
+int gs2g_mlp_gelu_bwd(const float* dact, int ldg, const float* pre, int ldp, void* dpre_bf16, int ldo, int rows,
+                      int cols, void* stream);
+/* dy = bf16(scale * (y - t)) on the first cols_valid columns, 0 on the rest;
+ * *loss += sum of (y - t)^2 over the valid entries (loss may be NULL). */
+int gs2g_mlp_mse_grad(const float* y, const float* t, int ld, void* dy_bf16, int rows, int cols, int cols_valid,
+                      float scale, float* loss, void* stream);
+/* out[c] = sum over rows of x[r][c] (bf16 in, fp32 out) */
+int gs2g_mlp_colsum_bf16(const void* x, int ld, int rows, int cols, float* out, void* stream);
+/* out[c][r] = in[r][c] (bf16) */
+int gs2g_mlp_transpose_bf16(const void* in, int ldi, void* out, int ldo, int rows, int cols, void* stream);
+/* out = bf16(in), n elements */
+int gs2g_mlp_to_bf16(const float* in, void* out, int64_t n, void* stream);
+/* One Adam step (bias-corrected, step >= 1, L2 weight decay added to the
+ * gradient) on fp32 master weights; also writes their bf16
+ * copy when w_bf16 is not NULL. */
+int gs2g_mlp_adam(float* w, const float* g, float* m, float* v, void* w_bf16, int64_t n, float lr, float beta1,
+                  float beta2, float eps, int step, float weight_decay, void* stream);
+/* Start voltages from the network's standardised outputs y[rows x ldy]:
+ * bus b takes Va = y[va_index[b]] * y_std + y_mean when va_index[b] >= 0
+ * (pv and pq buses), else the angle of vinit[b]; Vm likewise through
+ * vm_index (pq buses), else |vinit[b]|.  v0 = complex [rows x n_bus]. */
+int gs2g_mlp_start_voltages(const float* y, int ldy, const float* y_mean, const float* y_std, const int* va_index,
+                            const int* vm_index, const double* vinit, int n_bus, double* v0, int rows, void* stream);
 
 /* acpf_nr_gpu: one solve from Vinit, V written back into `v_inout`.
  * Returns the status through *converged (1/0), *iters and *residual. */

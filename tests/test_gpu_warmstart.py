@@ -1,0 +1,97 @@
+"""Learned warm start end to end on the GPU: train the MLP on GPU-solved
+operating points of the 118-bus grid, then run the N-1 sweep from its
+predictions.  The answers must equal the flat-start FP64 answers within the
+mixed-precision bar, and the learned start must take fewer Newton steps and
+LU factorizations than a flat start.  A start that fails is restarted from
+Vinit inside the same launch."""
+
+import numpy as np
+import pytest
+
+from conftest import TOL_V_MIXED
+from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, RowStatus
+from gpusim2grid_b200.synthetic import injection_scenarios, n1_branches
+from oracle import nr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def learned118(g118):
+    from gpusim2grid_b200.warmstart import LearnedStart
+    ls = LearnedStart(g118, hidden=256, layers=2, seed=0)
+    rep = ls.train(n_rows=16384, epochs=30, batch=512, lr=1e-3, lr_decay=0.9, seed=1)
+    assert rep["n_unconverged"] == 0
+    assert rep["loss"][-1] < 0.1 * rep["loss"][0]
+    return ls
+
+
+def _sweep(g, precision, start, learned=None):
+    ca = ContingencyAnalysisGPU(g.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
+                                scheduling="continuous", tol=1e-8, start="flat", strategy="adaptive")
+    ca.set_branch_data(*g.branch_data())
+    ca.add_contingencies_by_branch_id([[int(b)] for b in n1_branches(g)])
+    if learned is not None:
+        ca.set_learned_start(learned)
+    ca.start = start
+    ca.compute()
+    return ca
+
+
+def test_learned_start_n1_parity_and_fewer_steps(g118, learned118):
+    ref = _sweep(g118, "fp64", "flat")
+    flat = _sweep(g118, "mixed", "flat")
+    warm = _sweep(g118, "mixed", "learned", learned118)
+    assert np.all(ref.get_row_status() == RowStatus.CONVERGED)
+    assert np.all(warm.get_row_status() == RowStatus.CONVERGED)
+    assert np.all(warm.last_residuals() < 1e-8)
+    assert np.abs(warm.V_results - ref.V_results).max() < TOL_V_MIXED
+    assert warm.get_row_iterations().sum() < flat.get_row_iterations().sum()
+    assert warm.get_row_factorizations().sum() < flat.get_row_factorizations().sum()
+    assert warm.warm_report["n_rescued"] == 0
+    # a sample against the FP64 oracle as well
+    rows = n1_branches(g118)
+    sample = np.random.default_rng(3).choice(len(rows), 8, replace=False)
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vo, so, _, _ = O.contingency_sweep(Y, V0, S, pv, pq, [[int(rows[r])] for r in sample], g118.branch_from,
+                                       g118.branch_to, g118.yff, g118.yft, g118.ytf, g118.ytt, 10, 1e-8)
+    assert np.all(so == O.CONVERGED)
+    assert np.abs(warm.V_results[sample] - Vo).max() < TOL_V_MIXED
+
+
+def test_learned_start_injection_rows(g118, learned118):
+    p, q = injection_scenarios(g118, 512, seed=11)
+    out = []
+    for start in ("flat", "learned"):
+        sw = InjectionSweepGPU(g118.as_tuple(), init_from_n_powerflow=False, precision="mixed", nb_iter=10,
+                               scheduling="continuous", start="flat", strategy="adaptive")
+        sw.set_injections(p, q, g118.sn_mva)
+        if start == "learned":
+            sw.set_learned_start(learned118)
+        sw.compute()
+        out.append(sw)
+    flat, warm = out
+    assert np.all(warm.get_row_status() == RowStatus.CONVERGED)
+    assert np.abs(warm.V_results - flat.V_results).max() < TOL_V_MIXED
+    assert warm.get_row_iterations().sum() < flat.get_row_iterations().sum()
+
+
+def test_failed_start_rows_are_rescued_from_vinit(g118):
+    """Half the rows get a NaN start (their mismatch is NaN, so they end
+    DIVERGED at step 0); the kernel restarts exactly those from Vinit in the
+    same launch, and every row matches the flat-start run."""
+    p, q = injection_scenarios(g118, 64, seed=4)
+    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", start="flat")
+    flat = InjectionSweepGPU(g118.as_tuple(), **kw)
+    flat.set_injections(p, q, g118.sn_mva)
+    flat.compute()
+    sw = InjectionSweepGPU(g118.as_tuple(), **kw)
+    sw.set_injections(p, q, g118.sn_mva)
+    V0 = np.tile(g118.vinit(), (64, 1))
+    V0[::2] = np.nan
+    sw.set_start_voltages(V0)
+    sw.compute()
+    assert sw.session.timings()["n_rescued"] == 32
+    assert np.all(sw.get_row_status() == RowStatus.CONVERGED)
+    np.testing.assert_array_equal(sw.get_row_iterations(), flat.get_row_iterations())
+    assert np.abs(sw.V_results - flat.V_results).max() < TOL_V_MIXED

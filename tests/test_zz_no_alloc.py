@@ -28,7 +28,7 @@ class RunOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("tol", ctypes.c_double), ("fixed_iters", ctypes.c_int),
                 ("precision", ctypes.c_int), ("start", ctypes.c_int), ("pivot_floor", ctypes.c_double),
                 ("n_ctas", ctypes.c_int), ("profile_phases", ctypes.c_int), ("refactor_policy", ctypes.c_int),
-                ("refactor_ratio", ctypes.c_double), ("max_reuse", ctypes.c_int)]
+                ("refactor_ratio", ctypes.c_double), ("max_reuse", ctypes.c_int), ("rescue", ctypes.c_int)]
 
 
 def _capi():
@@ -64,7 +64,7 @@ def test_noalloc_matches_regular_entry_point(precision, tol_v):
     sbus = torch.from_numpy(((p + 1j * q) / g.sn_mva).astype(np.complex128)).to(dev)
     capi = _capi()
     opts = RunOpts(max_iter=10, tol=1e-8, fixed_iters=0, precision=precision, start=0, pivot_floor=0.0, n_ctas=0,
-                   profile_phases=0, refactor_policy=0, refactor_ratio=0.0, max_reuse=0)
+                   profile_phases=0, refactor_policy=0, refactor_ratio=0.0, max_reuse=0, rescue=0)
     for call in range(2):
         v_out = torch.full((n, g.n_bus), complex("nan+nanj"), dtype=torch.complex128, device=dev)
         res = torch.full((n,), -1.0, dtype=torch.float64, device=dev)
