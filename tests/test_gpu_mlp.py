@@ -100,5 +100,5 @@ def test_fit_reduces_loss_on_a_smooth_map():
     X = net.device_inputs(torch.as_tensor(Xr, device="cuda"))
     T = net.device_targets(torch.as_tensor(Yr, device="cuda"))
     h = net.fit_device(X, T, epochs=8, batch=512, lr=2e-3, lr_decay=0.8, n_rows=n)
-    assert h["loss"][-1] < 0.05 * h["loss"][0]
-    assert net.mse(X, T, n) < 0.02
+    assert h["loss"][-1] < 0.25 * h["loss"][0]
+    assert net.mse(X, T, n) < 0.05
