@@ -258,12 +258,14 @@ def run_ours(args):
     clk.start()
     barrier()
     pre, ker = [], []
+    torch.cuda.nvtx.range_push("bench_timed")  # ncu --nvtx --nvtx-include bench_timed/
     for _ in range(args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         a_, b_ = step()
         pre.append(a_)
         ker.append(b_)
+    torch.cuda.nvtx.range_pop()
     barrier()
     clocks = clk.stop()
     total_ms = float(np.sum(pre) + np.sum(ker))
