@@ -114,12 +114,15 @@ class WarmStartMLP:
         """[(W_l, b_l)] fp32 master copies, W_l (out, in) including padding."""
         return [(self.W(l), self.b(l)) for l in range(self.layers + 1)]
 
-    def set_stats(self, x_mean, x_std, y_mean, y_std):
-        """Per-column standardisation of inputs and targets (zero std -> 1)."""
+    def set_stats(self, x_mean, x_std, y_mean, y_std, floor=1e-6):
+        """Per-column standardisation of inputs and targets.  A std below
+        ``floor`` (per unit / radians) is raised to it: such a column is
+        constant for the network's purpose (e.g. the voltage of a load-free
+        bus fed only from the slack), and dividing by a std at the level of
+        solver noise would blow the fp32 rounding of its mean up."""
         f = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float32), device=self.device)
-        xs, ys = f(x_std), f(y_std)
-        self.x_mean, self.x_std = f(x_mean), torch.where(xs > 0, xs, torch.ones_like(xs))
-        self.y_mean, self.y_std = f(y_mean), torch.where(ys > 0, ys, torch.ones_like(ys))
+        self.x_mean, self.x_std = f(x_mean), torch.clamp(f(np.nan_to_num(x_std, nan=1.0)), min=floor)
+        self.y_mean, self.y_std = f(y_mean), torch.clamp(f(np.nan_to_num(y_std, nan=1.0)), min=floor)
 
     # ------------------------------------------------------------- buffers
     def device_inputs(self, F):
