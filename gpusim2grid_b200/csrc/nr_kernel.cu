@@ -80,10 +80,53 @@ __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
 }
 
 // Dense unit-lower forward solve y <- L^{-1} y and upper backward solve
-// y <- U^{-1} y on the tail (y is the tail part of the solve vector).
+// y <- U^{-1} y on the tail (yg: the tail part of the solve vector).  The
+// tail is processed in 32-wide column blocks: warp 0 solves the diagonal
+// block, then every other row of the block column takes a rank-32 update
+// as a dot product, one warp per row with the lanes along the block's
+// columns (one coalesced 128-byte load per row), four rows in flight per
+// warp.  y lives in ys (shared memory when it fits, else ys == yg).
 template <typename T>
-__device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ y, T* s_blk) {
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void block_column_update(const T* __restrict__ A, int ld, int c0, int cb, int r0, int r1,
+                                                    const T* s_blk, T* ys) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T xb = lane < cb ? s_blk[lane] : T(0);
+  const int col = c0 + (lane < cb ? lane : 0);
+  int i = r0 + warp;
+  for (; i + 3 * NWARP < r1; i += 4 * NWARP) {
+    const T a0 = A[(int64_t)i * ld + col];
+    const T a1 = A[(int64_t)(i + NWARP) * ld + col];
+    const T a2 = A[(int64_t)(i + 2 * NWARP) * ld + col];
+    const T a3 = A[(int64_t)(i + 3 * NWARP) * ld + col];
+    const T p0 = warp_sum(a0 * xb), p1 = warp_sum(a1 * xb);
+    const T p2 = warp_sum(a2 * xb), p3 = warp_sum(a3 * xb);
+    if (lane == 0) {
+      ys[i] -= p0;
+      ys[i + NWARP] -= p1;
+      ys[i + 2 * NWARP] -= p2;
+      ys[i + 3 * NWARP] -= p3;
+    }
+  }
+  for (; i < r1; i += NWARP) {
+    const T p = warp_sum(A[(int64_t)i * ld + col] * xb);
+    if (lane == 0) ys[i] -= p;
+  }
+}
+
+template <typename T>
+__device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ yg, T* s_blk, T* ys) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (ys != yg) {
+    for (int i = tid; i < n; i += BS) ys[i] = yg[i];
+    __syncthreads();
+  }
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int cb = min(32, n - c0);
     if (warp == 0) {
@@ -92,24 +135,19 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
       const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
 #pragma unroll
       for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c < lane) ? rp[c] : T(0);
-      T v = lane < cb ? y[c0 + lane] : T(0);
+      T v = lane < cb ? ys[c0 + lane] : T(0);
 #pragma unroll
       for (int c = 0; c < 32; ++c) {
         const T yc = __shfl_sync(0xffffffffu, v, c);
         v = fma(-arow[c], yc, v);
       }
       if (lane < cb) {
-        y[c0 + lane] = v;
+        ys[c0 + lane] = v;
         s_blk[lane] = v;
       }
     }
     __syncthreads();
-    for (int i = c0 + cb + tid; i < n; i += BS) {
-      const T* row = A + (int64_t)i * ld + c0;
-      T acc = y[i];
-      for (int c = 0; c < cb; ++c) acc -= row[c] * s_blk[c];
-      y[i] = acc;
-    }
+    block_column_update<T>(A, ld, c0, cb, c0 + cb, n, s_blk, ys);
     __syncthreads();
   }
   const int nblk = (n + 31) / 32;
@@ -121,7 +159,7 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
       const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
 #pragma unroll
       for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c >= lane && c < cb) ? rp[c] : T(lane == c ? 1 : 0);
-      T v = lane < cb ? y[c0 + lane] : T(0);
+      T v = lane < cb ? ys[c0 + lane] : T(0);
 #pragma unroll
       for (int c = 31; c >= 0; --c) {
         T xc = v / arow[c];  // meaningful on lane c only
@@ -130,17 +168,16 @@ __device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restri
         else if (lane < c) v = fma(-arow[c], xc, v);
       }
       if (lane < cb) {
-        y[c0 + lane] = v;
+        ys[c0 + lane] = v;
         s_blk[lane] = v;
       }
     }
     __syncthreads();
-    for (int i = tid; i < c0; i += BS) {
-      const T* row = A + (int64_t)i * ld + c0;
-      T acc = y[i];
-      for (int c = 0; c < cb; ++c) acc -= row[c] * s_blk[c];
-      y[i] = acc;
-    }
+    block_column_update<T>(A, ld, c0, cb, 0, c0, s_blk, ys);
+    __syncthreads();
+  }
+  if (ys != yg) {
+    for (int i = tid; i < n; i += BS) yg[i] = ys[i];
     __syncthreads();
   }
 }
@@ -448,7 +485,8 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         y[i] = acc;
       }
       __syncthreads();
-      if (P.nt > 0) dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk);
+      if (P.nt > 0)
+        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, P.nt <= dense::Smem<T>::elems ? s_dense : y + P.p);
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int k = P.lev_piv[q0];
