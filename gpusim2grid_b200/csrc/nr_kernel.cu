@@ -83,40 +83,46 @@ __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
 // y <- U^{-1} y on the tail (yg: the tail part of the solve vector).  The
 // tail is processed in 32-wide column blocks: warp 0 solves the diagonal
 // block, then every other row of the block column takes a rank-32 update
-// as a dot product, one warp per row with the lanes along the block's
-// columns (one coalesced 128-byte load per row), four rows in flight per
-// warp.  y lives in ys (shared memory when it fits, else ys == yg).
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
+// as a dot product, one thread per row reading its 32 values with 16-byte
+// vector loads (rows are 16-byte aligned: ld is a multiple of 8 and block
+// columns start at multiples of 32).  y lives in ys (shared memory when it
+// fits, else ys == yg).
 template <typename T>
 __device__ __forceinline__ void block_column_update(const T* __restrict__ A, int ld, int c0, int cb, int r0, int r1,
                                                     const T* s_blk, T* ys) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T xb = lane < cb ? s_blk[lane] : T(0);
-  const int col = c0 + (lane < cb ? lane : 0);
-  int i = r0 + warp;
-  for (; i + 3 * NWARP < r1; i += 4 * NWARP) {
-    const T a0 = A[(int64_t)i * ld + col];
-    const T a1 = A[(int64_t)(i + NWARP) * ld + col];
-    const T a2 = A[(int64_t)(i + 2 * NWARP) * ld + col];
-    const T a3 = A[(int64_t)(i + 3 * NWARP) * ld + col];
-    const T p0 = warp_sum(a0 * xb), p1 = warp_sum(a1 * xb);
-    const T p2 = warp_sum(a2 * xb), p3 = warp_sum(a3 * xb);
-    if (lane == 0) {
-      ys[i] -= p0;
-      ys[i + NWARP] -= p1;
-      ys[i + 2 * NWARP] -= p2;
-      ys[i + 3 * NWARP] -= p3;
+  for (int i = r0 + (int)threadIdx.x; i < r1; i += BS) {
+    const T* row = A + (int64_t)i * ld + c0;
+    T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
+    if (cb == 32) {
+      if constexpr (sizeof(T) == 4) {
+        const float4* r4 = reinterpret_cast<const float4*>(row);
+        float4 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = r4[q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          acc0 = fma(v[q].x, s_blk[4 * q], acc0);
+          acc1 = fma(v[q].y, s_blk[4 * q + 1], acc1);
+          acc2 = fma(v[q].z, s_blk[4 * q + 2], acc2);
+          acc3 = fma(v[q].w, s_blk[4 * q + 3], acc3);
+        }
+      } else {
+        const double2* r2 = reinterpret_cast<const double2*>(row);
+        double2 v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = r2[q];
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          acc0 = fma(v[q].x, s_blk[2 * q], acc0);
+          acc1 = fma(v[q].y, s_blk[2 * q + 1], acc1);
+          acc2 = fma(v[q + 1].x, s_blk[2 * q + 2], acc2);
+          acc3 = fma(v[q + 1].y, s_blk[2 * q + 3], acc3);
+        }
+      }
+    } else {
+      for (int c = 0; c < cb; ++c) acc0 = fma(row[c], s_blk[c], acc0);
     }
-  }
-  for (; i < r1; i += NWARP) {
-    const T p = warp_sum(A[(int64_t)i * ld + col] * xb);
-    if (lane == 0) ys[i] -= p;
+    ys[i] -= (acc0 + acc1) + (acc2 + acc3);
   }
 }
 
