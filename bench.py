@@ -43,8 +43,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "n1_sweep_case2000_synth"
-GRID = "case2000_synth"
+# name -> (grid, row kind, rows, scenario seed, training-row mix)
+WORKLOADS = {
+    # every non-islanding single outage of the 2000-bus grid at base injections
+    "n1_sweep_case2000_synth": ("case2000_synth", "n1", None, None, dict(broad=0.5)),
+    # 4096 load-scaling scenarios (global U(0.8,1.2) x per-bus lognormal(0,0.1)) on the 6500-bus grid
+    "injection_sweep_case6500_synth": ("case6500_synth", "injection", 4096, 1, dict(broad=1.0, p_outage=0.0)),
+    # 16384 rows on the 2000-bus grid, each a load-scaling scenario plus one single outage
+    "injection_n1_case2000_synth": ("case2000_synth", "injection_n1", 16384, 1, dict(broad=1.0, p_outage=0.9)),
+}
 MAX_ITER, TOL = 10, 1e-8
 METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
 
@@ -61,6 +68,7 @@ def _args():
     ap.add_argument("--cpu-sample-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="n1_sweep_case2000_synth")
     ap.add_argument("--start", choices=["learned", "flat"], default="learned",
                     help="learned: MLP warm start (trained untimed before the run); flat: Vinit")
     ap.add_argument("--train-rows", type=int, default=100000)
@@ -76,40 +84,58 @@ def _dist():
     return rank, world, local
 
 
-def _workload():
-    from gpusim2grid_b200.synthetic import grid_by_name, n1_branches
-    g = grid_by_name(GRID, 0)
-    rows = [[int(b)] for b in n1_branches(g)]
-    return g, rows
+def _workload(name):
+    """(grid, trips or None, p_mw or None, q_mvar or None) of a named workload."""
+    from gpusim2grid_b200.synthetic import grid_by_name, injection_scenarios, n1_branches
+    gname, kind, n_rows, seed, _ = WORKLOADS[name]
+    g = grid_by_name(gname, 0)
+    cand = n1_branches(g)
+    if kind == "n1":
+        return g, [[int(b)] for b in cand], None, None
+    p, q = injection_scenarios(g, n_rows, seed=seed)
+    if kind == "injection":
+        return g, None, p, q
+    return g, [[int(cand[r % cand.size])] for r in range(n_rows)], p, q
 
 
 # ---------------------------------------------------------------- CPU side
 def _cpu_rows(args_tuple):
-    from oracle.nr_oracle import contingency_sweep
+    """Oracle NR over rows given as (tripped branches, Sbus row or None)."""
+    from oracle import nr_oracle as O
     (Y, V0, S, pv, pq, rows, f, t, yff, yft, ytf, ytt) = args_tuple
-    Vs, st, it, res = contingency_sweep(Y, V0, S, pv, pq, rows, f, t, yff, yft, ytf, ytt, MAX_ITER, TOL)
-    return int((st == 0).sum()), int(it.sum())
+    conv = iters = 0
+    for trips, sb in rows:
+        Yr = O.trip_branches(Y, trips, f, t, yff, yft, ytf, ytt) if trips else Y
+        _, st, it, _ = O.nr_solve(Yr, V0, S if sb is None else sb, pv, pq, MAX_ITER, TOL)
+        conv += int(st == O.CONVERGED)
+        iters += int(it)
+    return conv, iters
 
 
-def cpu_baseline(g, rows, n_rows_sample, cores=None):
-    """Time the oracle port (FP64 NR, scipy SuperLU) over a sample of rows on
-    `cores` worker processes (spawned).  Returns (solves/s, cores, sample)."""
+def cpu_baseline(g, trips, p, q, n_rows_sample, cores=None):
+    """Time the oracle port (FP64 NR from flat, scipy SuperLU) over an evenly
+    spaced sample of the workload's rows on `cores` spawned worker
+    processes.  Returns (solves/s, cores, sample description)."""
     import multiprocessing as mp
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     cores = cores or os.cpu_count() or 1
     Y, V0, S, _, _, pv, pq = g.as_tuple()
-    sample = rows[:: max(1, len(rows) // n_rows_sample)][:n_rows_sample]
-    chunks = [sample[i::cores] for i in range(cores)]
+    n = len(trips) if trips is not None else p.shape[0]
+    idx = list(range(0, n, max(1, n // n_rows_sample)))[:n_rows_sample]
+    rows = [((trips[r] if trips is not None else []),
+             (None if p is None else (p[r] + 1j * q[r]) / g.sn_mva)) for r in idx]
+    chunks = [rows[i::cores] for i in range(cores)]
     payload = [(Y, V0, S, pv, pq, c, g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt) for c in chunks if c]
     ctx = mp.get_context("spawn")
     with ctx.Pool(len(payload)) as pool:
-        pool.map(_cpu_rows, payload[:1])  # warm the workers' imports
+        pool.map(_cpu_rows, [(Y, V0, S, pv, pq, rows[:1], g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt)]
+                 * len(payload))  # warm every worker's imports
         t0 = time.perf_counter()
         out = pool.map(_cpu_rows, payload)
         dt = time.perf_counter() - t0
     conv = sum(o[0] for o in out)
-    return conv / dt, len(payload), f"{len(sample)} of {len(rows)} N-1 rows, flat start, scipy SuperLU FP64 NR"
+    return conv / dt, len(payload), f"{len(rows)} of {n} rows (evenly spaced), flat start, scipy SuperLU FP64 NR"
 
 
 # ---------------------------------------------------------------- clocks
@@ -183,8 +209,41 @@ def algorithmic_flops(info):
 def _train_learned(g, args, device):
     from gpusim2grid_b200.warmstart import LearnedStart
     ls = LearnedStart(g, hidden=args.hidden, layers=2, device=device, seed=0)
-    rep = ls.train(n_rows=args.train_rows, epochs=args.train_epochs, batch=1024, lr=1e-3, lr_decay=0.8, seed=1)
-    return ls, rep
+    mix = dict(WORKLOADS[args.workload][4])
+    rep = ls.train(n_rows=args.train_rows, epochs=args.train_epochs, batch=1024, lr=1e-3, lr_decay=0.8, seed=7,
+                   **mix)
+    return ls, rep, mix
+
+
+def _facade(g, trips, p, q, args, local):
+    """The reference-facing facade for the workload's rows (host inputs)."""
+    from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, ScenarioSweepGPU
+    kw = dict(init_from_n_powerflow=False, precision=args.precision, nb_iter=MAX_ITER, scheduling="continuous",
+              tol=TOL, start="flat", device=local, strategy=args.strategy)
+    if p is None:
+        f = ContingencyAnalysisGPU(g.as_tuple(), **kw)
+        f.set_branch_data(*g.branch_data())
+        f.add_contingencies_by_branch_id(trips)
+    elif trips is None:
+        f = InjectionSweepGPU(g.as_tuple(), **kw)
+        f.set_injections(p, q, g.sn_mva)
+    else:
+        f = ScenarioSweepGPU(g.as_tuple(), **kw)
+        f.set_branch_data(*g.branch_data())
+        f.set_injections(p, q, g.sn_mva)
+        f.set_topology(trips)
+    return f
+
+
+def _set_rows(f, trips, p, q, g):
+    """Hand the workload's host row definitions to the facade again (e2e)."""
+    if p is None:
+        f.add_contingencies_by_branch_id(trips)
+    elif trips is None:
+        f.set_injections(p, q, g.sn_mva)
+    else:
+        f.set_injections(p, q, g.sn_mva)
+        f.set_topology(trips)
 
 
 def run_ours(args):
@@ -194,42 +253,41 @@ def run_ours(args):
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from gpusim2grid_b200 import ContingencyAnalysisGPU, RowStatus
+    from gpusim2grid_b200 import RowStatus
     from gpusim2grid_b200._native import lib
 
-    g, rows = _workload()
+    g, trips, p, q = _workload(args.workload)
     if args.rows > 0:
-        rows = rows[:args.rows]
-    n = len(rows)
+        trips = trips[:args.rows] if trips is not None else None
+        p, q = (p[:args.rows], q[:args.rows]) if p is not None else (None, None)
+    n = len(trips) if trips is not None else p.shape[0]
     learned = args.start == "learned"
     prec = lib.PREC_MIXED if args.precision == "mixed" else lib.PREC_FP64
-    ca = ContingencyAnalysisGPU(g.as_tuple(), init_from_n_powerflow=False, precision=args.precision,
-                                nb_iter=MAX_ITER, scheduling="continuous", tol=TOL, start="flat", device=local)
-    ca.set_branch_data(*g.branch_data())
-    ca.add_contingencies_by_branch_id(rows)
-    ca.strategy = args.strategy
+    ca = _facade(g, trips, p, q, args, local)
     strat = lib.REFACTOR_ADAPTIVE if args.strategy == "adaptive" else lib.REFACTOR_EVERY
     s = ca.session
     info = s.info()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # device-resident row definitions for the learned start's features
+    csr = _ids(trips) if trips is not None else None
+    sbus_dev = None if p is None else torch.as_tensor((p + 1j * q) / g.sn_mva, device="cuda")
 
     train = None
     ls = None
     ratio, reuse = 0.0, 0
     if learned:
         t0 = time.perf_counter()
-        ls, rep = _train_learned(g, args, local)
+        ls, rep, mix = _train_learned(g, args, local)
         train = {"rows": rep["n_rows"], "epochs": args.train_epochs, "hidden": args.hidden, "layers": 2,
+                 "row_mix": mix, "unconverged_dropped": rep["n_unconverged"],
                  "t_generate_solve_s": round(rep["t_rows_s"] + rep["t_solve_s"], 2),
                  "t_fit_s": round(rep["t_fit_s"], 2), "t_total_s": round(time.perf_counter() - t0, 2),
                  "loss_first_last": [round(rep["loss"][0], 5), round(rep["loss"][-1], 5)],
                  "val_mse": round(rep["val"][-1], 5) if rep["val"] else None,
-                 "note": "untimed: training rows are seeded synthetic operating points (load scaling and single "
-                         "outages) solved by this engine in FP64; the timed rows (base injections, every "
-                         "outage) are not among them"}
+                 "note": "untimed: training rows are seeded synthetic operating points (load scaling, single "
+                         "outages) solved by this engine in FP64, drawn with another seed than the timed rows"}
         ca.set_learned_start(ls)
         ratio, reuse = ca._learned_opts
-        ptr, ids = _ids(rows)
     start_mode = lib.START_ROWS if learned else lib.START_VINIT
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -240,7 +298,7 @@ def run_ours(args):
         if learned:
             buf = s.start_rows_buffer(n)
             ev0.record()
-            ls.start_voltages(None, (ptr, ids), n, out_ptr=buf)
+            ls.start_voltages(sbus_dev, csr, n, out_ptr=buf)
             ev1.record()
             ev1.synchronize()
             pre_ms = ev0.elapsed_time(ev1)
@@ -297,13 +355,14 @@ def run_ours(args):
     fp64_value, V64, st64, it64 = flat_arm(lib.PREC_FP64, lib.REFACTOR_EVERY)
     ok = (st == 0) & (st64 == 0)
     agree = float(np.abs(V_w[ok] - V64[ok]).max()) if ok.any() else None
+    same_flags = bool(np.array_equal(st == 0, st64 == 0))
     mixed_flat_value = None
     if learned and args.precision == "mixed":
-        mixed_flat_value, _, _, it_mf = flat_arm(lib.PREC_MIXED, lib.REFACTOR_ADAPTIVE)
+        mixed_flat_value, _, _, _ = flat_arm(lib.PREC_MIXED, lib.REFACTOR_ADAPTIVE)
 
     # phase split of the measured arm (one extra profiled run, not timed)
     if learned:
-        ls.start_voltages(None, (ptr, ids), n, out_ptr=s.start_rows_buffer(n))
+        ls.start_voltages(sbus_dev, csr, n, out_ptr=s.start_rows_buffer(n))
         torch.cuda.synchronize()
     s.run(MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, True, strat, ratio, reuse, learned)
     phases = dict(zip(["mismatch", "fill", "head_lu", "schur", "dense_lu", "solves", "update"],
@@ -315,19 +374,23 @@ def run_ours(args):
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ca.add_contingencies_by_branch_id(rows)
+        _set_rows(ca, trips, p, q, g)
         ca.compute()
         V = ca.V_results
         stt = ca.get_row_status()
         r = ca.last_residuals()
         e2e_s.append(time.perf_counter() - t0)
     e2e_value = world * int((stt == 0).sum()) / float(np.mean(e2e_s))
-    n_ids = sum(len(r_) for r_ in rows)
-    h2d = 4 * (n + 1) + 4 * n_ids + (16 * n_ids if learned else 0)
+    n_ids = sum(len(r_) for r_ in trips) if trips is not None else 0
+    h2d = (4 * (n + 1) + 4 * n_ids if trips is not None else 0) + (2 * p.nbytes if p is not None else 0)
+    if learned:
+        h2d += 16 * n_ids + (0 if p is None else n * g.n_bus * 16)
     d2h = V.nbytes + stt.nbytes + r.nbytes
 
     w = 4 if args.precision == "mixed" else 8
     b_fact, b_iter = algorithmic_bytes(info, w)
+    if p is not None:
+        b_iter += 16 * info["n_bus"]  # each step reads the row's Sbus
     launch_bytes = b_fact * total_factors + b_iter * total_iters
     kernel_ms = float(np.mean(ker))
     achieved_gbs = launch_bytes / (kernel_ms / 1e3) / 1e9
@@ -337,6 +400,7 @@ def run_ours(args):
     achieved_tflops = launch_flops / (kernel_ms / 1e3) / 1e12
     fma_peak = 71.4 if args.precision == "mixed" else 37.1
     per_step_launches = 1 + (ls.launches_per_call(n) if learned else 0)
+    gname = WORKLOADS[args.workload][0]
 
     line = {
         "metric": METRIC,
@@ -345,7 +409,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 mismatch/V, f32 J/LU, bf16 MLP" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": WORKLOAD, "grid": GRID, "rows": n, "start": args.start,
+        "config": {"workload": args.workload, "grid": gname, "rows": n, "start": args.start,
                    "precision": args.precision, "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
         "rows_converged": n_conv, "rows_rescued": n_rescued, "newton_iters_total": total_iters,
@@ -354,8 +418,10 @@ def run_ours(args):
         "ms_split": {"features_mlp_v0": round(float(np.mean(pre)), 4), "sweep_kernel": round(kernel_ms, 4)},
         "fp64_flat_value": round(fp64_value, 1),
         "speedup_vs_fp64_flat": round(value / world / fp64_value, 3),
+        "fp64_flat_iters_hist": {int(k): int(v) for k, v in zip(*np.unique(it64, return_counts=True))},
         "mixed_flat_value": None if mixed_flat_value is None else round(mixed_flat_value, 1),
-        "agreement_with_fp64": {"max_abs_dv_pu": agree, "rows_compared": int(ok.sum())},
+        "agreement_with_fp64": {"max_abs_dv_pu": agree, "rows_compared": int(ok.sum()),
+                                "same_convergence_flags": same_flags},
         "training": train,
         "phase_share": phases,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
@@ -371,7 +437,7 @@ def run_ours(args):
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_baseline(g, rows, args.cpu_sample_rows)
+        v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_sample_rows)
         line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
                                 "sample": sample}
     if world > 1:
@@ -392,23 +458,24 @@ def run_reference(args):
     rank, world, _ = _dist()
     if rank != 0:
         return
-    g, rows = _workload()
+    g, trips, p, q = _workload(args.workload)
     vals = []
     for _ in range(args.warmup):
-        cpu_baseline(g, rows, 8)
-    cores = None
+        cpu_baseline(g, trips, p, q, 8)
+    cores = sample = None
     for _ in range(args.steps):
-        v, cores, sample = cpu_baseline(g, rows, args.cpu_sample_rows)
+        v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_sample_rows)
         vals.append(v)
     value = float(np.mean(vals))
+    n = len(trips) if trips is not None else p.shape[0]
     print(json.dumps({
         "impl": "reference",
         "metric": METRIC,
         "value": round(value, 2), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": WORKLOAD, "grid": GRID, "rows": len(rows), "start": "flat", "tol_pu": TOL,
-                   "max_iter": MAX_ITER},
+        "config": {"workload": args.workload, "grid": WORKLOADS[args.workload][0], "rows": n, "start": "flat",
+                   "tol_pu": TOL, "max_iter": MAX_ITER},
         "cpu_baseline": {"value": round(value, 2), "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
