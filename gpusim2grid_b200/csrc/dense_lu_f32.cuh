@@ -1,0 +1,296 @@
+// Dense FP32 LU (no pivoting) of one matrix by one CTA of 256 threads, for
+// the tail of the mixed-precision batched Newton–Raphson factorization.
+// Device code only.
+//
+// Right-looking, 64-wide panels.  Per panel k0 (width kb; kb < 64 only for
+// the last panel, which has nothing below or to the right of it):
+//   1. the kb x kb diagonal block is copied to shared memory (identity
+//      padded to 64 x 64) and factored there by all threads, one column per
+//      step, and written back;
+//   2. L21 = A21 U11^-1: one thread per row of A21, the row in registers,
+//      forward substitution against U11 rows read as broadcast float4;
+//   3. U12 = L11^-1 A12: one thread per column of A12, the column in
+//      registers, substitution against the rows of L11^T (unit diagonal),
+//      which is transposed into the idle tile staging area first;
+//   4. A22 -= L21 U12 on 128 x 128 output tiles: the tile's A (128 x 64) and
+//      B (64 x 128) operands are staged by cp.async in one piece, each
+//      thread accumulates an 8 x 8 block (rows tr + 16 i, columns
+//      4 tc + 64 h + e: within a warp 4 consecutive rows and 8 consecutive
+//      float4 columns, so shared-memory reads are conflict-free), and the
+//      next tile's operands are in flight while a tile's results are
+//      written back.
+// A is row-major in global memory with leading dimension ld, a multiple of
+// 8 (rows 16-byte aligned); panels start at multiples of 64.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gs2g {
+namespace dense32 {
+
+constexpr int BS = 256;
+constexpr int KP = 64;          // panel width
+constexpr int SD = KP + 4;      // diagonal block stride (16-byte rows)
+constexpr int TM = 128, TN = 128;
+constexpr int SA = KP + 4;      // A tile [TM][SA]
+constexpr int SB = TN + 4;      // B tile [KP][SB]
+
+struct Smem {
+  static constexpr int d_elems = KP * SD;
+  static constexpr int r_elems = KP;  // reciprocal pivots
+  static constexpr int a_elems = TM * SA;
+  static constexpr int b_elems = KP * SB;
+  static constexpr int elems = d_elems + r_elems + a_elems + b_elems;
+  static constexpr int bytes = elems * 4;
+};
+
+__device__ __forceinline__ float clamp_piv(float piv, double floor_) {
+  const float f = (float)floor_;
+  if (fabsf(piv) < f) return piv < 0.f ? -f : f;
+  return piv;
+}
+
+// Shared-memory loads issued in program order (asm volatile): the TRSM
+// loops below hold 64 values per thread in registers, and letting the
+// compiler hoist their ~500 broadcast loads ahead of the arithmetic would
+// spill them.
+__device__ __forceinline__ float4 lds4(const float* p) {
+  float4 v;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float lds1(const float* p) {
+  float v;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(a));
+  return v;
+}
+
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+
+// Stage the A (rows i0.., 64 columns) and B (64 rows, columns j0..) tiles of
+// the trailing update, zero-filled outside [M) rows / [N) columns.
+__device__ __forceinline__ void stage_tile(float* sA, float* sB, const float* A21, const float* A12, int ld, int M,
+                                           int N, int i0, int j0) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < (TM * KP / 4) / BS; ++q) {  // 8 chunks per thread
+    const int c = tid + q * BS;
+    const int r = c >> 4, k = (c & 15) * 4;
+    const bool in = i0 + r < M;
+    cp_async16(sA + r * SA + k, in ? A21 + (int64_t)(i0 + r) * ld + k : A21, in ? 16 : 0);
+  }
+#pragma unroll
+  for (int q = 0; q < (KP * TN / 4) / BS; ++q) {  // 8 chunks per thread
+    const int c = tid + q * BS;
+    const int k = c >> 5, n = (c & 31) * 4;
+    int bytes = (N - j0 - n) * 4;
+    bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+    cp_async16(sB + k * SB + n, bytes ? A12 + (int64_t)k * ld + j0 + n : A12, bytes);
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+
+// A22[M x N] -= A21[M x 64] A12[64 x N].
+__device__ __noinline__ void trailing_update(float* A22, const float* A21, const float* A12, int ld, int M, int N, float* sA,
+                                float* sB) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tr = (warp >> 1) * 4 + (lane >> 3);  // 0..15
+  const int tc = (warp & 1) * 8 + (lane & 7);    // 0..15
+  const int n_ti = (M + TM - 1) / TM, n_tj = (N + TN - 1) / TN;
+  const int n_tiles = n_ti * n_tj;
+  stage_tile(sA, sB, A21, A12, ld, M, N, 0, 0);
+  for (int t = 0; t < n_tiles; ++t) {
+    const int i0 = (t / n_tj) * TM, j0 = (t % n_tj) * TN;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < KP; ++k) {
+      float a[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = sA[(tr + 16 * i) * SA + k];
+      const float4 b0 = *reinterpret_cast<const float4*>(sB + k * SB + 4 * tc);
+      const float4 b1 = *reinterpret_cast<const float4*>(sB + k * SB + 64 + 4 * tc);
+      const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();  // every thread is done reading this tile's operands
+    if (t + 1 < n_tiles) {
+      const int t1 = t + 1;
+      stage_tile(sA, sB, A21, A12, ld, M, N, (t1 / n_tj) * TM, (t1 % n_tj) * TN);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = i0 + tr + 16 * i;
+      if (r >= M) continue;
+      float* crow = A22 + (int64_t)r * ld + j0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = 64 * h + 4 * tc;
+        if (j0 + c + 3 < N) {
+          float4 v = *reinterpret_cast<const float4*>(crow + c);
+          v.x -= acc[i][4 * h];
+          v.y -= acc[i][4 * h + 1];
+          v.z -= acc[i][4 * h + 2];
+          v.w -= acc[i][4 * h + 3];
+          *reinterpret_cast<float4*>(crow + c) = v;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (j0 + c + e < N) crow[c + e] -= acc[i][4 * h + e];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Factor the identity-padded 64 x 64 block D (stride SD) in place; rp gets
+// the reciprocal pivots.  One column per step, two barriers per step:
+//   phase 1 (D[j][j] final): every thread derives the pivot, the threads
+//            holding column j below the diagonal scale it;
+//   phase 2: thread 0 stores the pivot and its reciprocal (nobody reads
+//            them in this phase); rows j+1.. take the rank-1 update, each
+//            thread one fixed column and every fourth row.
+__device__ __noinline__ void factor_diag(float* D, float* rp, double pfloor) {
+  const int tid = threadIdx.x;
+  const int c = tid & (KP - 1), r0 = tid >> 6;  // column, first row offset (0..3)
+  for (int j = 0; j < KP; ++j) {
+    const float piv = clamp_piv(D[j * SD + j], pfloor);
+    const float r = 1.f / piv;
+    if (tid > j && tid < KP) D[tid * SD + j] *= r;
+    __syncthreads();
+    if (tid == 0) {
+      D[j * SD + j] = piv;
+      rp[j] = r;
+    }
+    if (c > j) {
+      const float ujc = D[j * SD + c];
+      for (int i = j + 1 + r0; i < KP; i += 4) D[i * SD + c] = fmaf(-D[i * SD + j], ujc, D[i * SD + c]);
+    }
+    __syncthreads();
+  }
+}
+
+// x <- x M^-1 for the 64 values x of one thread, M upper triangular given by
+// its rows (stride SD) in shared memory: after x_p is final, x_q -= x_p M_pq
+// for q > p.  SCALE: x_p is multiplied by rp[p] (1 / M_pp) first; else M has
+// a unit diagonal.
+template <bool SCALE>
+__device__ __forceinline__ void subst64(float (&x)[KP], const float* M, const float* rp) {
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    if (SCALE) x[p] *= lds1(rp + p);
+    const float xp = x[p];
+    const float* mp = M + p * SD;
+#pragma unroll
+    for (int q = p + 1; q < KP && (q & 3); ++q) x[q] = fmaf(-xp, lds1(mp + q), x[q]);
+#pragma unroll
+    for (int q4 = ((p + 1) + 3) & ~3; q4 < KP; q4 += 4) {
+      const float4 u = lds4(mp + q4);
+      x[q4] = fmaf(-xp, u.x, x[q4]);
+      x[q4 + 1] = fmaf(-xp, u.y, x[q4 + 1]);
+      x[q4 + 2] = fmaf(-xp, u.z, x[q4 + 2]);
+      x[q4 + 3] = fmaf(-xp, u.w, x[q4 + 3]);
+    }
+  }
+}
+
+// L21 = A21 U11^-1 (x U11 = a per row), one thread per row.
+__device__ __noinline__ void trsm_rows(float* A21, int ld, int M, const float* D, const float* rp) {
+  for (int r = threadIdx.x; r < M; r += BS) {
+    float4* row = reinterpret_cast<float4*>(A21 + (int64_t)r * ld);
+    float x[KP];
+#pragma unroll
+    for (int q = 0; q < KP / 4; ++q) {
+      const float4 v = row[q];
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
+    }
+    subst64<true>(x, D, rp);
+#pragma unroll
+    for (int q = 0; q < KP / 4; ++q) row[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+  }
+}
+
+// U12 = L11^-1 A12 (per column: y^T L11^T = a^T, L11^T upper with unit
+// diagonal, given by its rows LT = rows of L11^T), one thread per column.
+__device__ __noinline__ void trsm_cols(float* A12, int ld, int N, const float* LT) {
+  for (int c = threadIdx.x; c < N; c += BS) {
+    float y[KP];
+    const float* src = A12 + c;
+#pragma unroll
+    for (int r = 0; r < KP; ++r, src += ld) {
+      y[r] = *src;
+      if ((r & 15) == 15) asm volatile("" ::: "memory");  // at most 16 loads in flight
+    }
+    subst64<false>(y, LT, nullptr);
+    // the stores walk the column again from an opaque copy of ld, so the 64
+    // load addresses are not kept alive across the substitution
+    int ld2;
+    asm volatile("mov.b32 %0, %1;\n" : "=r"(ld2) : "r"(ld));
+    float* dst = A12 + c;
+#pragma unroll
+    for (int r = 0; r < KP; ++r, dst += ld2) *dst = y[r];
+  }
+}
+
+// LU of A (n x n, leading dimension ld) in place.
+__device__ void lu(float* A, int n, int ld, float* smem, double pfloor) {
+  float* D = smem;
+  float* rp = D + Smem::d_elems;
+  float* sA = rp + Smem::r_elems;
+  float* sB = sA + Smem::a_elems;
+  const int tid = threadIdx.x;
+  for (int k0 = 0; k0 < n; k0 += KP) {
+    const int kb = min(KP, n - k0);
+    float* Akk = A + (int64_t)k0 * ld + k0;
+    for (int idx = tid; idx < KP * KP; idx += BS) {
+      const int r = idx >> 6, c = idx & 63;
+      D[r * SD + c] = (r < kb && c < kb) ? Akk[(int64_t)r * ld + c] : (r == c ? 1.f : 0.f);
+    }
+    __syncthreads();
+    factor_diag(D, rp, pfloor);
+    for (int idx = tid; idx < kb * kb; idx += BS) {
+      const int r = idx / kb, c = idx % kb;
+      Akk[(int64_t)r * ld + c] = D[r * SD + c];
+    }
+    const int m = n - k0 - kb;  // > 0 only with kb == 64
+    if (m > 0) {
+      float* A21 = A + (int64_t)(k0 + kb) * ld + k0;
+      float* A12 = A + (int64_t)k0 * ld + k0 + kb;
+      float* A22 = A + (int64_t)(k0 + kb) * ld + k0 + kb;
+      // L11^T into the (idle) tile staging area for the column solves
+      float* LT = sA;
+      for (int idx = tid; idx < KP * KP; idx += BS) {
+        const int r = idx >> 6, c = idx & 63;
+        LT[c * SD + r] = r > c ? D[r * SD + c] : 0.f;
+      }
+      __syncthreads();
+      trsm_rows(A21, ld, m, D, rp);
+      trsm_cols(A12, ld, m, LT);
+      __syncthreads();  // L21 and U12 complete (global writes of other threads)
+      trailing_update(A22, A21, A12, ld, m, m, sA, sB);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace dense32
+}  // namespace gs2g

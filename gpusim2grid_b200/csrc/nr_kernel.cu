@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "dense_lu.cuh"
+#include "dense_lu_f32.cuh"
 
 #include <cmath>
 #include <cstdint>
@@ -77,6 +78,20 @@ __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
   const T f = (T)floor_;
   if (fabs(piv) < f) return piv < T(0) ? -f : f;
   return piv;
+}
+
+// Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on the
+// DMMA tiles of dense_lu.cuh; both use the dynamic shared memory as scratch.
+template <typename T>
+__device__ __forceinline__ void dense_lu(T* S, int n, int ld, T* smem, double pfloor) {
+  if constexpr (sizeof(T) == 4)
+    gs2g::dense32::lu(S, n, ld, smem, pfloor);
+  else
+    dense::lu<T>(S, n, ld, smem, pfloor);
+}
+template <typename T>
+__host__ __device__ constexpr int dense_smem_elems() {
+  return sizeof(T) == 4 ? gs2g::dense32::Smem::elems : dense::Smem<T>::elems;
 }
 
 // Dense unit-lower forward solve y <- L^{-1} y and upper backward solve
@@ -467,7 +482,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
 
       prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
-      if (P.nt > 0) dense::lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+      if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
       }  // refactor
       ++since_factor;
 
@@ -492,7 +507,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       }
       __syncthreads();
       if (P.nt > 0)
-        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, P.nt <= dense::Smem<T>::elems ? s_dense : y + P.p);
+        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, P.nt <= dense_smem_elems<T>() ? s_dense : y + P.p);
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int k = P.lev_piv[q0];
@@ -543,7 +558,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
 
 template <typename T>
 int smem_bytes() {
-  return dense::Smem<T>::bytes;
+  return sizeof(T) == 4 ? gs2g::dense32::Smem::bytes : dense::Smem<T>::bytes;
 }
 
 }  // namespace
