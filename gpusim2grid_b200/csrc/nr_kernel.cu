@@ -458,23 +458,24 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       }
 
       prof.mark(PH_HEAD);
-      // ---- Schur update of the dense tail: warp per tail row ---------------
+      // ---- Schur update of the dense tail ----------------------------------
+      // warp per tail row, lane per column group: each lane sums every
+      // contribution to one entry S[ti][col] and writes it once
       {
         const int lane = tid & 31, warp = tid >> 5;
         for (int ti = warp; ti < P.nt; ti += NWARP) {
           T* Srow = S + (int64_t)ti * P.ld;
-          for (int q = P.schur_ptr[ti]; q < P.schur_ptr[ti + 1]; ++q) {
-            const int s = P.schur_sn[q], ar = P.schur_a[q];
-            const int w = P.sn_w[s], t = P.sn_t[s];
-            const T* Lr = HV + P.sn_L[s] + ar * w;
-            const T* Ub = HV + P.sn_U[s];
-            const int* tx = P.tidx + P.sn_tidx[s];
-            for (int b = lane; b < t; b += 32) {
-              T acc = T(0);
-              for (int c = 0; c < w; ++c) acc += Lr[c] * Ub[c * t + b];
-              Srow[tx[b]] -= acc;
+          const int g1 = P.sg_ptr[ti + 1];
+          for (int g = P.sg_ptr[ti] + lane; g < g1; g += 32) {
+            T acc = T(0);
+            const int e1 = P.se_ptr[g + 1];
+            for (int e = P.se_ptr[g]; e < e1; ++e) {
+              const T* Lr = HV + P.se_L[e];
+              const T* Ub = HV + P.se_U[e];
+              const int wt = P.se_wt[e], w = wt & 15, t = wt >> 4;
+              for (int c = 0; c < w; ++c) acc += Lr[c] * Ub[c * t];
             }
-            __syncwarp();
+            Srow[P.sg_col[g]] -= acc;
           }
         }
       }

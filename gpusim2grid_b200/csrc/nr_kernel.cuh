@@ -37,9 +37,12 @@ struct DevPlan {
   const int* sn_U;
   const int* sn_tidx;
   const int* tidx;
-  const int* schur_ptr;  // [nt + 1]
-  const int* schur_sn;
-  const int* schur_a;
+  const int* sg_ptr;  // [nt + 1] Schur column groups per tail row
+  const int* sg_col;  // tail column of each group
+  const int* se_ptr;  // [groups + 1] entries per group
+  const int* se_L;    // HV offset of the L values of each entry
+  const int* se_U;    // HV offset of the first U value of each entry
+  const int* se_wt;   // w | t << 4 (U stride t)
   const int* fw_ptr;  // [dim + 1]
   const int* fw_col;
   const int* fw_pos;

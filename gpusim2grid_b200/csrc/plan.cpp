@@ -515,6 +515,37 @@ Plan build_plan(int n_bus, const int* ybus_indptr, const int* ybus_indices,
     }
     P.schur_ptr[ti + 1] = (int)P.schur_sn.size();
   }
+  // column groups of the Schur update (see plan.hpp)
+  {
+    struct Ent {
+      int col, L, U, wt, ord;
+    };
+    std::vector<Ent> ents;
+    P.sg_ptr.assign(P.nt + 1, 0);
+    P.se_ptr.assign(1, 0);
+    for (int ti = 0; ti < P.nt; ++ti) {
+      ents.clear();
+      for (int q = P.schur_ptr[ti]; q < P.schur_ptr[ti + 1]; ++q) {
+        const int s = P.schur_sn[q], a = P.schur_a[q], w = P.sn_w[s], t = P.sn_t[s];
+        if (w >= 16 || t >= (1 << 27)) throw std::logic_error("build_plan: supernode too large for the Schur map");
+        for (int b = 0; b < t; ++b)
+          ents.push_back({P.tidx[P.sn_tidx[s] + b], P.sn_L[s] + a * w, P.sn_U[s] + b, w | (t << 4), (int)ents.size()});
+      }
+      std::sort(ents.begin(), ents.end(),
+                [](const Ent& x, const Ent& y) { return x.col != y.col ? x.col < y.col : x.ord < y.ord; });
+      for (size_t e = 0; e < ents.size(); ++e) {
+        if (e == 0 || ents[e].col != ents[e - 1].col) {
+          if (e > 0) P.se_ptr.push_back((int)P.se_L.size());
+          P.sg_col.push_back(ents[e].col);
+        }
+        P.se_L.push_back(ents[e].L);
+        P.se_U.push_back(ents[e].U);
+        P.se_wt.push_back(ents[e].wt);
+      }
+      if (!ents.empty()) P.se_ptr.push_back((int)P.se_L.size());
+      P.sg_ptr[ti + 1] = (int)P.sg_col.size();
+    }
+  }
   for (int64_t k = 0; k < P.nt; ++k) P.dense_madds += (P.nt - 1 - k) * (P.nt - 1 - k);
 
   // ---- solves -------------------------------------------------------------

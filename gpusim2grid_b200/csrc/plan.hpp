@@ -81,6 +81,12 @@ struct Plan {
   std::vector<int> tidx;  // tail-local row index of every tail row of every supernode
   // Schur items per tail row: [schur_ptr[ti], schur_ptr[ti+1]) of (sn, a)
   std::vector<int> schur_ptr, schur_sn, schur_a;
+  // The same update as column groups, the form the device runs: tail row ti
+  // owns groups [sg_ptr[ti], sg_ptr[ti+1]); group g updates S[ti][sg_col[g]]
+  // with the sum over entries [se_ptr[g], se_ptr[g+1]) of
+  //   sum_{c < w} HV[se_L[e] + c] * HV[se_U[e] + c * t],  w | t << 4 = se_wt[e]
+  // (entries of a group in supernode order).
+  std::vector<int> sg_ptr, sg_col, se_ptr, se_L, se_U, se_wt;
   int64_t schur_madds = 0, schur_volume = 0;
   int64_t dense_madds = 0;
 

@@ -154,9 +154,12 @@ void upload_plan(gs2g_session* s) {
   D.sn_U = upload_vec(s, P.sn_U);
   D.sn_tidx = upload_vec(s, P.sn_tidx);
   D.tidx = upload_vec(s, P.tidx);
-  D.schur_ptr = upload_vec(s, P.schur_ptr);
-  D.schur_sn = upload_vec(s, P.schur_sn);
-  D.schur_a = upload_vec(s, P.schur_a);
+  D.sg_ptr = upload_vec(s, P.sg_ptr);
+  D.sg_col = upload_vec(s, P.sg_col);
+  D.se_ptr = upload_vec(s, P.se_ptr);
+  D.se_L = upload_vec(s, P.se_L);
+  D.se_U = upload_vec(s, P.se_U);
+  D.se_wt = upload_vec(s, P.se_wt);
   D.fw_ptr = upload_vec(s, P.fw_ptr);
   D.fw_col = upload_vec(s, P.fw_col);
   D.fw_pos = upload_vec(s, P.fw_pos);
