@@ -115,6 +115,28 @@ class _BatchSweep:
         """(sbus_rows or None, trips CSR or None, n_rows) of the current rows."""
         raise NotImplementedError
 
+    def autotune(self, dense_rates=(40.0, 80.0, 160.0, 320.0, 640.0), repeats=2, batch_size=512):
+        """Pick the symbolic plan that solves the current rows fastest.  Each
+        candidate re-plans the head/tail split with another dense/scatter
+        cost ratio (``Session.replan``) and times ``repeats`` sweeps of the
+        current rows with the current start, precision and strategy (device
+        time of the sweep kernel); the fastest plan is kept.  Returns
+        {dense_rate: (tail_dim, best ms)} and the chosen rate."""
+        out = {}
+        best = (float("inf"), None)
+        for rate in dense_rates:
+            self._s.replan(1, float(rate), -1)
+            ms = []
+            for _ in range(max(1, int(repeats))):
+                self._run(batch_size)
+                ms.append(self._timings.t_kernel_ms)
+            out[float(rate)] = (int(self._s.info()["tail_dim"]), float(min(ms)))
+            if min(ms) < best[0]:
+                best = (min(ms), float(rate))
+        self._s.replan(1, best[1], -1)
+        self._ran = False
+        return out, best[1]
+
     @property
     def warm_report(self):
         """Timings of the last learned start: predict_ms (features, network

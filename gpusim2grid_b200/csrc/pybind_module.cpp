@@ -204,6 +204,10 @@ class Session {
     check(gs2g_set_start_rows_device(h(), n_rows, reinterpret_cast<const double*>(ptr)));
   }
 
+  void replan(int tail_policy, double dense_rate, int force_tau) {
+    check(gs2g_session_replan(h(), tail_policy, dense_rate, force_tau));
+  }
+
   uintptr_t start_rows_buffer(int n_rows) {
     double* p = nullptr;
     check(gs2g_start_rows_buffer(h(), n_rows, &p));
@@ -461,6 +465,8 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("set_start_rows", &Session::set_start_rows)
       .def("set_start_rows_device", &Session::set_start_rows_device)
       .def("start_rows_buffer", &Session::start_rows_buffer)
+      .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
+           py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)
       .def("set_vinit", &Session::set_vinit)
       .def("solve_base", &Session::solve_base)

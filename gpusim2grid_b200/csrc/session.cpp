@@ -73,6 +73,7 @@ struct gs2g_session {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   gs2g::Plan plan;
   gs2g::DevPlan dplan{};
+  std::vector<int> y_ip, y_ix, pv, pq;  // canonical pattern and bus sets, for re-planning
   std::vector<std::unique_ptr<DevBuf>> plan_bufs;
   int n_bus = 0;
   std::vector<double> ybus;  // canonical values, interleaved complex
@@ -450,6 +451,10 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
   topt.policy = tail_policy;
   s->plan = gs2g::build_plan(n_bus, ip.data(), ix.data(), pv, n_pv, pq, n_pq, topt);
   s->tm.plan_ms = s->plan.build_ms;
+  s->y_ip = ip;
+  s->y_ix = ix;
+  s->pv.assign(pv, pv + n_pv);
+  s->pq.assign(pq, pq + n_pq);
   s->vinit.assign(vinit, vinit + 2 * n_bus);
   s->sbus.assign(sbus, sbus + 2 * n_bus);
   ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
@@ -463,6 +468,26 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
   s->d_sbus.ensure(2 * n_bus * sizeof(double));
   ck(cudaMemcpy(s->d_sbus.p, sbus, 2 * n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Sbus");
   *out = s.release();
+  GS2G_CATCH
+}
+
+int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int force_tau) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_replan: NULL session");
+  if (tail_policy != 0 && tail_policy != 1) throw std::invalid_argument("session_replan: tail_policy must be 0 or 1");
+  if (!(dense_rate >= 0)) throw std::invalid_argument("session_replan: dense_rate must be >= 0");
+  DeviceGuard g(s->device);
+  gs2g::TailOptions topt;
+  topt.policy = tail_policy;
+  if (dense_rate > 0) topt.dense_rate = dense_rate;
+  topt.force_tau = force_tau;
+  gs2g::Plan P = gs2g::build_plan(s->n_bus, s->y_ip.data(), s->y_ix.data(), s->pv.data(), (int)s->pv.size(),
+                                  s->pq.data(), (int)s->pq.size(), topt);
+  ck(cudaStreamSynchronize(s->stream), "replan");
+  s->plan = std::move(P);
+  s->plan_bufs.clear();
+  upload_plan(s);
+  s->tm.plan_ms = s->plan.build_ms;
   GS2G_CATCH
 }
 

@@ -123,6 +123,14 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
                         const int* pv, int n_pv, const int* pq, int n_pq, int tail_policy,
                         gs2g_session** out);
 int gs2g_session_destroy(gs2g_session* s);
+/* Rebuild the session's symbolic plan with other head/tail options: the
+ * dense tail is extended with head columns while the planner's cost model,
+ * (tail^3 / 3) / dense_rate + Schur volume, says so (dense_rate <= 0 keeps
+ * the default 40; force_tau >= 0 forces the tail-row threshold; policy 0 =
+ * exact trailing clique only).  Row definitions stay valid.  Used by the
+ * facades' autotuner, which times candidate plans on the caller's rows
+ * (the reference's lu_plan builds one plan; no counterpart). */
+int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int force_tau);
 int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
 int gs2g_get_device(const gs2g_session* s, int* device);
 
