@@ -74,6 +74,8 @@ def _args():
     ap.add_argument("--train-rows", type=int, default=100000)
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--hidden", type=int, default=1024)
+    ap.add_argument("--tune-rates", type=float, nargs="*", default=[40.0, 160.0, 320.0],
+                    help="dense/scatter cost ratios the plan autotuner tries (none: keep the default plan)")
     return ap.parse_args()
 
 
@@ -288,6 +290,11 @@ def run_ours(args):
                          "outages) solved by this engine in FP64, drawn with another seed than the timed rows"}
         ca.set_learned_start(ls)
         ratio, reuse = ca._learned_opts
+    # one-time plan choice (untimed, like the symbolic analysis): the
+    # head/tail split that solves these rows fastest in the measured arm
+    ca.start = "learned" if learned else "flat"
+    tune, rate = ca.autotune(tuple(args.tune_rates), repeats=1) if args.tune_rates else ({}, None)
+    info = s.info()
     start_mode = lib.START_ROWS if learned else lib.START_VINIT
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -423,6 +430,8 @@ def run_ours(args):
         "agreement_with_fp64": {"max_abs_dv_pu": agree, "rows_compared": int(ok.sum()),
                                 "same_convergence_flags": same_flags},
         "training": train,
+        "plan": {"tail_dim": info["tail_dim"], "head_dim": info["head_dim"], "autotune_dense_rate": rate,
+                 "autotune_ms": {str(k): v[1] for k, v in tune.items()}},
         "phase_share": phases,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": None,

@@ -80,6 +80,25 @@ __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
   return piv;
 }
 
+// Sum of the Schur contributions of column group g (see Plan::sg_ptr).
+// Entries have width w <= 15 (1 or 2 here: supernodes are buses); the first
+// two products are loaded together.
+template <typename T>
+__device__ __forceinline__ T schur_group(const DevPlan& P, const T* __restrict__ HV, int g) {
+  T acc = T(0);
+  const int e1 = P.se_ptr[g + 1];
+  for (int e = P.se_ptr[g]; e < e1; ++e) {
+    const T* Lr = HV + P.se_L[e];
+    const T* Ub = HV + P.se_U[e];
+    const int wt = P.se_wt[e], w = wt & 15, t = wt >> 4;
+    const T l0 = Lr[0], u0 = Ub[0];
+    const T l1 = w > 1 ? Lr[1] : T(0), u1 = w > 1 ? Ub[t] : T(0);
+    acc += l0 * u0 + l1 * u1;
+    for (int c = 2; c < w; ++c) acc += Lr[c] * Ub[c * t];
+  }
+  return acc;
+}
+
 // Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on the
 // DMMA tiles of dense_lu.cuh; both use the dynamic shared memory as scratch.
 template <typename T>
@@ -103,41 +122,56 @@ __host__ __device__ constexpr int dense_smem_elems() {
 // columns start at multiples of 32).  y lives in ys (shared memory when it
 // fits, else ys == yg).
 template <typename T>
+__device__ __forceinline__ T row_dot32(const T* __restrict__ row, const T* s_blk) {
+  T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
+  if constexpr (sizeof(T) == 4) {
+    const float4* r4 = reinterpret_cast<const float4*>(row);
+    float4 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = r4[q];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      acc0 = fma(v[q].x, s_blk[4 * q], acc0);
+      acc1 = fma(v[q].y, s_blk[4 * q + 1], acc1);
+      acc2 = fma(v[q].z, s_blk[4 * q + 2], acc2);
+      acc3 = fma(v[q].w, s_blk[4 * q + 3], acc3);
+    }
+  } else {
+    const double2* r2 = reinterpret_cast<const double2*>(row);
+    double2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = r2[q];
+#pragma unroll
+    for (int q = 0; q < 16; q += 2) {
+      acc0 = fma(v[q].x, s_blk[2 * q], acc0);
+      acc1 = fma(v[q].y, s_blk[2 * q + 1], acc1);
+      acc2 = fma(v[q + 1].x, s_blk[2 * q + 2], acc2);
+      acc3 = fma(v[q + 1].y, s_blk[2 * q + 3], acc3);
+    }
+  }
+  return (acc0 + acc1) + (acc2 + acc3);
+}
+
+template <typename T>
 __device__ __forceinline__ void block_column_update(const T* __restrict__ A, int ld, int c0, int cb, int r0, int r1,
                                                     const T* s_blk, T* ys) {
-  for (int i = r0 + (int)threadIdx.x; i < r1; i += BS) {
-    const T* row = A + (int64_t)i * ld + c0;
-    T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
-    if (cb == 32) {
-      if constexpr (sizeof(T) == 4) {
-        const float4* r4 = reinterpret_cast<const float4*>(row);
-        float4 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = r4[q];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          acc0 = fma(v[q].x, s_blk[4 * q], acc0);
-          acc1 = fma(v[q].y, s_blk[4 * q + 1], acc1);
-          acc2 = fma(v[q].z, s_blk[4 * q + 2], acc2);
-          acc3 = fma(v[q].w, s_blk[4 * q + 3], acc3);
-        }
-      } else {
-        const double2* r2 = reinterpret_cast<const double2*>(row);
-        double2 v[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = r2[q];
-#pragma unroll
-        for (int q = 0; q < 16; q += 2) {
-          acc0 = fma(v[q].x, s_blk[2 * q], acc0);
-          acc1 = fma(v[q].y, s_blk[2 * q + 1], acc1);
-          acc2 = fma(v[q + 1].x, s_blk[2 * q + 2], acc2);
-          acc3 = fma(v[q + 1].y, s_blk[2 * q + 3], acc3);
-        }
-      }
-    } else {
-      for (int c = 0; c < cb; ++c) acc0 = fma(row[c], s_blk[c], acc0);
+  if (cb == 32) {
+    // two rows per thread per pass: both rows' loads are in flight together
+    int i = r0 + (int)threadIdx.x;
+    for (; i + BS < r1; i += 2 * BS) {
+      const T d0 = row_dot32<T>(A + (int64_t)i * ld + c0, s_blk);
+      const T d1 = row_dot32<T>(A + (int64_t)(i + BS) * ld + c0, s_blk);
+      ys[i] -= d0;
+      ys[i + BS] -= d1;
     }
-    ys[i] -= (acc0 + acc1) + (acc2 + acc3);
+    if (i < r1) ys[i] -= row_dot32<T>(A + (int64_t)i * ld + c0, s_blk);
+  } else {
+    for (int i = r0 + (int)threadIdx.x; i < r1; i += BS) {
+      const T* row = A + (int64_t)i * ld + c0;
+      T acc = T(0);
+      for (int c = 0; c < cb; ++c) acc = fma(row[c], s_blk[c], acc);
+      ys[i] -= acc;
+    }
   }
 }
 
@@ -460,22 +494,18 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       prof.mark(PH_HEAD);
       // ---- Schur update of the dense tail ----------------------------------
       // warp per tail row, lane per column group: each lane sums every
-      // contribution to one entry S[ti][col] and writes it once
+      // contribution to one entry S[ti][col] and writes it once; two groups
+      // per lane at a time keep more independent loads in flight
       {
         const int lane = tid & 31, warp = tid >> 5;
         for (int ti = warp; ti < P.nt; ti += NWARP) {
           T* Srow = S + (int64_t)ti * P.ld;
           const int g1 = P.sg_ptr[ti + 1];
-          for (int g = P.sg_ptr[ti] + lane; g < g1; g += 32) {
-            T acc = T(0);
-            const int e1 = P.se_ptr[g + 1];
-            for (int e = P.se_ptr[g]; e < e1; ++e) {
-              const T* Lr = HV + P.se_L[e];
-              const T* Ub = HV + P.se_U[e];
-              const int wt = P.se_wt[e], w = wt & 15, t = wt >> 4;
-              for (int c = 0; c < w; ++c) acc += Lr[c] * Ub[c * t];
-            }
-            Srow[P.sg_col[g]] -= acc;
+          for (int g = P.sg_ptr[ti] + lane; g < g1; g += 64) {
+            const bool two = g + 32 < g1;
+            T acc0 = schur_group<T>(P, HV, g), acc1 = two ? schur_group<T>(P, HV, g + 32) : T(0);
+            Srow[P.sg_col[g]] -= acc0;
+            if (two) Srow[P.sg_col[g + 32]] -= acc1;
           }
         }
       }
