@@ -21,6 +21,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "dense_lu.cuh"
 #include "dense_lu_f32.cuh"
 
@@ -175,60 +177,145 @@ __device__ __forceinline__ void block_column_update(const T* __restrict__ A, int
   }
 }
 
+// One 32-wide row segment of the factor held in registers (16-byte loads).
 template <typename T>
-__device__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ yg, T* s_blk, T* ys) {
+struct Seg32 {
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  static constexpr int NV = 32 * (int)sizeof(T) / 16;
+  V v[NV];
+  __device__ __forceinline__ void load(const T* row) {
+    const V* r = reinterpret_cast<const V*>(row);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = r[q];
+  }
+  __device__ __forceinline__ T dot(const T* s) const {
+    T acc0 = T(0), acc1 = T(0);
+    const T* e = reinterpret_cast<const T*>(v);
+#pragma unroll
+    for (int c = 0; c < 32; c += 2) {
+      acc0 = fma(e[c], s[c], acc0);
+      acc1 = fma(e[c + 1], s[c + 1], acc1);
+    }
+    return acc0 + acc1;
+  }
+};
+
+// Diagonal-block staging for the dense solves: warp 0 copies the 32 x 32
+// block of block column c0 (rows c0.., columns c0..; cb valid rows, n
+// valid columns) into dbuf (stride DSTR) with cp.async, one row per lane,
+// zero-filling past column n.
+template <typename T>
+__host__ __device__ constexpr int diag_stride() {
+  return 32 + 16 / (int)sizeof(T);
+}
+template <typename T>
+__device__ __forceinline__ void stage_diag(T* dbuf, const T* A, int ld, int n, int c0, int cb, int lane) {
+  constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte chunk
+  if (lane < cb) {
+    const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
+    T* dp = dbuf + lane * diag_stride<T>();
+#pragma unroll
+    for (int j = 0; j < 32 / EPC; ++j) {
+      int bytes = (n - c0 - j * EPC) * (int)sizeof(T);
+      bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dp + j * EPC);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(bytes ? rp + j * EPC : rp),
+                   "r"(bytes));
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void wait_staged() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncwarp();
+}
+
+// Dense tail solves (see the comment above block_column_update).  The factor
+// is read-only here, so its loads run ahead of the values they multiply:
+// every thread issues its first update row of block column k before waiting
+// for block k's diagonal solve, and warp 0 stages block k+1's diagonal block
+// in shared memory (cp.async) right after solving block k.  dbuf: 32 x
+// diag_stride shared-memory scratch.
+template <typename T>
+__device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ yg, T* s_blk, T* ys,
+                                          T* dbuf) {
+  constexpr int DS = diag_stride<T>();
+  constexpr bool PFROW = sizeof(T) == 4;  // row prefetch in registers (FP32 only: register budget)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (ys != yg) {
     for (int i = tid; i < n; i += BS) ys[i] = yg[i];
     __syncthreads();
   }
-  for (int c0 = 0; c0 < n; c0 += 32) {
-    const int cb = min(32, n - c0);
+  const int nblk = (n + 31) / 32;
+  Seg32<T> seg;
+  // ---- forward, unit lower ----
+  if (warp == 0) stage_diag<T>(dbuf, A, ld, n, 0, min(32, n), lane);
+  for (int k = 0; k < nblk; ++k) {
+    const int c0 = 32 * k, cb = min(32, n - c0);
+    const int r0 = c0 + cb;
+    const bool full = cb == 32;
+    const int i = r0 + tid;
+    if (PFROW && full && i < n) seg.load(A + (int64_t)i * ld + c0);
     if (warp == 0) {
-      // lane r loads row r of the diagonal block up front (independent loads)
-      T arow[32];
-      const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
-#pragma unroll
-      for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c < lane) ? rp[c] : T(0);
+      wait_staged();
       T v = lane < cb ? ys[c0 + lane] : T(0);
+      const T* dr = dbuf + lane * DS;
 #pragma unroll
       for (int c = 0; c < 32; ++c) {
-        const T yc = __shfl_sync(0xffffffffu, v, c);
-        v = fma(-arow[c], yc, v);
+        const T a = (lane < cb && c < lane) ? dr[c] : T(0);
+        v = fma(-a, __shfl_sync(0xffffffffu, v, c), v);
       }
+      __syncwarp();  // every lane has read dbuf before it is refilled
       if (lane < cb) {
         ys[c0 + lane] = v;
         s_blk[lane] = v;
       }
+      if (k + 1 < nblk) stage_diag<T>(dbuf, A, ld, n, c0 + 32, min(32, n - c0 - 32), lane);
     }
     __syncthreads();
-    block_column_update<T>(A, ld, c0, cb, c0 + cb, n, s_blk, ys);
+    if (full && PFROW) {
+      if (i < n) ys[i] -= seg.dot(s_blk);
+      block_column_update<T>(A, ld, c0, cb, r0 + BS, n, s_blk, ys);
+    } else {
+      block_column_update<T>(A, ld, c0, cb, r0, n, s_blk, ys);
+    }
     __syncthreads();
   }
-  const int nblk = (n + 31) / 32;
-  for (int bi = nblk - 1; bi >= 0; --bi) {
-    const int c0 = bi * 32;
-    const int cb = min(32, n - c0);
+  // ---- backward, upper ----
+  if (warp == 0) {
+    const int c0 = 32 * (nblk - 1);
+    stage_diag<T>(dbuf, A, ld, n, c0, n - c0, lane);
+  }
+  for (int k = nblk - 1; k >= 0; --k) {
+    const int c0 = 32 * k, cb = min(32, n - c0);
+    const bool full = cb == 32;
+    if (PFROW && full && tid < c0) seg.load(A + (int64_t)tid * ld + c0);
     if (warp == 0) {
-      T arow[32];
-      const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
-#pragma unroll
-      for (int c = 0; c < 32; ++c) arow[c] = (lane < cb && c >= lane && c < cb) ? rp[c] : T(lane == c ? 1 : 0);
+      wait_staged();
       T v = lane < cb ? ys[c0 + lane] : T(0);
+      const T* dr = dbuf + lane * DS;
 #pragma unroll
       for (int c = 31; c >= 0; --c) {
-        T xc = v / arow[c];  // meaningful on lane c only
+        const T a = (lane < cb && c >= lane && c < cb) ? dr[c] : T(lane == c ? 1 : 0);
+        T xc = v / a;  // meaningful on lane c only
         xc = __shfl_sync(0xffffffffu, xc, c);
         if (lane == c) v = xc;
-        else if (lane < c) v = fma(-arow[c], xc, v);
+        else if (lane < c) v = fma(-a, xc, v);
       }
+      __syncwarp();  // every lane has read dbuf before it is refilled
+      if (k > 0) stage_diag<T>(dbuf, A, ld, n, c0 - 32, 32, lane);
       if (lane < cb) {
         ys[c0 + lane] = v;
         s_blk[lane] = v;
       }
     }
     __syncthreads();
-    block_column_update<T>(A, ld, c0, cb, 0, c0, s_blk, ys);
+    if (full && PFROW) {
+      if (tid < c0) ys[tid] -= seg.dot(s_blk);
+      block_column_update<T>(A, ld, c0, cb, BS, c0, s_blk, ys);
+    } else {
+      block_column_update<T>(A, ld, c0, cb, 0, c0, s_blk, ys);
+    }
     __syncthreads();
   }
   if (ys != yg) {
@@ -538,7 +625,13 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       }
       __syncthreads();
       if (P.nt > 0)
-        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, P.nt <= dense_smem_elems<T>() ? s_dense : y + P.p);
+      {
+        // y tail in shared memory when it fits, the diagonal-block buffer after it
+        const bool y_in_smem = P.nt + 32 * diag_stride<T>() + 32 <= dense_smem_elems<T>();
+        T* ys = y_in_smem ? s_dense : y + P.p;
+        T* dbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
+        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, ys, dbuf);
+      }
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int k = P.lev_piv[q0];
