@@ -372,7 +372,8 @@ def run_ours(args):
         ls.start_voltages(sbus_dev, csr, n, out_ptr=s.start_rows_buffer(n))
         torch.cuda.synchronize()
     s.run(MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, True, strat, ratio, reuse, learned)
-    phases = dict(zip(["mismatch", "fill", "head_lu", "schur", "dense_lu", "solves", "update"],
+    phases = dict(zip(["mismatch", "fill", "head_lu", "schur", "dense_lu", "solve_head_fw", "solve_tail_fw",
+                       "solve_dense", "solve_head_bw", "update"],
                       [round(x, 4) for x in s.timings()["phase_share"]]))
 
     # end to end through the facade, host buffers in and out

@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         }
         __syncthreads();
       }
+      prof.mark(PH_SOLVE);
       for (int ti = tid; ti < P.nt; ti += BS) {
         const int i = P.p + ti;
         T acc = y[i];
@@ -624,6 +625,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         y[i] = acc;
       }
       __syncthreads();
+      prof.mark(PH_SOLVE_TAIL);
       if (P.nt > 0)
       {
         // y tail in shared memory when it fits, the diagonal-block buffer after it
@@ -632,6 +634,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         T* dbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
         dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, ys, dbuf);
       }
+      prof.mark(PH_SOLVE_DENSE);
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int k = P.lev_piv[q0];
@@ -642,7 +645,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         __syncthreads();
       }
 
-      prof.mark(PH_SOLVE);
+      prof.mark(PH_SOLVE_BACK);
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
         const int fp = P.fP[i], fq = P.fQ[i];

@@ -97,9 +97,12 @@ enum Phase : int {
   PH_HEAD = 2,      // sparse head LU
   PH_SCHUR = 3,     // Schur update of the tail
   PH_DENSE = 4,     // dense tail LU
-  PH_SOLVE = 5,     // triangular solves
-  PH_UPDATE = 6,    // voltage update
-  N_PHASES = 7
+  PH_SOLVE = 5,     // triangular solves: head forward
+  PH_SOLVE_TAIL = 6,   // forward rows of the tail against the head
+  PH_SOLVE_DENSE = 7,  // dense tail forward + backward
+  PH_SOLVE_BACK = 8,   // head backward
+  PH_UPDATE = 9,       // voltage update
+  N_PHASES = 10
 };
 
 // Per-CTA workspace bytes for precision `prec` (0: fp64 LU, 1: fp32 LU).

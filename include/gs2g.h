@@ -97,7 +97,9 @@ typedef struct gs2g_run_opts {
 #define GS2G_REFACTOR_EVERY 0
 #define GS2G_REFACTOR_ADAPTIVE 1
 
-#define GS2G_N_PHASES 7 /* mismatch, fill, head LU, Schur, dense LU, solves, update */
+/* mismatch, fill, head LU, Schur, dense LU, solve: head forward, tail forward,
+ * dense tail, head backward; update */
+#define GS2G_N_PHASES 10
 
 typedef struct gs2g_timings {
   double plan_ms;      /* symbolic analysis, once per session */
