@@ -115,107 +115,21 @@ __host__ __device__ constexpr int dense_smem_elems() {
   return sizeof(T) == 4 ? gs2g::dense32::Smem::elems : dense::Smem<T>::elems;
 }
 
-// Dense unit-lower forward solve y <- L^{-1} y and upper backward solve
-// y <- U^{-1} y on the tail (yg: the tail part of the solve vector).  The
-// tail is processed in 32-wide column blocks: warp 0 solves the diagonal
-// block, then every other row of the block column takes a rank-32 update
-// as a dot product, one thread per row reading its 32 values with 16-byte
-// vector loads (rows are 16-byte aligned: ld is a multiple of 8 and block
-// columns start at multiples of 32).  y lives in ys (shared memory when it
-// fits, else ys == yg).
+// Staging for the dense solves: warp 0 copies a 32 x 64 tile of the factor
+// (rows r0.. (nr valid), columns c0.. (valid below n)) into shared memory
+// with cp.async, one row per lane, zero-filling past column n.
 template <typename T>
-__device__ __forceinline__ T row_dot32(const T* __restrict__ row, const T* s_blk) {
-  T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
-  if constexpr (sizeof(T) == 4) {
-    const float4* r4 = reinterpret_cast<const float4*>(row);
-    float4 v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = r4[q];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      acc0 = fma(v[q].x, s_blk[4 * q], acc0);
-      acc1 = fma(v[q].y, s_blk[4 * q + 1], acc1);
-      acc2 = fma(v[q].z, s_blk[4 * q + 2], acc2);
-      acc3 = fma(v[q].w, s_blk[4 * q + 3], acc3);
-    }
-  } else {
-    const double2* r2 = reinterpret_cast<const double2*>(row);
-    double2 v[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = r2[q];
-#pragma unroll
-    for (int q = 0; q < 16; q += 2) {
-      acc0 = fma(v[q].x, s_blk[2 * q], acc0);
-      acc1 = fma(v[q].y, s_blk[2 * q + 1], acc1);
-      acc2 = fma(v[q + 1].x, s_blk[2 * q + 2], acc2);
-      acc3 = fma(v[q + 1].y, s_blk[2 * q + 3], acc3);
-    }
-  }
-  return (acc0 + acc1) + (acc2 + acc3);
-}
-
-template <typename T>
-__device__ __forceinline__ void block_column_update(const T* __restrict__ A, int ld, int c0, int cb, int r0, int r1,
-                                                    const T* s_blk, T* ys) {
-  if (cb == 32) {
-    // two rows per thread per pass: both rows' loads are in flight together
-    int i = r0 + (int)threadIdx.x;
-    for (; i + BS < r1; i += 2 * BS) {
-      const T d0 = row_dot32<T>(A + (int64_t)i * ld + c0, s_blk);
-      const T d1 = row_dot32<T>(A + (int64_t)(i + BS) * ld + c0, s_blk);
-      ys[i] -= d0;
-      ys[i + BS] -= d1;
-    }
-    if (i < r1) ys[i] -= row_dot32<T>(A + (int64_t)i * ld + c0, s_blk);
-  } else {
-    for (int i = r0 + (int)threadIdx.x; i < r1; i += BS) {
-      const T* row = A + (int64_t)i * ld + c0;
-      T acc = T(0);
-      for (int c = 0; c < cb; ++c) acc = fma(row[c], s_blk[c], acc);
-      ys[i] -= acc;
-    }
-  }
-}
-
-// One 32-wide row segment of the factor held in registers (16-byte loads).
-template <typename T>
-struct Seg32 {
-  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-  static constexpr int NV = 32 * (int)sizeof(T) / 16;
-  V v[NV];
-  __device__ __forceinline__ void load(const T* row) {
-    const V* r = reinterpret_cast<const V*>(row);
-#pragma unroll
-    for (int q = 0; q < NV; ++q) v[q] = r[q];
-  }
-  __device__ __forceinline__ T dot(const T* s) const {
-    T acc0 = T(0), acc1 = T(0);
-    const T* e = reinterpret_cast<const T*>(v);
-#pragma unroll
-    for (int c = 0; c < 32; c += 2) {
-      acc0 = fma(e[c], s[c], acc0);
-      acc1 = fma(e[c + 1], s[c + 1], acc1);
-    }
-    return acc0 + acc1;
-  }
-};
-
-// Diagonal-block staging for the dense solves: warp 0 copies the 32 x 32
-// block of block column c0 (rows c0.., columns c0..; cb valid rows, n
-// valid columns) into dbuf (stride DSTR) with cp.async, one row per lane,
-// zero-filling past column n.
-template <typename T>
-__host__ __device__ constexpr int diag_stride() {
-  return 32 + 16 / (int)sizeof(T);
+__host__ __device__ constexpr int stage_stride() {
+  return 64 + 16 / (int)sizeof(T);
 }
 template <typename T>
-__device__ __forceinline__ void stage_diag(T* dbuf, const T* A, int ld, int n, int c0, int cb, int lane) {
+__device__ __forceinline__ void stage_tile32x64(T* buf, const T* A, int ld, int n, int r0, int nr, int c0, int lane) {
   constexpr int EPC = 16 / sizeof(T);  // elements per 16-byte chunk
-  if (lane < cb) {
-    const T* rp = A + (int64_t)(c0 + lane) * ld + c0;
-    T* dp = dbuf + lane * diag_stride<T>();
+  if (lane < nr && c0 >= 0) {
+    const T* rp = A + (int64_t)(r0 + lane) * ld + c0;
+    T* dp = buf + lane * stage_stride<T>();
 #pragma unroll
-    for (int j = 0; j < 32 / EPC; ++j) {
+    for (int j = 0; j < 64 / EPC; ++j) {
       int bytes = (n - c0 - j * EPC) * (int)sizeof(T);
       bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
       const unsigned sa = (unsigned)__cvta_generic_to_shared(dp + j * EPC);
@@ -230,91 +144,197 @@ __device__ __forceinline__ void wait_staged() {
   __syncwarp();
 }
 
-// Dense tail solves (see the comment above block_column_update).  The factor
-// is read-only here, so its loads run ahead of the values they multiply:
-// every thread issues its first update row of block column k before waiting
-// for block k's diagonal solve, and warp 0 stages block k+1's diagonal block
-// in shared memory (cp.async) right after solving block k.  dbuf: 32 x
-// diag_stride shared-memory scratch.
+// Dense tail solves, y <- U^-1 L^-1 y on 32-wide block columns, pipelined.
+// In step k of the forward pass warp 0 applies block k's solution x_k to
+// the 32 rows of block k+1 and solves block k+1's diagonal block (from a
+// 32 x 64 tile [L(k+1,k) | L(k+1,k+1)] staged one step ahead), while warps
+// 1..7 apply x_k to every row below block k+1; one barrier per step.  The
+// backward pass mirrors it (rows above, U, reciprocal pivots computed per
+// lane).  x alternates between two 32-entry buffers in s_blk[0..63].
 template <typename T>
 __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld, T* __restrict__ yg, T* s_blk, T* ys,
-                                          T* dbuf) {
-  constexpr int DS = diag_stride<T>();
-  constexpr bool PFROW = sizeof(T) == 4;  // row prefetch in registers (FP32 only: register budget)
+                                          T* sbuf) {
+  constexpr int SS = stage_stride<T>();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (ys != yg) {
     for (int i = tid; i < n; i += BS) ys[i] = yg[i];
     __syncthreads();
   }
   const int nblk = (n + 31) / 32;
-  Seg32<T> seg;
   // ---- forward, unit lower ----
-  if (warp == 0) stage_diag<T>(dbuf, A, ld, n, 0, min(32, n), lane);
-  for (int k = 0; k < nblk; ++k) {
-    const int c0 = 32 * k, cb = min(32, n - c0);
-    const int r0 = c0 + cb;
-    const bool full = cb == 32;
-    const int i = r0 + tid;
-    if (PFROW && full && i < n) seg.load(A + (int64_t)i * ld + c0);
+  // prologue: solve block 0 (tile = [L(0,0) | ...], diagonal at column 0)
+  if (warp == 0) {
+    stage_tile32x64<T>(sbuf, A, ld, n, 0, min(32, n), 0, lane);
+    wait_staged();
+    const int cb = min(32, n);
+    T v = lane < cb ? ys[lane] : T(0);
+    const T* dr = sbuf + lane * SS;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      const T a = (lane < cb && c < lane) ? dr[c] : T(0);
+      v = fma(-a, __shfl_sync(0xffffffffu, v, c), v);
+    }
+    if (lane < cb) {
+      ys[lane] = v;
+      s_blk[lane] = v;
+    }
+    __syncwarp();
+    // tile of block 1: [L(1,0) | L(1,1)]
+    if (nblk > 1) stage_tile32x64<T>(sbuf, A, ld, n, 32, min(32, n - 32), 0, lane);
+  }
+  __syncthreads();
+  for (int k = 0; k + 1 < nblk; ++k) {
+    const int c0 = 32 * k;           // block k columns
+    const int r1 = c0 + 32;          // block k+1 rows
+    const int nb1 = min(32, n - r1);
+    const T* xk = s_blk + 32 * (k & 1);
+    T* xn = s_blk + 32 * ((k + 1) & 1);
     if (warp == 0) {
       wait_staged();
-      T v = lane < cb ? ys[c0 + lane] : T(0);
-      const T* dr = dbuf + lane * DS;
+      const T* tr = sbuf + lane * SS;  // row r1 + lane: [L(k+1,k) | L(k+1,k+1)]
+      T v = T(0);
+      if (lane < nb1) {
+        T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+        for (int c = 0; c < 32; c += 2) {
+          acc0 = fma(tr[c], xk[c], acc0);
+          acc1 = fma(tr[c + 1], xk[c + 1], acc1);
+        }
+        v = ys[r1 + lane] - (acc0 + acc1);
+      }
 #pragma unroll
       for (int c = 0; c < 32; ++c) {
-        const T a = (lane < cb && c < lane) ? dr[c] : T(0);
+        const T a = (lane < nb1 && c < lane) ? tr[32 + c] : T(0);
         v = fma(-a, __shfl_sync(0xffffffffu, v, c), v);
       }
-      __syncwarp();  // every lane has read dbuf before it is refilled
-      if (lane < cb) {
-        ys[c0 + lane] = v;
-        s_blk[lane] = v;
+      if (lane < nb1) {
+        ys[r1 + lane] = v;
+        xn[lane] = v;
       }
-      if (k + 1 < nblk) stage_diag<T>(dbuf, A, ld, n, c0 + 32, min(32, n - c0 - 32), lane);
-    }
-    __syncthreads();
-    if (full && PFROW) {
-      if (i < n) ys[i] -= seg.dot(s_blk);
-      block_column_update<T>(A, ld, c0, cb, r0 + BS, n, s_blk, ys);
+      __syncwarp();  // every lane has read the tile before it is refilled
+      if (k + 2 < nblk) stage_tile32x64<T>(sbuf, A, ld, n, r1 + 32, min(32, n - r1 - 32), r1, lane);
     } else {
-      block_column_update<T>(A, ld, c0, cb, r0, n, s_blk, ys);
+      // rows below block k+1 take x_k (warps 1..7)
+      const int t = tid - 32;
+      for (int i = r1 + 32 + t; i < n; i += BS - 32) {
+        const T* row = A + (int64_t)i * ld + c0;
+        T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
+        if constexpr (sizeof(T) == 4) {
+          const float4* r4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+          for (int q = 0; q < 8; q += 2) {
+            const float4 u = r4[q], w = r4[q + 1];
+            acc0 = fma(u.x, xk[4 * q], acc0);
+            acc1 = fma(u.y, xk[4 * q + 1], acc1);
+            acc2 = fma(u.z, xk[4 * q + 2], acc2);
+            acc3 = fma(u.w, xk[4 * q + 3], acc3);
+            acc0 = fma(w.x, xk[4 * q + 4], acc0);
+            acc1 = fma(w.y, xk[4 * q + 5], acc1);
+            acc2 = fma(w.z, xk[4 * q + 6], acc2);
+            acc3 = fma(w.w, xk[4 * q + 7], acc3);
+          }
+        } else {
+          const double2* r2 = reinterpret_cast<const double2*>(row);
+#pragma unroll
+          for (int q = 0; q < 16; q += 2) {
+            const double2 u = r2[q], w = r2[q + 1];
+            acc0 = fma(u.x, xk[2 * q], acc0);
+            acc1 = fma(u.y, xk[2 * q + 1], acc1);
+            acc2 = fma(w.x, xk[2 * q + 2], acc2);
+            acc3 = fma(w.y, xk[2 * q + 3], acc3);
+          }
+        }
+        ys[i] -= (acc0 + acc1) + (acc2 + acc3);
+      }
     }
     __syncthreads();
   }
   // ---- backward, upper ----
+  // tile of block j: rows 32j.., columns 32j..32j+63 = [U(j,j) | U(j,j+1)]
+  const int kl = nblk - 1;
   if (warp == 0) {
-    const int c0 = 32 * (nblk - 1);
-    stage_diag<T>(dbuf, A, ld, n, c0, n - c0, lane);
+    const int c0 = 32 * kl, cb = n - c0;
+    stage_tile32x64<T>(sbuf, A, ld, n, c0, cb, c0, lane);
+    wait_staged();
+    const T* dr = sbuf + lane * SS;
+    const T rd = lane < cb ? T(1) / dr[lane] : T(1);
+    T v = lane < cb ? ys[c0 + lane] : T(0);
+#pragma unroll
+    for (int c = 31; c >= 0; --c) {
+      const T xc = __shfl_sync(0xffffffffu, v * rd, c);
+      if (lane == c) v = xc;
+      else if (lane < c) v = fma(-((lane < cb && c < cb) ? dr[c] : T(0)), xc, v);
+    }
+    if (lane < cb) {
+      ys[c0 + lane] = v;
+      s_blk[32 * (kl & 1) + lane] = v;
+    }
+    __syncwarp();
+    if (kl > 0) stage_tile32x64<T>(sbuf, A, ld, n, c0 - 32, 32, c0 - 32, lane);
   }
-  for (int k = nblk - 1; k >= 0; --k) {
-    const int c0 = 32 * k, cb = min(32, n - c0);
-    const bool full = cb == 32;
-    if (PFROW && full && tid < c0) seg.load(A + (int64_t)tid * ld + c0);
+  __syncthreads();
+  for (int k = kl; k > 0; --k) {
+    const int c0 = 32 * k;        // block k columns (solved)
+    const int cb = min(32, n - c0);
+    const int r1 = c0 - 32;       // block k-1 rows
+    const T* xk = s_blk + 32 * (k & 1);
+    T* xn = s_blk + 32 * ((k - 1) & 1);
     if (warp == 0) {
       wait_staged();
-      T v = lane < cb ? ys[c0 + lane] : T(0);
-      const T* dr = dbuf + lane * DS;
+      const T* tr = sbuf + lane * SS;  // row r1 + lane: [U(k-1,k-1) | U(k-1,k)]
+      T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+      for (int c = 0; c < 32; c += 2) {
+        acc0 = fma(c < cb ? tr[32 + c] : T(0), xk[c], acc0);
+        acc1 = fma(c + 1 < cb ? tr[33 + c] : T(0), xk[c + 1], acc1);
+      }
+      T v = ys[r1 + lane] - (acc0 + acc1);
+      const T rd = T(1) / tr[lane];
 #pragma unroll
       for (int c = 31; c >= 0; --c) {
-        const T a = (lane < cb && c >= lane && c < cb) ? dr[c] : T(lane == c ? 1 : 0);
-        T xc = v / a;  // meaningful on lane c only
-        xc = __shfl_sync(0xffffffffu, xc, c);
+        const T xc = __shfl_sync(0xffffffffu, v * rd, c);
         if (lane == c) v = xc;
-        else if (lane < c) v = fma(-a, xc, v);
+        else if (lane < c) v = fma(-tr[c], xc, v);
       }
-      __syncwarp();  // every lane has read dbuf before it is refilled
-      if (k > 0) stage_diag<T>(dbuf, A, ld, n, c0 - 32, 32, lane);
-      if (lane < cb) {
-        ys[c0 + lane] = v;
-        s_blk[lane] = v;
-      }
-    }
-    __syncthreads();
-    if (full && PFROW) {
-      if (tid < c0) ys[tid] -= seg.dot(s_blk);
-      block_column_update<T>(A, ld, c0, cb, BS, c0, s_blk, ys);
+      ys[r1 + lane] = v;
+      xn[lane] = v;
+      __syncwarp();
+      if (k - 1 > 0) stage_tile32x64<T>(sbuf, A, ld, n, r1 - 32, 32, r1 - 32, lane);
     } else {
-      block_column_update<T>(A, ld, c0, cb, 0, c0, s_blk, ys);
+      // rows above block k-1 take x_k (warps 1..7)
+      const int t = tid - 32;
+      for (int i = t; i < r1; i += BS - 32) {
+        const T* row = A + (int64_t)i * ld + c0;
+        T acc = T(0);
+        if (cb == 32) {
+          T acc1 = T(0), acc2 = T(0), acc3 = T(0);
+          if constexpr (sizeof(T) == 4) {
+            const float4* r4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float4 u = r4[q];
+              acc = fma(u.x, xk[4 * q], acc);
+              acc1 = fma(u.y, xk[4 * q + 1], acc1);
+              acc2 = fma(u.z, xk[4 * q + 2], acc2);
+              acc3 = fma(u.w, xk[4 * q + 3], acc3);
+            }
+          } else {
+            const double2* r2 = reinterpret_cast<const double2*>(row);
+#pragma unroll
+            for (int q = 0; q < 16; q += 2) {
+              const double2 u = r2[q], w = r2[q + 1];
+              acc = fma(u.x, xk[2 * q], acc);
+              acc1 = fma(u.y, xk[2 * q + 1], acc1);
+              acc2 = fma(w.x, xk[2 * q + 2], acc2);
+              acc3 = fma(w.y, xk[2 * q + 3], acc3);
+            }
+          }
+          acc = (acc + acc1) + (acc2 + acc3);
+        } else {
+          for (int c = 0; c < cb; ++c) acc = fma(row[c], xk[c], acc);
+        }
+        ys[i] -= acc;
+      }
     }
     __syncthreads();
   }
@@ -384,7 +404,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   __shared__ int s_ek[MAX_EDITS];
   __shared__ double2 s_ev[MAX_EDITS];
   __shared__ double s_red[NWARP];
-  __shared__ T s_blk[32];
+  __shared__ T s_blk[64];
   T* s_dense = reinterpret_cast<T*>(smem_raw);
 
   const int tid = threadIdx.x;
@@ -629,10 +649,10 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       if (P.nt > 0)
       {
         // y tail in shared memory when it fits, the diagonal-block buffer after it
-        const bool y_in_smem = P.nt + 32 * diag_stride<T>() + 32 <= dense_smem_elems<T>();
+        const bool y_in_smem = P.nt + 32 * stage_stride<T>() + 32 <= dense_smem_elems<T>();
         T* ys = y_in_smem ? s_dense : y + P.p;
-        T* dbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
-        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, ys, dbuf);
+        T* sbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
+        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, ys, sbuf);
       }
       prof.mark(PH_SOLVE_DENSE);
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
