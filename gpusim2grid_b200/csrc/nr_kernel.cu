@@ -174,10 +174,8 @@ __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld
       const T a = (lane < cb && c < lane) ? dr[c] : T(0);
       v = fma(-a, __shfl_sync(0xffffffffu, v, c), v);
     }
-    if (lane < cb) {
-      ys[lane] = v;
-      s_blk[lane] = v;
-    }
+    if (lane < cb) ys[lane] = v;
+    s_blk[lane] = lane < cb ? v : T(0);
     __syncwarp();
     // tile of block 1: [L(1,0) | L(1,1)]
     if (nblk > 1) stage_tile32x64<T>(sbuf, A, ld, n, 32, min(32, n - 32), 0, lane);
@@ -207,10 +205,8 @@ __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld
         const T a = (lane < nb1 && c < lane) ? tr[32 + c] : T(0);
         v = fma(-a, __shfl_sync(0xffffffffu, v, c), v);
       }
-      if (lane < nb1) {
-        ys[r1 + lane] = v;
-        xn[lane] = v;
-      }
+      if (lane < nb1) ys[r1 + lane] = v;
+      xn[lane] = lane < nb1 ? v : T(0);
       __syncwarp();  // every lane has read the tile before it is refilled
       if (k + 2 < nblk) stage_tile32x64<T>(sbuf, A, ld, n, r1 + 32, min(32, n - r1 - 32), r1, lane);
     } else {
@@ -265,10 +261,8 @@ __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld
       if (lane == c) v = xc;
       else if (lane < c) v = fma(-((lane < cb && c < cb) ? dr[c] : T(0)), xc, v);
     }
-    if (lane < cb) {
-      ys[c0 + lane] = v;
-      s_blk[32 * (kl & 1) + lane] = v;
-    }
+    if (lane < cb) ys[c0 + lane] = v;
+    s_blk[32 * (kl & 1) + lane] = lane < cb ? v : T(0);  // no stale entries past cb
     __syncwarp();
     if (kl > 0) stage_tile32x64<T>(sbuf, A, ld, n, c0 - 32, 32, c0 - 32, lane);
   }
@@ -285,8 +279,8 @@ __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld
       T acc0 = T(0), acc1 = T(0);
 #pragma unroll
       for (int c = 0; c < 32; c += 2) {
-        acc0 = fma(c < cb ? tr[32 + c] : T(0), xk[c], acc0);
-        acc1 = fma(c + 1 < cb ? tr[33 + c] : T(0), xk[c + 1], acc1);
+        if (c < cb) acc0 = fma(tr[32 + c], xk[c], acc0);
+        if (c + 1 < cb) acc1 = fma(tr[33 + c], xk[c + 1], acc1);
       }
       T v = ys[r1 + lane] - (acc0 + acc1);
       const T rd = T(1) / tr[lane];
