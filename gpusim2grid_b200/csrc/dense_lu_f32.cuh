@@ -5,8 +5,8 @@
 // Right-looking, 64-wide panels.  Per panel k0 (width kb; kb < 64 only for
 // the last panel, which has nothing below or to the right of it):
 //   1. the kb x kb diagonal block is copied to shared memory (identity
-//      padded to 64 x 64) and factored there by all threads, one column per
-//      step, and written back;
+//      padded to 64 x 64), factored by two warps holding one row per
+//      thread in registers, and written back;
 //   2. L21 = A21 U11^-1: one thread per row of A21, the row in registers,
 //      forward substitution against U11 rows read as broadcast float4;
 //   3. U12 = L11^-1 A12: one thread per column of A12, the column in
@@ -36,6 +36,9 @@ constexpr int SD = KP + 4;      // diagonal block stride (16-byte rows)
 constexpr int TM = 128, TN = 128;
 constexpr int SA = KP + 4;      // A tile [TM][SA]
 constexpr int SB = TN + 4;      // B tile [KP][SB]
+#ifndef GS2G_DENSE32_EPI_ROWS
+#define GS2G_DENSE32_EPI_ROWS 2  // rows per epilogue batch (1, 2, 4 or 8)
+#endif
 
 struct Smem {
   static constexpr int d_elems = KP * SD;
@@ -110,6 +113,15 @@ __device__ __noinline__ void trailing_update(float* A22, const float* A21, const
     const int i0 = (t / n_tj) * TM, j0 = (t % n_tj) * TN;
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    // bring this tile's output rows toward L2 while the tile computes
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = i0 + tr + 16 * i;
+      if (r < M && j0 + 4 * tc < N)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(A22 + (int64_t)r * ld + j0 + 4 * tc));
+      if (r < M && j0 + 64 + 4 * tc < N)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(A22 + (int64_t)r * ld + j0 + 64 + 4 * tc));
+    }
     float acc[8][8];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -133,25 +145,39 @@ __device__ __noinline__ void trailing_update(float* A22, const float* A21, const
       const int t1 = t + 1;
       stage_tile(sA, sB, A21, A12, ld, M, N, (t1 / n_tj) * TM, (t1 % n_tj) * TN);
     }
+    // epilogue in batches of EB rows: all loads of a batch are issued before
+    // its stores (the compiler cannot reorder them across the stores)
+    constexpr int EB = GS2G_DENSE32_EPI_ROWS;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = i0 + tr + 16 * i;
-      if (r >= M) continue;
-      float* crow = A22 + (int64_t)r * ld + j0;
+    for (int ib = 0; ib < 8; ib += EB) {
+      float4 cv[EB][2];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c = 64 * h + 4 * tc;
-        if (j0 + c + 3 < N) {
-          float4 v = *reinterpret_cast<const float4*>(crow + c);
-          v.x -= acc[i][4 * h];
-          v.y -= acc[i][4 * h + 1];
-          v.z -= acc[i][4 * h + 2];
-          v.w -= acc[i][4 * h + 3];
-          *reinterpret_cast<float4*>(crow + c) = v;
-        } else {
+      for (int i = 0; i < EB; ++i) {
+        const int r = i0 + tr + 16 * (ib + i);
 #pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (j0 + c + e < N) crow[c + e] -= acc[i][4 * h + e];
+        for (int h = 0; h < 2; ++h) {
+          const int c = j0 + 64 * h + 4 * tc;
+          cv[i][h] = (r < M && c + 3 < N) ? *reinterpret_cast<const float4*>(A22 + (int64_t)r * ld + c)
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < EB; ++i) {
+        const int r = i0 + tr + 16 * (ib + i);
+        if (r >= M) continue;
+        float* crow = A22 + (int64_t)r * ld;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int c = j0 + 64 * h + 4 * tc;
+          const float* a = acc[ib + i] + 4 * h;
+          if (c + 3 < N) {
+            *reinterpret_cast<float4*>(crow + c) =
+                make_float4(cv[i][h].x - a[0], cv[i][h].y - a[1], cv[i][h].z - a[2], cv[i][h].w - a[3]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (c + e < N) crow[c + e] -= a[e];
+          }
         }
       }
     }
@@ -160,30 +186,52 @@ __device__ __noinline__ void trailing_update(float* A22, const float* A21, const
 }
 
 // Factor the identity-padded 64 x 64 block D (stride SD) in place; rp gets
-// the reciprocal pivots.  One column per step, two barriers per step:
-//   phase 1 (D[j][j] final): every thread derives the pivot, the threads
-//            holding column j below the diagonal scale it;
-//   phase 2: thread 0 stores the pivot and its reciprocal (nobody reads
-//            them in this phase); rows j+1.. take the rank-1 update, each
-//            thread one fixed column and every fourth row.
+// the reciprocal pivots.  Warps 0 and 1 hold one row each in registers
+// (thread r: row r).  Step j: thread j clamps its pivot and publishes its
+// row (final: L part, pivot, U part) to D; a 64-thread named barrier; rows
+// below j take l = x_j / u_jj and x_c -= l u_jc (c > j), reading row j as
+// broadcast float4.  One lightweight barrier per step; warps 2..7 skip.
 __device__ __noinline__ void factor_diag(float* D, float* rp, double pfloor) {
-  const int tid = threadIdx.x;
-  const int c = tid & (KP - 1), r0 = tid >> 6;  // column, first row offset (0..3)
-  for (int j = 0; j < KP; ++j) {
-    const float piv = clamp_piv(D[j * SD + j], pfloor);
-    const float r = 1.f / piv;
-    if (tid > j && tid < KP) D[tid * SD + j] *= r;
-    __syncthreads();
-    if (tid == 0) {
-      D[j * SD + j] = piv;
-      rp[j] = r;
+  const int r = threadIdx.x;
+  if (r < KP) {
+    float x[KP];
+#pragma unroll
+    for (int q = 0; q < KP / 4; ++q) {
+      const float4 v = lds4(D + r * SD + 4 * q);
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
     }
-    if (c > j) {
-      const float ujc = D[j * SD + c];
-      for (int i = j + 1 + r0; i < KP; i += 4) D[i * SD + c] = fmaf(-D[i * SD + j], ujc, D[i * SD + c]);
+    asm volatile("bar.sync 1, 64;\n" ::: "memory");  // all rows read before any is rewritten
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+      if (r == j) {
+        x[j] = clamp_piv(x[j], pfloor);
+        rp[j] = 1.f / x[j];
+#pragma unroll
+        for (int q = 0; q < KP / 4; ++q)
+          *reinterpret_cast<float4*>(D + j * SD + 4 * q) = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+      }
+      asm volatile("bar.sync 1, 64;\n" ::: "memory");
+      if (r > j) {
+        const float* uj = D + j * SD;
+        const float l = x[j] * (1.f / lds1(uj + j));
+        x[j] = l;
+#pragma unroll
+        for (int c = j + 1; c < KP && (c & 3); ++c) x[c] = fmaf(-l, lds1(uj + c), x[c]);
+#pragma unroll
+        for (int c4 = ((j + 1) + 3) & ~3; c4 < KP; c4 += 4) {
+          const float4 u = lds4(uj + c4);
+          x[c4] = fmaf(-l, u.x, x[c4]);
+          x[c4 + 1] = fmaf(-l, u.y, x[c4 + 1]);
+          x[c4 + 2] = fmaf(-l, u.z, x[c4 + 2]);
+          x[c4 + 3] = fmaf(-l, u.w, x[c4 + 3]);
+        }
+      }
     }
-    __syncthreads();
   }
+  __syncthreads();
 }
 
 // x <- x M^-1 for the 64 values x of one thread, M upper triangular given by
