@@ -82,23 +82,56 @@ __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
   return piv;
 }
 
-// Sum of the Schur contributions of column group g (see Plan::sg_ptr).
-// Entries have width w <= 15 (1 or 2 here: supernodes are buses); the first
-// two products are loaded together.
+// Contribution of one Schur entry (see Plan::se_rec): sum_{c<w} L[c] U[c t].
+// w <= 15 (1 or 2 here: supernodes are buses); the first two products are
+// loaded together.
 template <typename T>
-__device__ __forceinline__ T schur_group(const DevPlan& P, const T* __restrict__ HV, int g) {
-  T acc = T(0);
-  const int e1 = P.se_ptr[g + 1];
-  for (int e = P.se_ptr[g]; e < e1; ++e) {
-    const T* Lr = HV + P.se_L[e];
-    const T* Ub = HV + P.se_U[e];
-    const int wt = P.se_wt[e], w = wt & 15, t = wt >> 4;
-    const T l0 = Lr[0], u0 = Ub[0];
-    const T l1 = w > 1 ? Lr[1] : T(0), u1 = w > 1 ? Ub[t] : T(0);
-    acc += l0 * u0 + l1 * u1;
-    for (int c = 2; c < w; ++c) acc += Lr[c] * Ub[c * t];
-  }
+__device__ __forceinline__ T schur_entry(const T* __restrict__ HV, int4 rec) {
+  const T* Lr = HV + rec.x;
+  const T* Ub = HV + rec.y;
+  const int w = rec.z & 15, t = rec.z >> 4;
+  const T l0 = Lr[0], u0 = Ub[0];
+  const T l1 = w > 1 ? Lr[1] : T(0), u1 = w > 1 ? Ub[t] : T(0);
+  T acc = l0 * u0 + l1 * u1;
+  for (int c = 2; c < w; ++c) acc += Lr[c] * Ub[c * t];
   return acc;
+}
+
+// Schur update of the dense tail: warp per tail row, lane per column group
+// (each lane sums every contribution to one entry S[ti][col] and writes it
+// once), four groups per lane in flight: their entry records are loaded
+// together, then their factor values.
+template <typename T>
+__device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__ HV, T* __restrict__ S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int ti = warp; ti < P.nt; ti += NWARP) {
+    T* Srow = S + (int64_t)ti * P.ld;
+    const int g0 = P.sg_ptr[ti], g1 = P.sg_ptr[ti + 1];
+    for (int gb = g0; gb < g1; gb += 128) {
+      int ge[4], e0[4], e1[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        ge[u] = gb + lane + 32 * u;
+        const bool in = ge[u] < g1;
+        e0[u] = in ? P.se_ptr[ge[u]] : 0;
+        e1[u] = in ? P.se_ptr[ge[u] + 1] : 0;
+      }
+      T acc[4] = {T(0), T(0), T(0), T(0)};
+      // first entry of each group (nearly every group has one or two)
+      int4 rec[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) rec[u] = e0[u] < e1[u] ? P.se_rec[e0[u]] : make_int4(0, 0, 0, 0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (e0[u] < e1[u]) acc[u] = schur_entry<T>(HV, rec[u]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        for (int e = e0[u] + 1; e < e1[u]; ++e) acc[u] += schur_entry<T>(HV, P.se_rec[e]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (ge[u] < g1) Srow[P.sg_col[ge[u]]] -= acc[u];
+    }
+  }
 }
 
 // Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on the
@@ -594,22 +627,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
 
       prof.mark(PH_HEAD);
       // ---- Schur update of the dense tail ----------------------------------
-      // warp per tail row, lane per column group: each lane sums every
-      // contribution to one entry S[ti][col] and writes it once; two groups
-      // per lane at a time keep more independent loads in flight
-      {
-        const int lane = tid & 31, warp = tid >> 5;
-        for (int ti = warp; ti < P.nt; ti += NWARP) {
-          T* Srow = S + (int64_t)ti * P.ld;
-          const int g1 = P.sg_ptr[ti + 1];
-          for (int g = P.sg_ptr[ti] + lane; g < g1; g += 64) {
-            const bool two = g + 32 < g1;
-            T acc0 = schur_group<T>(P, HV, g), acc1 = two ? schur_group<T>(P, HV, g + 32) : T(0);
-            Srow[P.sg_col[g]] -= acc0;
-            if (two) Srow[P.sg_col[g + 32]] -= acc1;
-          }
-        }
-      }
+      schur_update<T>(P, HV, S);
       __syncthreads();
 
       prof.mark(PH_SCHUR);

@@ -40,9 +40,7 @@ struct DevPlan {
   const int* sg_ptr;  // [nt + 1] Schur column groups per tail row
   const int* sg_col;  // tail column of each group
   const int* se_ptr;  // [groups + 1] entries per group
-  const int* se_L;    // HV offset of the L values of each entry
-  const int* se_U;    // HV offset of the first U value of each entry
-  const int* se_wt;   // w | t << 4 (U stride t)
+  const int4* se_rec;  // per entry: HV offset of its L values, of its first U value, w | t << 4 (U stride t)
   const int* fw_ptr;  // [dim + 1]
   const int* fw_col;
   const int* fw_pos;

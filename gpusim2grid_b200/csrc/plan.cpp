@@ -545,6 +545,13 @@ Plan build_plan(int n_bus, const int* ybus_indptr, const int* ybus_indices,
       if (!ents.empty()) P.se_ptr.push_back((int)P.se_L.size());
       P.sg_ptr[ti + 1] = (int)P.sg_col.size();
     }
+    P.se_rec.resize(4 * P.se_L.size());
+    for (size_t e = 0; e < P.se_L.size(); ++e) {
+      P.se_rec[4 * e] = P.se_L[e];
+      P.se_rec[4 * e + 1] = P.se_U[e];
+      P.se_rec[4 * e + 2] = P.se_wt[e];
+      P.se_rec[4 * e + 3] = 0;
+    }
   }
   for (int64_t k = 0; k < P.nt; ++k) P.dense_madds += (P.nt - 1 - k) * (P.nt - 1 - k);
 

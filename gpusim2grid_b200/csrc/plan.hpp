@@ -87,6 +87,7 @@ struct Plan {
   //   sum_{c < w} HV[se_L[e] + c] * HV[se_U[e] + c * t],  w | t << 4 = se_wt[e]
   // (entries of a group in supernode order).
   std::vector<int> sg_ptr, sg_col, se_ptr, se_L, se_U, se_wt;
+  std::vector<int> se_rec;  // [4 * entries]: (se_L, se_U, se_wt, 0) packed for one 16-byte load
   int64_t schur_madds = 0, schur_volume = 0;
   int64_t dense_madds = 0;
 

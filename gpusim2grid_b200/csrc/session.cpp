@@ -158,9 +158,7 @@ void upload_plan(gs2g_session* s) {
   D.sg_ptr = upload_vec(s, P.sg_ptr);
   D.sg_col = upload_vec(s, P.sg_col);
   D.se_ptr = upload_vec(s, P.se_ptr);
-  D.se_L = upload_vec(s, P.se_L);
-  D.se_U = upload_vec(s, P.se_U);
-  D.se_wt = upload_vec(s, P.se_wt);
+  D.se_rec = reinterpret_cast<const int4*>(upload_vec(s, P.se_rec));
   D.fw_ptr = upload_vec(s, P.fw_ptr);
   D.fw_col = upload_vec(s, P.fw_col);
   D.fw_pos = upload_vec(s, P.fw_pos);
