@@ -86,6 +86,8 @@ struct gs2g_session {
   std::vector<int> br_from, br_to;
   std::vector<double> yff, yft, ytf, ytt;
   std::vector<int> k_ff, k_tt, k_ft, k_tf;  // Ybus entry of each branch term
+  std::vector<uint8_t> is_bridge;           // branch whose loss alone islands the grid
+  int base_components = 1;                  // connected components of the branch graph
 
   // row definitions
   int n_ctg = 0;
@@ -191,6 +193,64 @@ struct DSU {
   }
 };
 
+// Bridges of the branch graph (Tarjan's low-link, iterative, over branch ids
+// so parallel branches are never bridges) and its component count.  A row
+// that trips a bridge islands the grid; a row that trips one non-bridge
+// branch does not, so the per-row connectivity check runs only for rows
+// that trip two or more non-bridge branches.
+void compute_bridges(gs2g_session* s) {
+  const int n = s->n_bus, m = s->n_branch;
+  std::vector<int> deg(n + 1, 0);
+  for (int l = 0; l < m; ++l) {
+    ++deg[s->br_from[l] + 1];
+    ++deg[s->br_to[l] + 1];
+  }
+  for (int v = 0; v < n; ++v) deg[v + 1] += deg[v];
+  std::vector<int> adj_v(2 * m), adj_e(2 * m), fill(deg.begin(), deg.end() - 1);
+  for (int l = 0; l < m; ++l) {
+    const int f = s->br_from[l], t = s->br_to[l];
+    adj_v[fill[f]] = t;
+    adj_e[fill[f]++] = l;
+    adj_v[fill[t]] = f;
+    adj_e[fill[t]++] = l;
+  }
+  s->is_bridge.assign(m, 0);
+  std::vector<int> tin(n, -1), low(n, 0), it(n, 0), pe(n, -1);
+  std::vector<int> stack;
+  int timer = 0, comps = 0;
+  for (int root = 0; root < n; ++root) {
+    if (tin[root] >= 0) continue;
+    ++comps;
+    stack.push_back(root);
+    tin[root] = low[root] = timer++;
+    it[root] = deg[root];
+    while (!stack.empty()) {
+      const int v = stack.back();
+      if (it[v] < deg[v + 1]) {
+        const int k = it[v]++;
+        const int w = adj_v[k], e = adj_e[k];
+        if (e == pe[v]) continue;
+        if (tin[w] < 0) {
+          pe[w] = e;
+          tin[w] = low[w] = timer++;
+          it[w] = deg[w];
+          stack.push_back(w);
+        } else {
+          low[v] = std::min(low[v], tin[w]);
+        }
+      } else {
+        stack.pop_back();
+        if (!stack.empty()) {
+          const int u = stack.back();
+          low[u] = std::min(low[u], low[v]);
+          if (low[v] > tin[u]) s->is_bridge[pe[v]] = 1;
+        }
+      }
+    }
+  }
+  s->base_components = comps;
+}
+
 void assemble_rows(gs2g_session* s) {
   if (!s->rows_dirty) return;
   const int n = s->n_bus;
@@ -223,15 +283,20 @@ void assemble_rows(gs2g_session* s) {
       std::sort(uniq.begin(), uniq.end());
       uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
       if (!uniq.empty()) {
-        DSU d(n);
-        size_t ui = 0;
-        int comps = n;
-        for (int l = 0; l < s->n_branch; ++l) {
-          while (ui < uniq.size() && uniq[ui] < l) ++ui;
-          if (ui < uniq.size() && uniq[ui] == l) continue;
-          if (d.u(s->br_from[l], s->br_to[l])) --comps;
+        bool island = s->base_components > 1;
+        for (size_t q = 0; q < uniq.size() && !island; ++q) island = s->is_bridge[uniq[q]] != 0;
+        if (!island && uniq.size() >= 2) {
+          DSU d(n);
+          size_t ui = 0;
+          int comps = n;
+          for (int l = 0; l < s->n_branch; ++l) {
+            while (ui < uniq.size() && uniq[ui] < l) ++ui;
+            if (ui < uniq.size() && uniq[ui] == l) continue;
+            if (d.u(s->br_from[l], s->br_to[l])) --comps;
+          }
+          island = comps > 1;
         }
-        if (comps > 1) {
+        if (island) {
           skip[r] = 1;
           any_skip = true;
           eptr[r + 1] = (int)ek.size();
@@ -591,6 +656,7 @@ int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const i
   s->k_tt.swap(ktt);
   s->k_ft.swap(kft);
   s->k_tf.swap(ktf);
+  compute_bridges(s);
   s->rows_dirty = true;
   GS2G_CATCH
 }

@@ -108,3 +108,24 @@ def test_injection_6500_full_size_properties(g6500, precision):
         F = O.mismatch(Y, sw.V_results[r], (p[r] + 1j * q[r]) / g6500.sn_mva, pvpq, pq_)
         assert abs(np.abs(F).max() - sw.last_residuals()[r]) < 1e-10
         assert np.abs(F).max() < 1e-8
+
+
+def test_islanding_flags_every_single_and_some_double_outages(g118):
+    """Single outages are flagged from the bridges of the branch graph,
+    multi-branch outages by a connectivity check: both must agree with the
+    oracle's connectivity check for every single-branch row and for double
+    outages that include non-bridge pairs."""
+    m = g118.n_branch
+    rows = [[b] for b in range(m)]
+    rng = np.random.default_rng(7)
+    for _ in range(64):
+        rows.append(sorted(int(v) for v in rng.choice(m, 2, replace=False)))
+    ca = ContingencyAnalysisGPU(g118.as_tuple(), init_from_n_powerflow=False, nb_iter=10, scheduling="continuous",
+                                start="flat")
+    ca.set_branch_data(*g118.branch_data())
+    ca.add_contingencies_by_branch_id(rows)
+    ca.compute()
+    st = ca.get_row_status()
+    for r, ids in enumerate(rows):
+        islanded = bool(O.islands(g118.n_bus, g118.branch_from, g118.branch_to, ids))
+        assert (st[r] == RowStatus.NOT_SIMULATED) == islanded, (r, ids)
