@@ -31,7 +31,7 @@ from ._common import (BatchTimings, RowStatus, default_tol, grid_arrays, make_se
                       resolve_scheduling)
 from ._native import lib
 
-__all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU"]
+__all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU", "compute_many"]
 
 _START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS, "learned": lib.START_ROWS}
 _STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE}
@@ -353,3 +353,51 @@ class ScenarioSweepGPU(InjectionSweepGPU):
     def get_disconnected(self):
         """(n_rows,) bool: rows whose topology islands the grid (never solved)."""
         return self.get_row_status() == RowStatus.NOT_SIMULATED
+
+
+def compute_many(sweeps, batch_size=0):
+    """Solve the current rows of several sweeps -- any mix of grids, each
+    facade with its own grid, rows and start -- in ONE persistent kernel
+    launch (``gs2g_run_multi``): the launch's CTAs take rows from one queue
+    across the grids, each row on its own grid's symbolic plan, so a batch
+    of small and large grids keeps every SM busy until the whole batch
+    drains.  Precision, ``nb_iter``, ``tol``, scheduling and strategy must
+    agree across the sweeps.  Afterwards every facade reads its own results
+    as after its own ``compute()``; returns the launch's kernel time (ms)."""
+    sweeps = list(sweeps)
+    if not sweeps:
+        raise ValueError("compute_many needs at least one sweep")
+    f0 = sweeps[0]
+    for f in sweeps[1:]:
+        if (f._prec, f.nb_iter, f.tol, f.scheduling, f._strategy) != (f0._prec, f0.nb_iter, f0.tol, f0.scheduling,
+                                                                      f0._strategy):
+            raise ValueError("compute_many: precision, nb_iter, tol, scheduling and strategy must agree")
+    starts = {f._start for f in sweeps}
+    if len(starts) != 1:
+        raise ValueError("compute_many: every sweep must use the same start")
+    start = starts.pop()
+    t0 = time.perf_counter()
+    ratio, reuse = float(f0.refactor_ratio), int(f0.max_reuse)
+    if start == "learned":
+        import torch
+        for f in sweeps:
+            sbus, trips, n = f._row_defs()
+            f._learned.start_voltages(sbus, trips, n, out_ptr=f._s.start_rows_buffer(n))
+        torch.cuda.current_stream().synchronize()
+        for f in sweeps:
+            f._learned.net.check()
+        ratio, reuse = f0._learned_opts
+    lib.run_multi([f._s for f in sweeps], f0.nb_iter, f0.tol, f0.scheduling == "chunked", f0._prec, _START[start],
+                  0.0, max(int(batch_size), 0), False, _STRATEGY[f0._strategy], ratio, reuse,
+                  start in ("rows", "learned"))
+    total_ms = (time.perf_counter() - t0) * 1e3
+    kernel_ms = 0.0
+    for f in sweeps:
+        tm = f._s.timings()
+        kernel_ms = tm["kernel_ms"]
+        f._timings = BatchTimings(n_rows=f._s.n_rows(), total_iters=int(tm["total_iters"]), t_plan_ms=tm["plan_ms"],
+                                  t_upload_ms=tm["upload_ms"], t_kernel_ms=tm["kernel_ms"], t_total_ms=total_ms)
+        f._ran = True
+        f._host = None
+    return kernel_ms
+

@@ -420,23 +420,26 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
   return w;
 }
 
+// Shared-memory scratch of one CTA, handed to solve_row.
 template <typename T>
-#ifndef GS2G_MIN_CTAS_PER_SM
-#define GS2G_MIN_CTAS_PER_SM 2
-#endif
-__global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const DevPlan P, const SweepArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_row;
-  __shared__ int s_ne;
-  __shared__ int s_ek[MAX_EDITS];
-  __shared__ double2 s_ev[MAX_EDITS];
-  __shared__ double s_red[NWARP];
-  __shared__ T s_blk[64];
-  T* s_dense = reinterpret_cast<T*>(smem_raw);
+struct RowShared {
+  int* s_ne;
+  int* s_ek;
+  double2* s_ev;
+  double* s_red;
+  T* s_blk;
+  T* s_dense;
+};
 
+// The whole Newton loop of one row of one grid, by the calling CTA: start
+// voltage, edits, mismatch / Jacobian / factorization / solves / update
+// until the row converges, diverges or uses its budget (with the optional
+// rescue attempt), then the row's outputs.  ws: the CTA's workspace.
+template <typename T>
+__device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, const int row, char* ws,
+                                          const RowShared<T>& sh, PhaseProf& prof) {
   const int tid = threadIdx.x;
   const WsLayout L = ws_layout<T>(P);
-  char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   double2* V = reinterpret_cast<double2*>(ws + L.V);
   double2* I = reinterpret_cast<double2*>(ws + L.I);
   double* F = reinterpret_cast<double*>(ws + L.F);
@@ -445,17 +448,12 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   T* y = reinterpret_cast<T*>(ws + L.y);
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const int n = P.n_bus;
-  PhaseProf prof;
-  prof.init(a.phase_cycles != nullptr && tid == 0);
-
-  for (;;) {
-    if (tid == 0) s_row = atomicAdd(a.queue, 1);
-    __syncthreads();
-    const int row = s_row;
-    if (row >= a.n_rows) {
-      prof.flush(a.phase_cycles);
-      return;
-    }
+  int& s_ne = *sh.s_ne;
+  int* s_ek = sh.s_ek;
+  double2* s_ev = sh.s_ev;
+  double* s_red = sh.s_red;
+  T* s_blk = sh.s_blk;
+  T* s_dense = sh.s_dense;
     double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
 
     if (a.row_skip != nullptr && a.row_skip[row]) {
@@ -466,7 +464,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
         a.iters_out[row] = 0;
       }
       __syncthreads();
-      continue;
+      return;
     }
     if (tid == 0) {
       int ne = 0;
@@ -712,6 +710,76 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
       if (a.factors_out != nullptr) a.factors_out[row] = n_factor;
     }
     __syncthreads();
+}
+
+template <typename T>
+#ifndef GS2G_MIN_CTAS_PER_SM
+#define GS2G_MIN_CTAS_PER_SM 2
+#endif
+__global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const DevPlan P, const SweepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_row;
+  __shared__ int s_ne;
+  __shared__ int s_ek[MAX_EDITS];
+  __shared__ double2 s_ev[MAX_EDITS];
+  __shared__ double s_red[NWARP];
+  __shared__ T s_blk[64];
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw)};
+  char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
+  PhaseProf prof;
+  prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
+  for (;;) {
+    if (threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
+    __syncthreads();
+    const int row = s_row;
+    if (row >= a.n_rows) {
+      prof.flush(a.phase_cycles);
+      return;
+    }
+    solve_row<T>(P, a, row, ws, sh, prof);
+  }
+}
+
+// One persistent launch over the rows of several grids: row r of the
+// launch is row r - row_begin[g] of grid g (row_begin ascending, n_grids
+// <= MAX_GRIDS).  A CTA loads a grid's plan and arguments into shared
+// memory when its next row belongs to another grid than its last one; the
+// workspace stride covers the largest grid.
+template <typename T>
+__global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
+    sweep_kernel_multi(const GridEntry* __restrict__ grids, int n_grids, const int* __restrict__ row_begin,
+                       int n_rows, int* queue, char* workspace, int64_t ws_stride, unsigned long long* phase_cycles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_row;
+  __shared__ int s_ne;
+  __shared__ int s_ek[MAX_EDITS];
+  __shared__ double2 s_ev[MAX_EDITS];
+  __shared__ double s_red[NWARP];
+  __shared__ T s_blk[64];
+  __shared__ __align__(16) GridEntry s_grid;
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw)};
+  char* ws = workspace + (int64_t)blockIdx.x * ws_stride;
+  PhaseProf prof;
+  prof.init(phase_cycles != nullptr && threadIdx.x == 0);
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_row = atomicAdd(queue, 1);
+    __syncthreads();
+    const int row = s_row;
+    if (row >= n_rows) {
+      prof.flush(phase_cycles);
+      return;
+    }
+    int g = 0;
+    while (g + 1 < n_grids && row >= row_begin[g + 1]) ++g;
+    if (g != cur) {
+      const int* src = reinterpret_cast<const int*>(grids + g);
+      int* dst = reinterpret_cast<int*>(&s_grid);
+      for (int i = threadIdx.x; i < (int)(sizeof(GridEntry) / sizeof(int)); i += BS) dst[i] = src[i];
+      __syncthreads();
+      cur = g;
+    }
+    solve_row<T>(s_grid.P, s_grid.a, row - row_begin[g], ws, sh, prof);
   }
 }
 
@@ -733,7 +801,12 @@ cudaError_t opt_in_smem() {
   cudaError_t e = cudaFuncSetAttribute(sweep_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        smem_bytes<float>());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(sweep_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(sweep_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<double>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_kernel_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem_bytes<float>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(sweep_kernel_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               smem_bytes<double>());
 }
 }  // namespace
@@ -749,6 +822,22 @@ int sweep_ctas(int prec, int device) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<double>, BS, smem_bytes<double>());
   if (per_sm < 1) per_sm = 1;
   return n_sm * per_sm;
+}
+
+int launch_sweep_multi(const GridEntry* d_grids, int n_grids, const int* d_row_begin, int n_rows, int* queue,
+                       char* workspace, int64_t ws_stride, unsigned long long* phase_cycles, int prec, int n_ctas,
+                       void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0 || n_grids <= 0 || n_grids > MAX_GRIDS) return (int)cudaErrorInvalidValue;
+  const cudaError_t e = opt_in_smem();
+  if (e != cudaSuccess) return (int)e;
+  if (prec == 1)
+    sweep_kernel_multi<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(d_grids, n_grids, d_row_begin, n_rows, queue,
+                                                                       workspace, ws_stride, phase_cycles);
+  else
+    sweep_kernel_multi<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(d_grids, n_grids, d_row_begin, n_rows,
+                                                                         queue, workspace, ws_stride, phase_cycles);
+  return (int)cudaGetLastError();
 }
 
 int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {

@@ -113,6 +113,22 @@ int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
 // CTAs that fit at once for `prec` (for sizing the workspace).
 int sweep_ctas(int prec, int device);
 
+// Several grids in one persistent launch (see sweep_kernel_multi): the plan
+// and the per-grid launch arguments of each grid (SweepArgs fields n_rows,
+// ybus, v0, sbus, edits, skip, options and outputs; its queue, workspace and
+// phase_cycles are not used).
+constexpr int MAX_GRIDS = 16;
+struct GridEntry {
+  DevPlan P;
+  SweepArgs a;
+};
+// d_grids [n_grids] and d_row_begin [n_grids + 1] in device memory; queue
+// zeroed by the caller; workspace n_ctas * ws_stride bytes, ws_stride >=
+// workspace_bytes of every grid.
+int launch_sweep_multi(const GridEntry* d_grids, int n_grids, const int* d_row_begin, int n_rows, int* queue,
+                       char* workspace, int64_t ws_stride, unsigned long long* phase_cycles, int prec, int n_ctas,
+                       void* stream);
+
 // Size of the file-scope device array the allocation-free sweep uses as its
 // scratch (row queue + per-CTA workspaces).
 constexpr int64_t kStaticScratchBytes = int64_t(64) << 20;

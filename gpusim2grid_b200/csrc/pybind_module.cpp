@@ -384,6 +384,25 @@ py::dict plan_info(int n_bus, IArr indptr, IArr indices, IArr pv, IArr pq, int t
   return d;
 }
 
+// Several sessions' current rows in one persistent launch (gs2g_run_multi).
+void run_multi(const std::vector<Session*>& sessions, int max_iter, double tol, bool fixed_iters, int precision,
+               int start, double pivot_floor, int n_ctas, bool profile, int refactor, double refactor_ratio,
+               int max_reuse, bool rescue) {
+  std::vector<gs2g_session*> hs;
+  for (Session* s : sessions) {
+    if (!s) throw py::value_error("run_multi: None in the session list");
+    hs.push_back(reinterpret_cast<gs2g_session*>(s->handle()));
+  }
+  gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
+                              refactor_ratio, max_reuse, rescue);
+  int rc;
+  {
+    py::gil_scoped_release nogil;
+    rc = gs2g_run_multi(hs.data(), (int)hs.size(), &o);
+  }
+  check(rc);
+}
+
 // ---- warm-start MLP: raw device pointers (integers) from the caller's tensors
 template <class T>
 T* P(uintptr_t p) {
@@ -450,6 +469,10 @@ PYBIND11_MODULE(_gs2g, m) {
   m.def("max_edits_per_row", &gs2g_max_edits_per_row);
   m.def("acpf_nr", &acpf_nr);
   bind_mlp(m);
+  m.def("run_multi", &run_multi, py::arg("sessions"), py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"),
+        py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0,
+        py::arg("profile") = false, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0,
+        py::arg("max_reuse") = 0, py::arg("rescue") = false);
   py::class_<Session>(m, "Session")
       .def(py::init<int, int, IArr, IArr, CArr, CArr, CArr, IArr, IArr, int>(), py::arg("device"), py::arg("n_bus"),
            py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),

@@ -104,6 +104,7 @@ struct gs2g_session {
   DevBuf d_sbus_rows, d_edit_ptr, d_edit_k, d_edit_val, d_row_skip;
   DevBuf d_v_out, d_res, d_status, d_iters, d_factors;
   DevBuf d_ws, d_queue, d_phase;
+  DevBuf d_multi;  // grid table of gs2g_run_multi (when this session leads)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
 
@@ -345,16 +346,13 @@ struct OutBufs {
   int* factors = nullptr;
 };
 
-float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
-             const double* sbus, int64_t sbus_stride, bool use_rows, const OutBufs& out, int n_ctas_req) {
+// Launch arguments of one grid's rows (everything but the queue, the
+// workspace and the phase counters).
+gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
+                          const double* sbus, int64_t sbus_stride, bool use_rows, const OutBufs& out) {
   if (o.precision != GS2G_PREC_FP64 && o.precision != GS2G_PREC_MIXED)
     throw std::invalid_argument("precision must be GS2G_PREC_FP64 or GS2G_PREC_MIXED");
   if (o.max_iter < 0) throw std::invalid_argument("max_iter must be >= 0");
-  int n_ctas = n_ctas_req > 0 ? n_ctas_req : gs2g::sweep_ctas(o.precision, s->device);
-  n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
-  const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
-  s->d_ws.ensure((size_t)wsb * n_ctas);
-  s->d_queue.ensure(2 * sizeof(int));  // [0] row queue, [1] rescue count
   gs2g::SweepArgs a{};
   a.n_rows = n_rows;
   a.ybus = s->d_ybus.as<double>();
@@ -373,9 +371,6 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   a.res_out = out.res;
   a.status_out = out.status;
   a.iters_out = out.iters;
-  a.queue = s->d_queue.as<int>();
-  a.workspace = s->d_ws.as<char>();
-  a.ws_stride = wsb;
   a.pivot_floor = o.pivot_floor;
   if (o.refactor_policy != GS2G_REFACTOR_EVERY && o.refactor_policy != GS2G_REFACTOR_ADAPTIVE)
     throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY or GS2G_REFACTOR_ADAPTIVE");
@@ -385,8 +380,22 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   a.factors_out = out.factors;
   const bool rescue = o.rescue != 0 && v0_stride != 0 && !o.fixed_iters;
   a.rescue_v0 = rescue ? s->d_vinit.as<double>() : nullptr;
-  a.n_rescued = s->d_queue.as<int>() + 1;
   a.phase_cycles = nullptr;
+  return a;
+}
+
+float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
+             const double* sbus, int64_t sbus_stride, bool use_rows, const OutBufs& out, int n_ctas_req) {
+  gs2g::SweepArgs a = make_args(s, o, n_rows, v0, v0_stride, sbus, sbus_stride, use_rows, out);
+  int n_ctas = n_ctas_req > 0 ? n_ctas_req : gs2g::sweep_ctas(o.precision, s->device);
+  n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
+  const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
+  s->d_ws.ensure((size_t)wsb * n_ctas);
+  s->d_queue.ensure(2 * sizeof(int));  // [0] row queue, [1] rescue count
+  a.queue = s->d_queue.as<int>();
+  a.workspace = s->d_ws.as<char>();
+  a.ws_stride = wsb;
+  a.n_rescued = s->d_queue.as<int>() + 1;
   if (o.profile_phases) {
     s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
     ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
@@ -814,14 +823,18 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual) {
   GS2G_CATCH
 }
 
-int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
-  GS2G_TRY
-  if (!s) throw std::invalid_argument("NULL session");
-  gs2g_run_opts o = checked(o_);
-  DeviceGuard g(s->device);
-  auto t0 = std::chrono::steady_clock::now();
-  assemble_rows(s);
-  s->tm.upload_ms = ms_since(t0);
+namespace {
+// Row sources and output buffers of a session's assembled rows.
+struct RunPrep {
+  int nr;
+  const double* v0;
+  int64_t v0s;
+  const double* sb;
+  int64_t sbs;
+  OutBufs ob;
+};
+
+RunPrep prepare_rows(gs2g_session* s, const gs2g_run_opts& o) {
   const int nr = s->n_rows;
   const int n = s->n_bus;
   const double* v0 = s->d_vinit.as<double>();
@@ -847,10 +860,104 @@ int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
   s->d_factors.ensure((size_t)std::max(nr, 1) * sizeof(int));
   OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>(),
              s->d_factors.as<int>()};
-  s->tm.kernel_ms = launch(s, o, nr, v0, v0s, sb, sbs, true, ob, o.n_ctas);
+  return RunPrep{nr, v0, v0s, sb, sbs, ob};
+}
+}  // namespace
+
+int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  gs2g_run_opts o = checked(o_);
+  DeviceGuard g(s->device);
+  auto t0 = std::chrono::steady_clock::now();
+  assemble_rows(s);
+  s->tm.upload_ms = ms_since(t0);
+  const RunPrep rp = prepare_rows(s, o);
+  const int nr = rp.nr;
+  s->tm.kernel_ms = launch(s, o, nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob, o.n_ctas);
   s->last_rows_run = nr;
   s->tm.total_ms = ms_since(t0);
   s->tm.total_iters = -1;
+  GS2G_CATCH
+}
+
+int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run_opts* o_) {
+  GS2G_TRY
+  if (!sessions || n_sessions < 1 || n_sessions > gs2g::MAX_GRIDS)
+    throw std::invalid_argument("run_multi: between 1 and " + std::to_string(gs2g::MAX_GRIDS) + " sessions");
+  for (int i = 0; i < n_sessions; ++i) {
+    if (!sessions[i]) throw std::invalid_argument("run_multi: NULL session");
+    if (sessions[i]->device != sessions[0]->device) throw std::invalid_argument("run_multi: sessions on different devices");
+    for (int j = 0; j < i; ++j)
+      if (sessions[j] == sessions[i]) throw std::invalid_argument("run_multi: a session is listed twice");
+  }
+  gs2g_run_opts o = checked(o_);
+  gs2g_session* s0 = sessions[0];
+  DeviceGuard g(s0->device);
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<gs2g::GridEntry> ge(n_sessions);
+  std::vector<int> begin(n_sessions + 1, 0);
+  int64_t wsb = 0;
+  s0->d_queue.ensure(2 * sizeof(int));
+  for (int i = 0; i < n_sessions; ++i) {
+    gs2g_session* s = sessions[i];
+    assemble_rows(s);
+    const RunPrep rp = prepare_rows(s, o);
+    ge[i].P = s->dplan;
+    ge[i].a = make_args(s, o, rp.nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
+    ge[i].a.n_rescued = s0->d_queue.as<int>() + 1;
+    begin[i + 1] = begin[i] + rp.nr;
+    wsb = std::max(wsb, gs2g::workspace_bytes(s->dplan, o.precision));
+  }
+  const double upload_ms = ms_since(t0);
+  const int total = begin[n_sessions];
+  int n_ctas = o.n_ctas > 0 ? o.n_ctas : gs2g::sweep_ctas(o.precision, s0->device);
+  n_ctas = std::max(1, std::min(n_ctas, std::max(total, 1)));
+  const size_t ge_bytes = sizeof(gs2g::GridEntry) * n_sessions;
+  s0->d_multi.ensure(ge_bytes + sizeof(int) * (n_sessions + 1));
+  ck(cudaMemcpy(s0->d_multi.p, ge.data(), ge_bytes, cudaMemcpyHostToDevice), "upload grids");
+  int* d_begin = reinterpret_cast<int*>(s0->d_multi.as<char>() + ge_bytes);
+  ck(cudaMemcpy(d_begin, begin.data(), sizeof(int) * (n_sessions + 1), cudaMemcpyHostToDevice), "upload grids");
+  s0->d_ws.ensure((size_t)wsb * n_ctas);
+  unsigned long long* phase = nullptr;
+  if (o.profile_phases) {
+    s0->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
+    ck(cudaMemsetAsync(s0->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s0->stream), "phase reset");
+    phase = s0->d_phase.as<unsigned long long>();
+  }
+  ck(cudaMemsetAsync(s0->d_queue.p, 0, 2 * sizeof(int), s0->stream), "queue reset");
+  ck(cudaEventRecord(s0->ev0, s0->stream), "event");
+  if (total > 0)
+    ck((cudaError_t)gs2g::launch_sweep_multi(reinterpret_cast<const gs2g::GridEntry*>(s0->d_multi.p), n_sessions,
+                                             d_begin, total, s0->d_queue.as<int>(), s0->d_ws.as<char>(), wsb, phase,
+                                             o.precision, n_ctas, s0->stream),
+       "multi-grid sweep launch");
+  ck(cudaEventRecord(s0->ev1, s0->stream), "event");
+  ck(cudaStreamSynchronize(s0->stream), "multi-grid sweep");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, s0->ev0, s0->ev1), "event time");
+  int rescued = 0;
+  ck(cudaMemcpy(&rescued, s0->d_queue.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost), "rescue count");
+  for (int i = 0; i < n_sessions; ++i) {
+    gs2g_session* s = sessions[i];
+    s->last_rows_run = begin[i + 1] - begin[i];
+    s->tm.kernel_ms = ms;
+    s->tm.upload_ms = upload_ms;
+    s->tm.total_ms = ms_since(t0);
+    s->tm.total_iters = -1;
+    s->tm.n_rescued = i == 0 ? rescued : 0;
+    for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
+  }
+  if (o.profile_phases) {
+    unsigned long long cyc[gs2g::N_PHASES];
+    ck(cudaMemcpy(cyc, s0->d_phase.p, sizeof(cyc), cudaMemcpyDeviceToHost), "read phases");
+    double tot = 0;
+    for (int q = 0; q < gs2g::N_PHASES; ++q) tot += (double)cyc[q];
+    for (int q = 0; q < gs2g::N_PHASES; ++q) {
+      s0->tm.phase_cycles[q] = (double)cyc[q];
+      s0->tm.phase_share[q] = tot > 0 ? cyc[q] / tot : 0;
+    }
+  }
   GS2G_CATCH
 }
 

@@ -176,6 +176,16 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual);
 
 /* Run every row.  Results stay on the device until read. */
 int gs2g_run(gs2g_session* s, const gs2g_run_opts* o);
+/* Several grids in ONE persistent launch: the current rows of every session
+ * (as gs2g_run would run them, same options for all) are solved by one
+ * kernel launch whose CTAs take rows from one queue across the grids, each
+ * with its own symbolic plan.  Results land in each session's own buffers
+ * (gs2g_get_results etc. per session).  All sessions on one device, each
+ * listed once, at most 16.  The launch runs on the first session's stream;
+ * gs2g_timings of every session get its kernel time (rescue count and phase
+ * counters on the first).  The reference runs one grid per session; this
+ * serves the heterogeneous batch (rows of 118- to 10000-bus grids). */
+int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run_opts* o);
 int gs2g_n_rows(const gs2g_session* s);
 int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters);
 /* LU factorizations each row of the last run performed. */

@@ -1,0 +1,59 @@
+"""Rows of several grids in one persistent launch (``compute_many`` /
+``gs2g_run_multi``): every row must come out exactly as when its own grid's
+sweep runs alone -- same kernel, same per-row arithmetic -- and match the
+FP64 oracle on a sample."""
+
+import numpy as np
+import pytest
+
+from conftest import TOL_V_FP64, TOL_V_MIXED
+from gpusim2grid_b200 import RowStatus, ScenarioSweepGPU, compute_many
+from gpusim2grid_b200.synthetic import grid_by_name, injection_scenarios, scenario_outages
+from oracle import nr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _sweep(g, n_rows, precision, seed):
+    sw = ScenarioSweepGPU(g.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
+                          scheduling="continuous", start="flat", strategy="adaptive")
+    sw.set_branch_data(*g.branch_data())
+    p, q = injection_scenarios(g, n_rows, seed=seed)
+    sw.set_injections(p, q, g.sn_mva)
+    sw.set_topology(scenario_outages(g, n_rows, max_trips=2, seed=seed + 1))
+    return sw, p, q
+
+
+@pytest.mark.parametrize("precision,tol_v", [("fp64", TOL_V_FP64), ("mixed", TOL_V_MIXED)])
+def test_multi_grid_launch_equals_separate_sweeps(precision, tol_v):
+    spec = [("case118_synth", 48), ("case2000_synth", 40), ("case6500_synth", 16)]
+    grids = [grid_by_name(name, 0) for name, _ in spec]
+    multi = [_sweep(g, n, precision, 20 + i)[0] for i, (g, (_, n)) in enumerate(zip(grids, spec))]
+    alone = [_sweep(g, n, precision, 20 + i) for i, (g, (_, n)) in enumerate(zip(grids, spec))]
+    ms = compute_many(multi)
+    assert ms > 0
+    for sw_m, (sw_a, p, q), g in zip(multi, alone, grids):
+        sw_a.compute()
+        np.testing.assert_array_equal(sw_m.get_row_status(), sw_a.get_row_status())
+        np.testing.assert_array_equal(sw_m.get_row_iterations(), sw_a.get_row_iterations())
+        ok = sw_a.get_row_status() == RowStatus.CONVERGED
+        assert ok.mean() > 0.9
+        np.testing.assert_array_equal(sw_m.V_results[ok], sw_a.V_results[ok])
+    # one 118-bus and one 2000-bus row against the FP64 oracle
+    for sw_m, (sw_a, p, q), g in list(zip(multi, alone, grids))[:2]:
+        st = sw_m.get_row_status()
+        r = int(np.flatnonzero(st == RowStatus.CONVERGED)[0])
+        ids = sw_m.get_topology()[r] if hasattr(sw_m, "get_topology") else sw_m._topo[r]
+        Y, V0, S, _, _, pv, pq = g.as_tuple()
+        Yr = O.trip_branches(Y, ids, g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt) if ids else Y
+        Vo, so, _, _ = O.nr_solve(Yr, V0, (p[r] + 1j * q[r]) / g.sn_mva, pv, pq, 10, 1e-8)
+        assert so == O.CONVERGED
+        assert np.abs(sw_m.V_results[r] - Vo).max() < tol_v
+
+
+def test_multi_grid_rejects_mismatched_options():
+    g = grid_by_name("case118_synth", 0)
+    a, _, _ = _sweep(g, 8, "mixed", 1)
+    b, _, _ = _sweep(g, 8, "fp64", 2)
+    with pytest.raises(ValueError):
+        compute_many([a, b])
