@@ -39,7 +39,9 @@ def test_multi_grid_launch_equals_separate_sweeps(precision, tol_v):
         ok = sw_a.get_row_status() == RowStatus.CONVERGED
         assert ok.mean() > 0.9
         np.testing.assert_array_equal(sw_m.V_results[ok], sw_a.V_results[ok])
-    # one 118-bus and one 2000-bus row against the FP64 oracle
+    # one 118-bus and one 2000-bus row against the FP64 oracle: the adaptive
+    # (chord) strategy stops at another point of the 1e-8 mismatch ball than
+    # full Newton, so the bar is the 1e-6 pu one in both precisions
     for sw_m, (sw_a, p, q), g in list(zip(multi, alone, grids))[:2]:
         st = sw_m.get_row_status()
         r = int(np.flatnonzero(st == RowStatus.CONVERGED)[0])
@@ -48,7 +50,7 @@ def test_multi_grid_launch_equals_separate_sweeps(precision, tol_v):
         Yr = O.trip_branches(Y, ids, g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt) if ids else Y
         Vo, so, _, _ = O.nr_solve(Yr, V0, (p[r] + 1j * q[r]) / g.sn_mva, pv, pq, 10, 1e-8)
         assert so == O.CONVERGED
-        assert np.abs(sw_m.V_results[r] - Vo).max() < tol_v
+        assert np.abs(sw_m.V_results[r] - Vo).max() < TOL_V_MIXED
 
 
 def test_multi_grid_rejects_mismatched_options():
