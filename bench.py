@@ -51,6 +51,10 @@ WORKLOADS = {
     "injection_sweep_case6500_synth": ("case6500_synth", "injection", 4096, 1, dict(broad=1.0, p_outage=0.0)),
     # 16384 rows on the 2000-bus grid, each a load-scaling scenario plus one single outage
     "injection_n1_case2000_synth": ("case2000_synth", "injection_n1", 16384, 1, dict(broad=1.0, p_outage=0.9)),
+    # 8192 rows, 2048 on each of the 118/2000/6500/10000-bus grids, each a load-scaling scenario plus 0-2
+    # tripped non-islanding branches, all in one persistent launch
+    "heterogeneous_8192_case118_2000_6500_10000": ("case118_synth,case2000_synth,case6500_synth,case10000_synth",
+                                                    "multi", 2048, 3, dict(broad=1.0, p_outage=0.9)),
 }
 MAX_ITER, TOL = 10, 1e-8
 METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
@@ -87,9 +91,17 @@ def _dist():
 
 
 def _workload(name):
-    """(grid, trips or None, p_mw or None, q_mvar or None) of a named workload."""
-    from gpusim2grid_b200.synthetic import grid_by_name, injection_scenarios, n1_branches
+    """(grid, trips or None, p_mw or None, q_mvar or None) of a named workload;
+    for the heterogeneous workload, a list of such tuples (one per grid)."""
+    from gpusim2grid_b200.synthetic import grid_by_name, injection_scenarios, n1_branches, scenario_outages
     gname, kind, n_rows, seed, _ = WORKLOADS[name]
+    if kind == "multi":
+        parts = []
+        for i, gn in enumerate(gname.split(",")):
+            g = grid_by_name(gn, 0)
+            p, q = injection_scenarios(g, n_rows, seed=seed + 10 * i)
+            parts.append((g, scenario_outages(g, n_rows, max_trips=2, seed=seed + 10 * i + 1), p, q))
+        return parts
     g = grid_by_name(gname, 0)
     cand = n1_branches(g)
     if kind == "n1":
@@ -463,21 +475,191 @@ def _ids(rows):
     return ptr, np.fromiter((b for r in rows for b in r), dtype=np.int32, count=int(ptr[-1]))
 
 
+def cpu_baseline_multi(parts, n_rows_sample):
+    """The oracle port over an equal share of the sample from every grid; the
+    workload holds equal row counts per grid, so its rate is the harmonic
+    mean of the per-grid rates."""
+    share = max(1, n_rows_sample // len(parts))
+    secs, cores, samples = 0.0, None, []
+    for g, trips, p, q in parts:
+        v, cores, sample = cpu_baseline(g, trips, p, q, share)
+        secs += 1.0 / max(v, 1e-12)
+        samples.append(f"{g.name}: {sample}")
+    return len(parts) / secs, cores, "; ".join(samples)
+
+
+def run_ours_multi(args):
+    """The heterogeneous workload: rows of four grids in one persistent launch."""
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    from gpusim2grid_b200 import RowStatus, compute_many
+    from gpusim2grid_b200._native import lib
+
+    parts = _workload(args.workload)
+    learned = args.start == "learned"
+    prec = lib.PREC_MIXED if args.precision == "mixed" else lib.PREC_FP64
+    facades = [_facade(g, trips, p, q, args, local) for g, trips, p, q in parts]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    csrs = [_ids(trips) for _, trips, _, _ in parts]
+    sbus = [torch.as_tensor((p + 1j * q) / g.sn_mva, device="cuda") for g, _, p, q in parts]
+    n_rows = [p.shape[0] for _, _, p, _ in parts]
+    train = []
+    learners = []
+    if learned:
+        for (g, _, _, _), f in zip(parts, facades):
+            t0 = time.perf_counter()
+            ls, rep, mix = _train_learned(g, args, local)
+            learners.append(ls)
+            train.append({"grid": g.name, "rows": rep["n_rows"], "unconverged_dropped": rep["n_unconverged"],
+                          "t_total_s": round(time.perf_counter() - t0, 2),
+                          "val_mse": round(rep["val"][-1], 5) if rep["val"] else None})
+            f.set_learned_start(ls)
+    for f in facades:
+        f.start = "learned" if learned else "flat"
+        if args.tune_rates:
+            f.autotune(tuple(args.tune_rates), repeats=1)
+    ratio, reuse = facades[0]._learned_opts if learned else (0.0, 0)
+    strat = lib.REFACTOR_ADAPTIVE if args.strategy == "adaptive" else lib.REFACTOR_EVERY
+    sessions = [f.session for f in facades]
+    start_mode = lib.START_ROWS if learned else lib.START_VINIT
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    def step():
+        pre_ms = 0.0
+        if learned:
+            bufs = [s.start_rows_buffer(n) for s, n in zip(sessions, n_rows)]
+            ev0.record()
+            for ls, sb, c, n, b in zip(learners, sbus, csrs, n_rows, bufs):
+                ls.start_voltages(sb, c, n, out_ptr=b)
+            ev1.record()
+            ev1.synchronize()
+            pre_ms = ev0.elapsed_time(ev1)
+        lib.run_multi(sessions, MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, False, strat, ratio, reuse, learned)
+        return pre_ms, sessions[0].timings()["kernel_ms"]
+
+    for _ in range(args.warmup):
+        step()
+    clk = ClockSampler(local)
+    clk.start()
+    torch.cuda.synchronize()
+    pre, ker = [], []
+    torch.cuda.nvtx.range_push("bench_timed")
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a_, b_ = step()
+        pre.append(a_)
+        ker.append(b_)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    total_ms = float(np.sum(pre) + np.sum(ker))
+    res = [s.results() for s in sessions]
+    n_conv = sum(int((r[2] == RowStatus.CONVERGED).sum()) for r in res)
+    iters = np.concatenate([r[3] for r in res])
+    n_total = int(sum(n_rows))
+    value = world * n_conv * args.steps / (total_ms / 1e3)
+
+    def flat_arm(p_, strat_):
+        lib.run_multi(sessions, MAX_ITER, TOL, False, p_, lib.START_VINIT, 0.0, 0, False, strat_)
+        ms_ = []
+        for _ in range(max(1, min(args.steps, 3))):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            lib.run_multi(sessions, MAX_ITER, TOL, False, p_, lib.START_VINIT, 0.0, 0, False, strat_)
+            ms_.append(sessions[0].timings()["kernel_ms"])
+        r_ = [s.results() for s in sessions]
+        return sum(int((x[2] == 0).sum()) for x in r_) / (np.mean(ms_) / 1e3), r_
+
+    fp64_value, res64 = flat_arm(lib.PREC_FP64, lib.REFACTOR_EVERY)
+    agree, same = 0.0, True
+    for r, r64 in zip(res, res64):
+        ok = (r[2] == 0) & (r64[2] == 0)
+        if ok.any():
+            agree = max(agree, float(np.abs(r[0][ok] - r64[0][ok]).max()))
+        same = same and bool(np.array_equal(r[2] == 0, r64[2] == 0))
+    mixed_flat_value = flat_arm(lib.PREC_MIXED, lib.REFACTOR_ADAPTIVE)[0] if learned else None
+
+    # end to end: host rows in, every grid's voltages / statuses / residuals out
+    e2e_s = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f, (g, trips, p, q) in zip(facades, parts):
+            _set_rows(f, trips, p, q, g)
+        compute_many(facades)
+        outs = [(f.V_results, f.get_row_status(), f.last_residuals()) for f in facades]
+        e2e_s.append(time.perf_counter() - t0)
+    n_conv_e2e = sum(int((o[1] == 0).sum()) for o in outs)
+    e2e_value = world * n_conv_e2e / float(np.mean(e2e_s))
+    h2d = sum(2 * p.nbytes + 4 * (len(t) + 1) + 4 * sum(len(x) for x in t) for _, t, p, _ in parts)
+    if learned:
+        h2d += sum(p.shape[0] * g.n_bus * 16 + 16 * sum(len(x) for x in t) for g, t, p, _ in parts)
+    d2h = sum(o[0].nbytes + o[1].nbytes + o[2].nbytes for o in outs)
+
+    per_step_launches = 1 + (sum(ls.launches_per_call(n) for ls, n in zip(learners, n_rows)) if learned else 0)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 mismatch/V, f32 J/LU, bf16 MLP" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": args.workload, "grids": [g.name for g, _, _, _ in parts], "rows": n_total,
+                   "rows_per_grid": n_rows, "start": args.start, "precision": args.precision,
+                   "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER, "launch": "one persistent launch",
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "rows_converged": n_conv, "mean_iters": round(float(iters.mean()), 3),
+        "iters_hist": {int(k): int(v) for k, v in zip(*np.unique(iters, return_counts=True))},
+        "ms_split": {"features_mlp_v0": round(float(np.mean(pre)), 4), "sweep_kernel": round(float(np.mean(ker)), 4)},
+        "fp64_flat_value": round(fp64_value, 1),
+        "speedup_vs_fp64_flat": round(value / world / fp64_value, 3),
+        "mixed_flat_value": None if mixed_flat_value is None else round(mixed_flat_value, 1),
+        "agreement_with_fp64": {"max_abs_dv_pu": agree, "same_convergence_flags": same},
+        "training": train,
+        "plan_tails": [s.info()["tail_dim"] for s in sessions],
+        "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps * per_step_launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_baseline_multi(parts, args.cpu_sample_rows)
+        line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
+                                "sample": sample}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
     rank, world, _ = _dist()
     if rank != 0:
         return
-    g, trips, p, q = _workload(args.workload)
+    w = _workload(args.workload)
+    multi = isinstance(w, list)
+    base = (lambda k: cpu_baseline_multi(w, k)) if multi else (lambda k: cpu_baseline(*w, k))
     vals = []
     for _ in range(args.warmup):
-        cpu_baseline(g, trips, p, q, 8)
+        base(8)
     cores = sample = None
     for _ in range(args.steps):
-        v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_sample_rows)
+        v, cores, sample = base(args.cpu_sample_rows)
         vals.append(v)
     value = float(np.mean(vals))
-    n = len(trips) if trips is not None else p.shape[0]
+    if multi:
+        n = sum(p.shape[0] for _, _, p, _ in w)
+    else:
+        g, trips, p, q = w
+        n = len(trips) if trips is not None else p.shape[0]
     print(json.dumps({
         "impl": "reference",
         "metric": METRIC,
@@ -498,5 +680,7 @@ if __name__ == "__main__":
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif WORKLOADS[a.workload][1] == "multi":
+        run_ours_multi(a)
     else:
         run_ours(a)
