@@ -544,8 +544,10 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // for at most max_reuse steps (an inexact Newton / chord step: the FP64
       // mismatch still drives the iterate to the same fixed point).  nrm is
       // block-uniform, so the branch is taken by the whole CTA.
-      const bool refactor = !have_factor || a.refactor_policy == 0 || !(nrm <= a.refactor_ratio * last_nrm) ||
-                            since_factor >= a.max_reuse;
+      // (the rescue attempt restarts from Vinit, far from the solution: full
+      // Newton there)
+      const bool refactor = !have_factor || a.refactor_policy == 0 || attempt > 0 ||
+                            !(nrm <= a.refactor_ratio * last_nrm) || since_factor >= a.max_reuse;
       last_nrm = nrm;
       if (refactor) {
         have_factor = true;

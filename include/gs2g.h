@@ -88,9 +88,10 @@ typedef struct gs2g_run_opts {
   int max_reuse;         /* adaptive: <= 0 selects 3 */
   /* 1: with GS2G_START_ROWS and the continuous schedule, a row that ends
    * unconverged (MAX_ITER or DIVERGED) from its given start restarts once
-   * from Vinit inside the same launch, with a fresh max_iter budget; its
-   * iteration and factorization counts include both attempts.  Guards a
-   * learned or otherwise predicted start against a bad prediction. */
+   * from Vinit inside the same launch, with a fresh max_iter budget and a
+   * new LU every step; its iteration and factorization counts include both
+   * attempts.  Guards a learned or otherwise predicted start against a bad
+   * prediction. */
   int rescue;
 } gs2g_run_opts;
 
