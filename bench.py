@@ -390,17 +390,23 @@ def run_ours(args):
 
     # end to end through the facade, host buffers in and out
     ca.start = "learned" if learned else "flat"
-    e2e_s = []
+    e2e_s, e2e_parts = [], []
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _set_rows(ca, trips, p, q, g)
+        t1 = time.perf_counter()
         ca.compute()
+        t2 = time.perf_counter()
         V = ca.V_results
         stt = ca.get_row_status()
         r = ca.last_residuals()
-        e2e_s.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        e2e_s.append(t3 - t0)
+        e2e_parts.append((t1 - t0, t2 - t1, t3 - t2, ca.timings.t_kernel_ms / 1e3))
     e2e_value = world * int((stt == 0).sum()) / float(np.mean(e2e_s))
+    e2e_split = dict(zip(["rows_in_ms", "compute_ms", "results_out_ms", "kernel_ms"],
+                         [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
     n_ids = sum(len(r_) for r_ in trips) if trips is not None else 0
     h2d = (4 * (n + 1) + 4 * n_ids if trips is not None else 0) + (2 * p.nbytes if p is not None else 0)
     if learned:
@@ -454,7 +460,7 @@ def run_ours(args):
                          "frac": round(achieved_tflops / fma_peak, 4),
                          "note": "FP64 (or FP32) FMA pipe; peak measured by a DFMA/FFMA loop on this pool"},
         "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "split": e2e_split},
         "gpu_launches": args.steps * per_step_launches,
         "clocks": clocks,
     }
