@@ -37,6 +37,23 @@ _START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROW
 _STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE}
 
 
+def _rows_csr(branch_ids_per_row):
+    """(rows, ptr, ids) of branch-id lists, each row's duplicates dropped
+    (first occurrence kept).  Rows of one id each (the N-1 case), given as
+    lists or as an integer array, take a vectorised path."""
+    if isinstance(branch_ids_per_row, np.ndarray) and branch_ids_per_row.ndim == 2 and \
+            branch_ids_per_row.shape[1] == 1:
+        flat = np.ascontiguousarray(branch_ids_per_row[:, 0], dtype=np.int32)
+    elif len(branch_ids_per_row) and all(len(r) == 1 for r in branch_ids_per_row):
+        flat = np.fromiter((int(r[0]) for r in branch_ids_per_row), dtype=np.int32, count=len(branch_ids_per_row))
+    else:
+        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_row]
+        ptr, ids = _ids_csr(rows)
+        return rows, ptr, ids
+    ptr = np.arange(flat.size + 1, dtype=np.int32)
+    return flat[:, None].tolist(), ptr, flat
+
+
 def _ids_csr(rows):
     ptr = np.zeros(len(rows) + 1, dtype=np.int32)
     flat = []
@@ -282,16 +299,16 @@ class ContingencyAnalysisGPU(_BatchSweep):
         is tripped once).  Replaces previously given contingencies."""
         if self._n_branches is None:
             raise RuntimeError("set_branch_data() must be called before add_contingencies_by_branch_id()")
-        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_ctg]
-        ptr, ids = _ids_csr(rows)
+        rows, ptr, ids = _rows_csr(branch_ids_per_ctg)
         self._s.set_contingencies(ptr, ids)
         self._ctg = rows
+        self._ctg_csr = (ptr, ids)
 
     def get_contingencies(self):
         return [list(r) for r in self._ctg]
 
     def _row_defs(self):
-        return None, self._ctg, len(self._ctg)
+        return None, self._ctg_csr, len(self._ctg)
 
     @property
     def n_contingencies(self):
@@ -339,16 +356,16 @@ class ScenarioSweepGPU(InjectionSweepGPU):
     def set_topology(self, branch_ids_per_scenario):
         if self._n_branches is None:
             raise RuntimeError("set_branch_data() must be called before set_topology()")
-        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_scenario]
-        ptr, ids = _ids_csr(rows)
+        rows, ptr, ids = _rows_csr(branch_ids_per_scenario)
         self._s.set_contingencies(ptr, ids)
         self._topo = rows
+        self._topo_csr = (ptr, ids)
 
     def _row_defs(self):
         if self._inj is None:
             raise RuntimeError("set_injections() must be called before compute()")
         p, q, sn = self._inj
-        return (p + 1j * q) / sn, self._topo, self._n_scen
+        return (p + 1j * q) / sn, (self._topo_csr if self._topo is not None else None), self._n_scen
 
     def get_disconnected(self):
         """(n_rows,) bool: rows whose topology islands the grid (never solved)."""

@@ -110,6 +110,9 @@ struct gs2g_session {
 
   gs2g_timings tm{};
   int last_rows_run = 0;
+  // pinned double buffer for large result copies (see d2h_staged)
+  mutable void* h_stage = nullptr;
+  mutable cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -571,6 +574,9 @@ int gs2g_session_destroy(gs2g_session* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    for (cudaEvent_t e : s->ev_stage)
+      if (e) cudaEventDestroy(e);
+    if (s->h_stage) cudaFreeHost(s->h_stage);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
   }
@@ -963,13 +969,44 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
 
 int gs2g_n_rows(const gs2g_session* s) { return s ? s->last_rows_run : 0; }
 
+namespace {
+// Large device-to-host copies into the caller's (pageable) memory go through
+// a pinned double buffer of the session: chunk i+1 is in flight while chunk
+// i is copied out on the host.
+void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes) {
+  constexpr size_t kChunk = size_t(8) << 20;
+  if (bytes < 2 * kChunk) {
+    ck(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "read results");
+    return;
+  }
+  if (!s->h_stage) {
+    ck(cudaMallocHost(&s->h_stage, 2 * kChunk), "pinned staging buffer");
+    for (cudaEvent_t& e : s->ev_stage) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  }
+  char* buf[2] = {static_cast<char*>(s->h_stage), static_cast<char*>(s->h_stage) + kChunk};
+  const size_t nch = (bytes + kChunk - 1) / kChunk;
+  auto issue = [&](size_t i) {
+    const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
+    ck(cudaMemcpyAsync(buf[i & 1], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, s->stream),
+       "read results");
+    ck(cudaEventRecord(s->ev_stage[i & 1], s->stream), "event");
+  };
+  issue(0);
+  for (size_t i = 0; i < nch; ++i) {
+    if (i + 1 < nch) issue(i + 1);  // into the buffer chunk i-1 left, already copied out
+    ck(cudaEventSynchronize(s->ev_stage[i & 1]), "read results");
+    const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
+    std::memcpy(static_cast<char*>(dst) + off, buf[i & 1], len);
+  }
+}
+}  // namespace
+
 int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters) {
   GS2G_TRY
   if (!s) throw std::invalid_argument("NULL session");
   DeviceGuard g(s->device);
   const size_t nr = s->last_rows_run, n = s->n_bus;
-  if (v_out && nr)
-    ck(cudaMemcpy(v_out, s->d_v_out.p, nr * n * 2 * sizeof(double), cudaMemcpyDeviceToHost), "read V");
+  if (v_out && nr) d2h_staged(s, v_out, s->d_v_out.p, nr * n * 2 * sizeof(double));
   if (residuals && nr) ck(cudaMemcpy(residuals, s->d_res.p, nr * sizeof(double), cudaMemcpyDeviceToHost), "read res");
   if (status && nr) ck(cudaMemcpy(status, s->d_status.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read status");
   if (iters && nr) ck(cudaMemcpy(iters, s->d_iters.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read iters");
