@@ -84,10 +84,9 @@ def _args():
 
 
 def _dist():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from gpusim2grid_b200.replicas import rank_info
+    info = rank_info()
+    return info.rank, info.world, info.local
 
 
 def _workload(name):
@@ -262,11 +261,10 @@ def _set_rows(f, trips, p, q, g):
 
 def run_ours(args):
     import torch
+    from gpusim2grid_b200 import replicas
     rank, world, local = _dist()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    replicas.init("nccl", timeout_s=600)
     from gpusim2grid_b200 import RowStatus
     from gpusim2grid_b200._native import lib
 
@@ -325,9 +323,7 @@ def run_ours(args):
         return pre_ms, s.timings()["kernel_ms"]
 
     def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
 
     for _ in range(args.warmup):
         step()
@@ -345,11 +341,7 @@ def run_ours(args):
     torch.cuda.nvtx.range_pop()
     barrier()
     clocks = clk.stop()
-    total_ms = float(np.sum(pre) + np.sum(ker))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(float(np.sum(pre) + np.sum(ker)), device="cuda")
     V_w, res, st, it = s.results()
     n_conv = int((st == RowStatus.CONVERGED).sum())
     total_iters = int(it.sum())
@@ -468,9 +460,7 @@ def run_ours(args):
         v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_sample_rows)
         line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
                                 "sample": sample}
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    replicas.finish()
     if rank == 0:
         print(json.dumps(line))
 
@@ -497,11 +487,10 @@ def cpu_baseline_multi(parts, n_rows_sample):
 def run_ours_multi(args):
     """The heterogeneous workload: rows of four grids in one persistent launch."""
     import torch
+    from gpusim2grid_b200 import replicas
     rank, world, local = _dist()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    replicas.init("nccl", timeout_s=900)
     from gpusim2grid_b200 import RowStatus, compute_many
     from gpusim2grid_b200._native import lib
 
@@ -554,7 +543,7 @@ def run_ours_multi(args):
         step()
     clk = ClockSampler(local)
     clk.start()
-    torch.cuda.synchronize()
+    replicas.barrier()
     pre, ker = [], []
     torch.cuda.nvtx.range_push("bench_timed")
     for _ in range(args.steps):
@@ -564,9 +553,9 @@ def run_ours_multi(args):
         pre.append(a_)
         ker.append(b_)
     torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
+    replicas.barrier()
     clocks = clk.stop()
-    total_ms = float(np.sum(pre) + np.sum(ker))
+    total_ms = replicas.max_over_ranks(float(np.sum(pre) + np.sum(ker)), device="cuda")
     res = [s.results() for s in sessions]
     n_conv = sum(int((r[2] == RowStatus.CONVERGED).sum()) for r in res)
     iters = np.concatenate([r[3] for r in res])
@@ -643,9 +632,7 @@ def run_ours_multi(args):
         v, cores, sample = cpu_baseline_multi(parts, args.cpu_sample_rows)
         line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
                                 "sample": sample}
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    replicas.finish()
     if rank == 0:
         print(json.dumps(line))
 
