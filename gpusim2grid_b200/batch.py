@@ -186,6 +186,38 @@ class _BatchSweep:
                                 np.ascontiguousarray(branch_to, dtype=np.int32),
                                 c(yff_eff), c(yft_eff), c(ytf_eff), c(ytt_eff))
         self._n_branches = len(branch_from)
+        self._limits = False
+
+    def set_branch_limits(self, rate_mva, sn_mva=100.0):
+        """Branch limits in MVA (one per branch of ``set_branch_data``; <= 0:
+        unlimited).  From then on every ``compute()`` also evaluates each
+        converged row's branch flows and loadings on the GPU as the row
+        finishes (the reference's ``compute_branch_flows`` +
+        ``check_limit_violations``); read them with ``branch_loading()``.
+        ``None`` turns it off."""
+        if self._n_branches is None:
+            raise RuntimeError("set_branch_data() must be called before set_branch_limits()")
+        if rate_mva is None:
+            self._s.set_branch_limits(np.zeros(0), float(sn_mva))
+            self._limits = False
+            return
+        rate = np.ascontiguousarray(rate_mva, dtype=np.float64)
+        if rate.shape != (self._n_branches,):
+            raise ValueError(f"rate_mva must have one entry per branch ({self._n_branches})")
+        self._s.set_branch_limits(rate, float(sn_mva))
+        self._limits = True
+
+    def branch_loading(self):
+        """(loading, n_violations, max_loading) of the last ``compute()``:
+        loading (n_rows, n_branches) float32 = max(|S_from|, |S_to|) / limit
+        (0 for tripped or unlimited branches, NaN for rows that did not
+        converge); n_violations (n_rows,) branches above their limit (-1: row
+        not converged); max_loading (n_rows,)."""
+        if not self._ran:
+            raise RuntimeError("Call compute() first.")
+        if not getattr(self, "_limits", False):
+            raise RuntimeError("set_branch_limits() was not called")
+        return self._s.branch_loading(int(self._n_branches))
 
     def set_start_voltages(self, V0):
         """Per-row start voltages (n_rows, n_bus) complex; switches ``start`` to 'rows'."""

@@ -75,6 +75,18 @@ __device__ double block_nanmax(double v, double* s_red) {
   return r;
 }
 
+// Sum over the block (every thread gets it); s_red holds NWARP doubles.
+__device__ double block_sum(double v, double* s_red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  for (int w = 0; w < NWARP; ++w) r += s_red[w];
+  __syncthreads();
+  return r;
+}
+
 template <typename T>
 __device__ __forceinline__ T clamp_pivot(T piv, double floor_) {
   const T f = (T)floor_;
@@ -458,6 +470,13 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
 
     if (a.row_skip != nullptr && a.row_skip[row]) {
       for (int i = tid; i < n; i += BS) vout[i] = make_double2(NAN, NAN);
+      if (a.loading_out != nullptr) {
+        for (int l = tid; l < a.n_branch; l += BS) a.loading_out[(int64_t)row * a.n_branch + l] = NAN;
+        if (tid == 0) {
+          a.nviol_out[row] = -1;
+          a.maxload_out[row] = NAN;
+        }
+      }
       if (tid == 0) {
         a.res_out[row] = NAN;
         a.status_out[row] = ROW_NOT_SIMULATED;
@@ -703,6 +722,42 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     if (tid == 0 && a.n_rescued != nullptr) atomicAdd(a.n_rescued, 1);
     __syncthreads();
     }  // attempts
+
+    // ---- branch flows and limit check as the row leaves --------------------
+    // (the reference's compute_branch_flows + check_limit_violations passes,
+    // done by the row's own CTA on the V it still holds)
+    if (a.loading_out != nullptr) {
+      const bool ok = status == ROW_CONVERGED;
+      const int q0 = a.trip_ptr != nullptr ? a.trip_ptr[row] : 0;
+      const int q1 = a.trip_ptr != nullptr ? a.trip_ptr[row + 1] : 0;
+      double lmax = 0.0;
+      int nv = 0;
+      for (int l = tid; l < a.n_branch; l += BS) {
+        float ld = NAN;
+        if (ok) {
+          bool tripped = false;
+          for (int q = q0; q < q1; ++q) tripped |= a.trip_ids[q] == l;
+          ld = 0.f;
+          if (!tripped && a.br_rate[l] > 0.0) {
+            const double2* yb = reinterpret_cast<const double2*>(a.br_y) + 4 * (int64_t)l;
+            const double2 Vf = V[a.br_from[l]], Vt = V[a.br_to[l]];
+            const double2 Sf = cmul(Vf, conj2(cadd(cmul(yb[0], Vf), cmul(yb[1], Vt))));
+            const double2 St = cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt))));
+            const double r = fmax(hypot(Sf.x, Sf.y), hypot(St.x, St.y)) / a.br_rate[l];
+            ld = (float)r;
+            lmax = fmax(lmax, r);
+            nv += r > 1.0;
+          }
+        }
+        a.loading_out[(int64_t)row * a.n_branch + l] = ld;
+      }
+      lmax = block_nanmax(lmax, s_red);
+      const double nv_all = block_sum(double(nv), s_red);
+      if (tid == 0) {
+        a.nviol_out[row] = ok ? (int)nv_all : -1;
+        a.maxload_out[row] = ok ? (float)lmax : NAN;
+      }
+    }
 
     for (int i = tid; i < n; i += BS) vout[i] = V[i];
     if (tid == 0) {

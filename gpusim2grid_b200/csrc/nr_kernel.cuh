@@ -73,6 +73,17 @@ struct SweepArgs {
   // the restarts (nullptr: not counted)
   const double* rescue_v0;
   int* n_rescued;
+  // branch flows and limit check when the row leaves (loading_out nullptr: off)
+  int n_branch;
+  const int* br_from;
+  const int* br_to;
+  const double* br_y;     // [n_branch * 4] complex: yff, yft, ytf, ytt
+  const double* br_rate;  // [n_branch] limits, per unit (<= 0: no limit)
+  const int* trip_ptr;    // [n_rows + 1] tripped branch ids per row (nullptr: none)
+  const int* trip_ids;
+  float* loading_out;     // [n_rows * n_branch] max(|S_from|, |S_to|) / rate (0: tripped or no limit)
+  int* nviol_out;         // [n_rows] branches above their limit (-1: row not converged)
+  float* maxload_out;     // [n_rows]
   // outputs
   double* v_out;          // [n_rows * n_bus] complex
   double* res_out;        // [n_rows]

@@ -260,6 +260,27 @@ class Session {
 
   int n_rows() const { return gs2g_n_rows(h()); }
 
+  void set_branch_limits(DArr rate_mva, double sn_mva) {
+    check(gs2g_set_branch_limits(h(), (int)rate_mva.size(), rate_mva.data(), sn_mva));
+  }
+
+  py::tuple branch_loading(int n_branch) const {
+    const int nr = gs2g_n_rows(h());
+    py::array_t<float> ld({nr, n_branch});
+    py::array_t<int> nv(nr);
+    py::array_t<float> mx(nr);
+    int rc;
+    {
+      float* lp = ld.mutable_data();
+      int* np_ = nv.mutable_data();
+      float* mp = mx.mutable_data();
+      py::gil_scoped_release nogil;
+      rc = gs2g_get_branch_loading(h(), lp, np_, mp);
+    }
+    check(rc);
+    return py::make_tuple(ld, nv, mx);
+  }
+
   py::tuple results() const {
     const int nr = gs2g_n_rows(h());
     py::array_t<cplx> V({nr, n_bus_});
@@ -488,6 +509,8 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("set_start_rows", &Session::set_start_rows)
       .def("set_start_rows_device", &Session::set_start_rows_device)
       .def("start_rows_buffer", &Session::start_rows_buffer)
+      .def("set_branch_limits", &Session::set_branch_limits)
+      .def("branch_loading", &Session::branch_loading)
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)

@@ -88,6 +88,11 @@ struct gs2g_session {
   std::vector<int> k_ff, k_tt, k_ft, k_tf;  // Ybus entry of each branch term
   std::vector<uint8_t> is_bridge;           // branch whose loss alone islands the grid
   int base_components = 1;                  // connected components of the branch graph
+  DevBuf d_br_from, d_br_to, d_br_y;        // branch data on the device (flows)
+  DevBuf d_br_rate;                         // limits in per unit
+  bool limits_on = false;
+  DevBuf d_trip_ptr, d_trip_ids;            // tripped branches per assembled row
+  DevBuf d_loading, d_nviol, d_maxload;     // flow outputs of the last run
 
   // row definitions
   int n_ctg = 0;
@@ -277,6 +282,12 @@ void assemble_rows(gs2g_session* s) {
        "upload sbus rows");
   }
   if (s->rows_have_edits) {
+    s->d_trip_ptr.ensure((nr + 1) * sizeof(int));
+    s->d_trip_ids.ensure(std::max<size_t>(s->ctg_ids.size(), 1) * sizeof(int));
+    ck(cudaMemcpy(s->d_trip_ptr.p, s->ctg_ptr.data(), (nr + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload trips");
+    if (!s->ctg_ids.empty())
+      ck(cudaMemcpy(s->d_trip_ids.p, s->ctg_ids.data(), s->ctg_ids.size() * sizeof(int), cudaMemcpyHostToDevice),
+         "upload trips");
     std::vector<int> eptr(nr + 1, 0), ek;
     std::vector<double> ev;
     std::vector<uint8_t> skip(nr, 0);
@@ -384,6 +395,22 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   const bool rescue = o.rescue != 0 && v0_stride != 0 && !o.fixed_iters;
   a.rescue_v0 = rescue ? s->d_vinit.as<double>() : nullptr;
   a.phase_cycles = nullptr;
+  if (use_rows && s->limits_on) {
+    const size_t nr = (size_t)std::max(n_rows, 1);
+    s->d_loading.ensure(nr * s->n_branch * sizeof(float));
+    s->d_nviol.ensure(nr * sizeof(int));
+    s->d_maxload.ensure(nr * sizeof(float));
+    a.n_branch = s->n_branch;
+    a.br_from = s->d_br_from.as<int>();
+    a.br_to = s->d_br_to.as<int>();
+    a.br_y = s->d_br_y.as<double>();
+    a.br_rate = s->d_br_rate.as<double>();
+    a.trip_ptr = s->rows_have_edits ? s->d_trip_ptr.as<int>() : nullptr;
+    a.trip_ids = s->rows_have_edits ? s->d_trip_ids.as<int>() : nullptr;
+    a.loading_out = s->d_loading.as<float>();
+    a.nviol_out = s->d_nviol.as<int>();
+    a.maxload_out = s->d_maxload.as<float>();
+  }
   return a;
 }
 
@@ -672,6 +699,26 @@ int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const i
   s->k_ft.swap(kft);
   s->k_tf.swap(ktf);
   compute_bridges(s);
+  {
+    DeviceGuard g(s->device);
+    std::vector<double> y(8 * (size_t)n_branch);
+    for (int l = 0; l < n_branch; ++l) {
+      const double* src[4] = {yff, yft, ytf, ytt};
+      for (int q = 0; q < 4; ++q) {
+        y[8 * l + 2 * q] = src[q][2 * l];
+        y[8 * l + 2 * q + 1] = src[q][2 * l + 1];
+      }
+    }
+    s->d_br_from.ensure(std::max(n_branch, 1) * sizeof(int));
+    s->d_br_to.ensure(std::max(n_branch, 1) * sizeof(int));
+    s->d_br_y.ensure(std::max<size_t>(y.size(), 1) * sizeof(double));
+    if (n_branch) {
+      ck(cudaMemcpy(s->d_br_from.p, from, n_branch * sizeof(int), cudaMemcpyHostToDevice), "upload branches");
+      ck(cudaMemcpy(s->d_br_to.p, to, n_branch * sizeof(int), cudaMemcpyHostToDevice), "upload branches");
+      ck(cudaMemcpy(s->d_br_y.p, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice), "upload branches");
+    }
+  }
+  s->limits_on = false;  // limits belong to the branch set they were given for
   s->rows_dirty = true;
   GS2G_CATCH
 }
@@ -1020,6 +1067,38 @@ int gs2g_get_factor_counts(const gs2g_session* s, int* factors) {
   if (s->last_rows_run)
     ck(cudaMemcpy(factors, s->d_factors.p, (size_t)s->last_rows_run * sizeof(int), cudaMemcpyDeviceToHost),
        "read factor counts");
+  GS2G_CATCH
+}
+
+int gs2g_set_branch_limits(gs2g_session* s, int n_branch, const double* rate_mva, double sn_mva) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  if (n_branch == 0) {
+    s->limits_on = false;
+    return GS2G_OK;
+  }
+  if (n_branch != s->n_branch || !rate_mva || !(sn_mva > 0))
+    throw std::invalid_argument("set_branch_limits: needs one limit per branch of set_branch_data and sn_mva > 0");
+  DeviceGuard g(s->device);
+  std::vector<double> pu(n_branch);
+  for (int l = 0; l < n_branch; ++l) pu[l] = rate_mva[l] / sn_mva;
+  s->d_br_rate.ensure(n_branch * sizeof(double));
+  ck(cudaMemcpy(s->d_br_rate.p, pu.data(), n_branch * sizeof(double), cudaMemcpyHostToDevice), "upload limits");
+  s->limits_on = true;
+  GS2G_CATCH
+}
+
+int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violations, float* max_loading) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  if (!s->limits_on || !s->d_loading.p) throw std::runtime_error("get_branch_loading: no limits were set for the last run");
+  DeviceGuard g(s->device);
+  const size_t nr = s->last_rows_run;
+  if (loading && nr) d2h_staged(s, loading, s->d_loading.p, nr * s->n_branch * sizeof(float));
+  if (n_violations && nr)
+    ck(cudaMemcpy(n_violations, s->d_nviol.p, nr * sizeof(int), cudaMemcpyDeviceToHost), "read violations");
+  if (max_loading && nr)
+    ck(cudaMemcpy(max_loading, s->d_maxload.p, nr * sizeof(float), cudaMemcpyDeviceToHost), "read violations");
   GS2G_CATCH
 }
 

@@ -191,6 +191,18 @@ int gs2g_n_rows(const gs2g_session* s);
 int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters);
 /* LU factorizations each row of the last run performed. */
 int gs2g_get_factor_counts(const gs2g_session* s, int* factors);
+/* Branch flows and limit check as each row leaves the GPU (the reference's
+ * compute_branch_flows_kernel, src/_cpp/acpf_nr_kernels.cu:87-183, and
+ * check_limit_violations, src/_cpp/contingency/violation_kernels.cu:297,
+ * done by the row's own CTA on its final V).  rate_mva: one limit per branch
+ * of gs2g_set_branch_data (<= 0: unlimited); n_branch = 0 turns it off.
+ * Per row and branch: loading = max(|S_from|, |S_to|) / rate (0 for tripped
+ * or unlimited branches, NaN for rows that did not converge or were not
+ * simulated); per row: branches with loading > 1 (-1: not converged) and the
+ * largest loading.  Setting branch data again turns the limits off. */
+int gs2g_set_branch_limits(gs2g_session* s, int n_branch, const double* rate_mva, double sn_mva);
+/* loading [n_rows x n_branch], n_violations [n_rows], max_loading [n_rows]; any may be NULL. */
+int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violations, float* max_loading);
 /* Device pointers of the last run's results (valid until the next run or destroy). */
 int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
 int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);

@@ -195,3 +195,26 @@ def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="conve
         V, st, it, nrm = nr_solve(Y, V0, Sbus_rows[r], pv, pq, max_iter, tol, mode)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
+
+
+def branch_flows(V, f, t, yff, yft, ytf, ytt):
+    """Complex power entering every branch at its from and to ends, the
+    reference's formulas (``src/_cpp/acpf_nr_kernels.cu:87-183``):
+    S_from = V_f conj(yff V_f + yft V_t), S_to = V_t conj(ytf V_f + ytt V_t)."""
+    V = np.asarray(V)
+    f = np.asarray(f)
+    t = np.asarray(t)
+    return V[f] * np.conj(yff * V[f] + yft * V[t]), V[t] * np.conj(ytf * V[f] + ytt * V[t])
+
+
+def branch_loading(V, f, t, yff, yft, ytf, ytt, rate_pu, tripped=()):
+    """Per-branch loading max(|S_from|, |S_to|) / rate (0 for tripped or
+    unlimited branches), the reference's limit check
+    (``contingency/violation_kernels.cu:297``)."""
+    Sf, St = branch_flows(V, f, t, yff, yft, ytf, ytt)
+    smax = np.maximum(np.abs(Sf), np.abs(St))
+    rate = np.asarray(rate_pu, dtype=np.float64)
+    out = np.where(rate > 0, smax / np.where(rate > 0, rate, 1.0), 0.0)
+    if len(tripped):
+        out[list(tripped)] = 0.0
+    return out

@@ -91,3 +91,24 @@ def test_fixed_mode_runs_exact_steps(g118):
     Vb, _, _, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
     V, st, it, res = O.nr_solve(Y, Vb, S, pv, pq, 4, 1e-8, mode="fixed")
     assert it == 4 and st == O.CONVERGED and res < 1e-8
+
+
+def test_branch_flows_balance_every_bus(g118):
+    """At a converged solution the flows leaving every bus through its
+    branches add up to the bus injection V conj(Y V) (the branches' pi models
+    are the whole Ybus of the synthetic grids)."""
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    V, st, _, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-10)
+    assert st == O.CONVERGED
+    Sf, St = O.branch_flows(V, g118.branch_from, g118.branch_to, g118.yff, g118.yft, g118.ytf, g118.ytt)
+    out = np.zeros(g118.n_bus, dtype=np.complex128)
+    np.add.at(out, g118.branch_from, Sf)
+    np.add.at(out, g118.branch_to, St)
+    np.testing.assert_allclose(out, V * np.conj(Y @ V), atol=1e-10)
+    # loading: unlimited and tripped branches load 0
+    rate = np.abs(Sf) * 2
+    rate[:3] = 0
+    ld = O.branch_loading(V, g118.branch_from, g118.branch_to, g118.yff, g118.yft, g118.ytf, g118.ytt, rate,
+                          tripped=[5])
+    assert np.all(ld[:3] == 0) and ld[5] == 0
+    np.testing.assert_allclose(ld[6:], np.maximum(np.abs(Sf), np.abs(St))[6:] / rate[6:])
