@@ -58,6 +58,10 @@ WORKLOADS = {
 }
 MAX_ITER, TOL = 10, 1e-8
 METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
+# DRAM bytes (read + write) of one sweep-kernel launch, from the ncu capture
+# summarised in profiles/sweep_kernel_full_n1_case2000_learned.md (same
+# workload, 3203 LUs and 14023 Newton steps in that launch)
+NCU_TRAFFIC = {"n1_sweep_case2000_synth": (69.64e9, 3203, 14023)}
 
 
 def _args():
@@ -445,7 +449,12 @@ def run_ours(args):
                  "autotune_ms": {str(k): v[1] for k, v in tune.items()}},
         "phase_share": phases,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved_gbs / peak, 4), "traffic": None,
+                     "frac": round(achieved_gbs / peak, 4),
+                     "traffic": None if args.workload not in NCU_TRAFFIC else {
+                         "dram_bytes_per_launch": NCU_TRAFFIC[args.workload][0],
+                         "algorithmic_bytes_same_launch": b_fact * NCU_TRAFFIC[args.workload][1]
+                         + b_iter * NCU_TRAFFIC[args.workload][2],
+                         "source": "ncu capture, profiles/sweep_kernel_full_n1_case2000_learned.md"},
                      "note": f"sweep kernel; peak {peak_kind}; algorithmic bytes per launch = {b_fact} per LU x "
                              f"{total_factors} LUs + {b_iter} per Newton step x {total_iters} steps"},
         "fma_roofline": {"achieved": round(achieved_tflops, 3), "peak": fma_peak, "unit": "TFLOP/s",
