@@ -94,6 +94,10 @@ class _BatchSweep:
         self.strategy = strategy
         self.refactor_ratio = 0.3
         self.max_reuse = 3
+        # mixed precision, continuous schedule: rows that end MAX_ITER or
+        # DIVERGED are re-solved in plain FP64 from Vinit, whose verdict stands
+        self.fallback = "fp64"
+        self._fallback_rows = 0
         self._learned = None
         self._warm = {}
         self._n_branches = None
@@ -247,11 +251,38 @@ class _BatchSweep:
         tm = self._s.timings()
         if self._start == "learned":
             self._warm["n_rescued"] = int(tm["n_rescued"])
+        kernel_ms = tm["kernel_ms"]
+        kernel_ms += self._fp64_fallback(n_ctas)
+        tm = dict(tm, kernel_ms=kernel_ms)
         self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
                                      t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
                                      t_kernel_ms=tm["kernel_ms"], t_total_ms=(time.perf_counter() - t0) * 1e3)
         self._ran = True
         self._host = None
+
+    def _fp64_fallback(self, n_ctas=0):
+        """Re-solve, in plain FP64 from Vinit, the rows a mixed-precision
+        continuous run left MAX_ITER or DIVERGED (the north star's "flat-start
+        FP64 NR remains the fallback").  Returns its kernel ms."""
+        self._fallback_rows = 0
+        if self.fallback != "fp64" or self._prec != lib.PREC_MIXED or self.scheduling != "continuous":
+            return 0.0
+        import torch
+        st = torch.from_dlpack(self._s.dlpack("status"))
+        bad = ((st == int(RowStatus.MAX_ITER)) | (st == int(RowStatus.DIVERGED))).nonzero().flatten()
+        if bad.numel() == 0:
+            return 0.0
+        rows = bad.to(torch.int32).cpu().numpy()
+        self._s.run_subset(rows, self.nb_iter, self.tol, False, lib.PREC_FP64, lib.START_VINIT, 0.0, n_ctas,
+                           lib.REFACTOR_EVERY)
+        self._fallback_rows = int(rows.size)
+        self._host = None
+        return float(self._s.timings()["kernel_ms"])
+
+    @property
+    def fallback_rows(self):
+        """Rows the last ``compute()`` re-solved in FP64 (see ``fallback``)."""
+        return self._fallback_rows
 
     def compute(self, batch_size=512):
         """Solve every row.  Returns a DLPack capsule (n_rows, n_bus) complex128
@@ -439,13 +470,15 @@ def compute_many(sweeps, batch_size=0):
     lib.run_multi([f._s for f in sweeps], f0.nb_iter, f0.tol, f0.scheduling == "chunked", f0._prec, _START[start],
                   0.0, max(int(batch_size), 0), False, _STRATEGY[f0._strategy], ratio, reuse,
                   start in ("rows", "learned"))
+    kernel_ms = sweeps[0]._s.timings()["kernel_ms"]
+    for f in sweeps:
+        f._ran = True
+        kernel_ms += f._fp64_fallback()
     total_ms = (time.perf_counter() - t0) * 1e3
-    kernel_ms = 0.0
     for f in sweeps:
         tm = f._s.timings()
-        kernel_ms = tm["kernel_ms"]
         f._timings = BatchTimings(n_rows=f._s.n_rows(), total_iters=int(tm["total_iters"]), t_plan_ms=tm["plan_ms"],
-                                  t_upload_ms=tm["upload_ms"], t_kernel_ms=tm["kernel_ms"], t_total_ms=total_ms)
+                                  t_upload_ms=tm["upload_ms"], t_kernel_ms=kernel_ms, t_total_ms=total_ms)
         f._ran = True
         f._host = None
     return kernel_ms

@@ -788,12 +788,12 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   for (;;) {
     if (threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
     __syncthreads();
-    const int row = s_row;
-    if (row >= a.n_rows) {
+    const int q = s_row;
+    if (q >= a.n_rows) {
       prof.flush(a.phase_cycles);
       return;
     }
-    solve_row<T>(P, a, row, ws, sh, prof);
+    solve_row<T>(P, a, a.row_map != nullptr ? a.row_map[q] : q, ws, sh, prof);
   }
 }
 
@@ -836,7 +836,8 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
       __syncthreads();
       cur = g;
     }
-    solve_row<T>(s_grid.P, s_grid.a, row - row_begin[g], ws, sh, prof);
+    const int lr = row - row_begin[g];
+    solve_row<T>(s_grid.P, s_grid.a, s_grid.a.row_map != nullptr ? s_grid.a.row_map[lr] : lr, ws, sh, prof);
   }
 }
 

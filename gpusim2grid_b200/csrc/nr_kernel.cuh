@@ -51,7 +51,8 @@ struct DevPlan {
 
 // One launch = one sweep over a list of rows.
 struct SweepArgs {
-  int n_rows;
+  int n_rows;             // rows of this launch (queue length)
+  const int* row_map;     // [n_rows] row of the session solved for queue entry q (nullptr: q itself)
   const double* ybus;     // [2 * nnz_y] interleaved complex base Ybus values
   const double* v0;       // start voltage, complex, row r at v0 + 2 * r * v0_stride
   int64_t v0_stride;      // in complex elements (0: shared)

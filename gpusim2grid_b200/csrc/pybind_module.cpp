@@ -204,6 +204,20 @@ class Session {
     check(gs2g_set_start_rows_device(h(), n_rows, reinterpret_cast<const double*>(ptr)));
   }
 
+  void run_subset(IArr rows, int max_iter, double tol, bool fixed_iters, int precision, int start,
+                  double pivot_floor, int n_ctas, int refactor, double refactor_ratio, int max_reuse, bool rescue) {
+    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, false, refactor,
+                                refactor_ratio, max_reuse, rescue);
+    const int n = (int)rows.size();
+    const int* rp = rows.data();
+    int rc;
+    {
+      py::gil_scoped_release nogil;
+      rc = gs2g_run_subset(h(), &o, n, rp);
+    }
+    check(rc);
+  }
+
   void replan(int tail_policy, double dense_rate, int force_tau) {
     check(gs2g_session_replan(h(), tail_policy, dense_rate, force_tau));
   }
@@ -510,6 +524,10 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("set_start_rows_device", &Session::set_start_rows_device)
       .def("start_rows_buffer", &Session::start_rows_buffer)
       .def("set_branch_limits", &Session::set_branch_limits)
+      .def("run_subset", &Session::run_subset, py::arg("rows"), py::arg("max_iter"), py::arg("tol"),
+           py::arg("fixed_iters"), py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0,
+           py::arg("n_ctas") = 0, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
+           py::arg("rescue") = false)
       .def("branch_loading", &Session::branch_loading)
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)

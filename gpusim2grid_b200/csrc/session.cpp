@@ -110,6 +110,7 @@ struct gs2g_session {
   DevBuf d_v_out, d_res, d_status, d_iters, d_factors;
   DevBuf d_ws, d_queue, d_phase;
   DevBuf d_multi;  // grid table of gs2g_run_multi (when this session leads)
+  DevBuf d_row_map;  // rows of gs2g_run_subset
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
 
@@ -929,6 +930,46 @@ int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
   const int nr = rp.nr;
   s->tm.kernel_ms = launch(s, o, nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob, o.n_ctas);
   s->last_rows_run = nr;
+  s->tm.total_ms = ms_since(t0);
+  s->tm.total_iters = -1;
+  GS2G_CATCH
+}
+
+int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const int* rows) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  gs2g_run_opts o = checked(o_);
+  if (n_sub < 0 || (n_sub > 0 && !rows)) throw std::invalid_argument("run_subset: bad row list");
+  DeviceGuard g(s->device);
+  auto t0 = std::chrono::steady_clock::now();
+  assemble_rows(s);
+  if (s->last_rows_run != s->n_rows)
+    throw std::invalid_argument("run_subset: run the full batch (gs2g_run) before re-running a subset of it");
+  for (int i = 0; i < n_sub; ++i)
+    if (rows[i] < 0 || rows[i] >= s->n_rows) throw std::invalid_argument("run_subset: row index out of range");
+  s->tm.upload_ms = ms_since(t0);
+  const RunPrep rp = prepare_rows(s, o);
+  s->d_row_map.ensure(std::max(n_sub, 1) * sizeof(int));
+  if (n_sub) ck(cudaMemcpy(s->d_row_map.p, rows, n_sub * sizeof(int), cudaMemcpyHostToDevice), "upload row map");
+  gs2g::SweepArgs a = make_args(s, o, n_sub, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
+  a.row_map = s->d_row_map.as<int>();
+  int n_ctas = o.n_ctas > 0 ? o.n_ctas : gs2g::sweep_ctas(o.precision, s->device);
+  n_ctas = std::max(1, std::min(n_ctas, std::max(n_sub, 1)));
+  const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
+  s->d_ws.ensure((size_t)wsb * n_ctas);
+  s->d_queue.ensure(2 * sizeof(int));
+  a.queue = s->d_queue.as<int>();
+  a.workspace = s->d_ws.as<char>();
+  a.ws_stride = wsb;
+  a.n_rescued = s->d_queue.as<int>() + 1;
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck(cudaEventRecord(s->ev0, s->stream), "event");
+  if (n_sub > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "subset launch");
+  ck(cudaEventRecord(s->ev1, s->stream), "event");
+  ck(cudaStreamSynchronize(s->stream), "subset sweep");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
+  s->tm.kernel_ms = ms;
   s->tm.total_ms = ms_since(t0);
   s->tm.total_iters = -1;
   GS2G_CATCH

@@ -177,6 +177,12 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual);
 
 /* Run every row.  Results stay on the device until read. */
 int gs2g_run(gs2g_session* s, const gs2g_run_opts* o);
+/* Re-run some rows of the last full run in place (other options allowed,
+ * e.g. FP64 from Vinit for the rows a mixed-precision run did not converge):
+ * rows[0..n_sub) index the assembled rows; their outputs are overwritten,
+ * every other row's stay.  Needs a full gs2g_run of the same rows first.
+ * The facades use it for the FP64 fallback of mixed-precision sweeps. */
+int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o, int n_sub, const int* rows);
 /* Several grids in ONE persistent launch: the current rows of every session
  * (as gs2g_run would run them, same options for all) are solved by one
  * kernel launch whose CTAs take rows from one queue across the grids, each
