@@ -252,7 +252,7 @@ class _BatchSweep:
         if self._start == "learned":
             self._warm["n_rescued"] = int(tm["n_rescued"])
         kernel_ms = tm["kernel_ms"]
-        kernel_ms += self._fp64_fallback(n_ctas)
+        kernel_ms += self.fp64_fallback(n_ctas)
         tm = dict(tm, kernel_ms=kernel_ms)
         self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
                                      t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
@@ -260,7 +260,7 @@ class _BatchSweep:
         self._ran = True
         self._host = None
 
-    def _fp64_fallback(self, n_ctas=0):
+    def fp64_fallback(self, n_ctas=0):
         """Re-solve, in plain FP64 from Vinit, the rows a mixed-precision
         continuous run left MAX_ITER or DIVERGED (the north star's "flat-start
         FP64 NR remains the fallback").  Returns its kernel ms."""
@@ -473,7 +473,7 @@ def compute_many(sweeps, batch_size=0):
     kernel_ms = sweeps[0]._s.timings()["kernel_ms"]
     for f in sweeps:
         f._ran = True
-        kernel_ms += f._fp64_fallback()
+        kernel_ms += f.fp64_fallback()
     total_ms = (time.perf_counter() - t0) * 1e3
     for f in sweeps:
         tm = f._s.timings()
