@@ -34,7 +34,8 @@ from ._native import lib
 __all__ = ["ContingencyAnalysisGPU", "InjectionSweepGPU", "ScenarioSweepGPU", "compute_many"]
 
 _START = {"base": lib.START_BASE, "flat": lib.START_VINIT, "rows": lib.START_ROWS, "learned": lib.START_ROWS}
-_STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE}
+_STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAPTIVE,
+             "base_chord": lib.REFACTOR_BASE_CHORD}
 
 
 def _rows_csr(branch_ids_per_row):

@@ -511,7 +511,12 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     // it, with a fresh Newton budget (iterations and factorizations add up)
     for (int attempt = 0;; ++attempt) {
     int it = 0;
-    bool have_factor = false;
+    // policy 2 starts on the base case's factor (shared by every CTA, read
+    // only) and moves to the row's own factor at its first refactor
+    const bool on_base = a.refactor_policy == 2 && a.base_ws != nullptr && attempt == 0 && !a.factor_only;
+    const T* fHV = on_base ? reinterpret_cast<const T*>(a.base_ws + L.HV) : HV;
+    const T* fS = on_base ? reinterpret_cast<const T*>(a.base_ws + L.S) : S;
+    bool have_factor = on_base;
     int since_factor = 0;
     double last_nrm = INFINITY;
     for (;;) {
@@ -546,7 +551,9 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       nrm = block_nanmax(lmax, s_red);
       prof.mark(PH_MISMATCH);
       const bool finite = isfinite(nrm);
-      if (a.fixed_iters) {
+      if (a.factor_only) {
+        // factor the Jacobian at the start voltage, nothing else
+      } else if (a.fixed_iters) {
         if (it >= a.max_iter || !finite) {
           status = !finite ? ROW_DIVERGED : (nrm < a.tol ? ROW_CONVERGED : ROW_MAX_ITER);
           break;
@@ -565,7 +572,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // block-uniform, so the branch is taken by the whole CTA.
       // (the rescue attempt restarts from Vinit, far from the solution: full
       // Newton there)
-      const bool refactor = !have_factor || a.refactor_policy == 0 || attempt > 0 ||
+      const bool refactor = a.factor_only || !have_factor || a.refactor_policy == 0 || attempt > 0 ||
                             !(nrm <= a.refactor_ratio * last_nrm) || since_factor >= a.max_reuse;
       last_nrm = nrm;
       if (refactor) {
@@ -652,8 +659,11 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
       if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+      fHV = HV;
+      fS = S;
       }  // refactor
       ++since_factor;
+      if (a.factor_only) break;
 
       prof.mark(PH_DENSE);
       // ---- solves -----------------------------------------------------------
@@ -663,7 +673,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int i = P.lev_piv[q0];
           T acc = y[i];
-          for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= HV[P.fw_pos[q]] * y[P.fw_col[q]];
+          for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
           y[i] = acc;
         }
         __syncthreads();
@@ -672,7 +682,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       for (int ti = tid; ti < P.nt; ti += BS) {
         const int i = P.p + ti;
         T acc = y[i];
-        for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= HV[P.fw_pos[q]] * y[P.fw_col[q]];
+        for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
         y[i] = acc;
       }
       __syncthreads();
@@ -683,15 +693,15 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
         const bool y_in_smem = P.nt + 32 * stage_stride<T>() + 32 <= dense_smem_elems<T>();
         T* ys = y_in_smem ? s_dense : y + P.p;
         T* sbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
-        dense_solves<T>(S, P.nt, P.ld, y + P.p, s_blk, ys, sbuf);
+        dense_solves<T>(fS, P.nt, P.ld, y + P.p, s_blk, ys, sbuf);
       }
       prof.mark(PH_SOLVE_DENSE);
       for (int lv = P.n_levels - 1; lv >= 0; --lv) {
         for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
           const int k = P.lev_piv[q0];
           T acc = y[k];
-          for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) acc -= HV[P.bw_pos[q]] * y[P.bw_row[q]];
-          y[k] = acc / HV[k];
+          for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) acc -= fHV[P.bw_pos[q]] * y[P.bw_row[q]];
+          y[k] = acc / fHV[k];
         }
         __syncthreads();
       }

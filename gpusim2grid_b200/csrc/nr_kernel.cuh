@@ -65,7 +65,8 @@ struct SweepArgs {
   int max_iter;
   double tol;
   int fixed_iters;        // 1: exactly max_iter steps then the residual; 0: stop at tol
-  int refactor_policy;    // 0: refactor every step; 1: reuse the LU while ||F|| contracts
+  int refactor_policy;    // 0: refactor every step; 1: reuse the LU while ||F|| contracts;
+                          // 2: as 1, starting on the base case's factor (base_ws)
   double refactor_ratio;  // policy 1: refactor when ||F_k|| > ratio * ||F_{k-1}||
   int max_reuse;          // policy 1: refactor after this many steps on one LU
   int* factors_out;       // [n_rows] LU factorizations per row (nullptr: not recorded)
@@ -74,6 +75,11 @@ struct SweepArgs {
   // the restarts (nullptr: not counted)
   const double* rescue_v0;
   int* n_rescued;
+  // policy 2: workspace (ws_layout of this plan and precision) holding the
+  // base case's factor, shared read-only by every CTA; factor_only: factor
+  // the Jacobian at the start voltage into the CTA's workspace and stop
+  const char* base_ws;
+  int factor_only;
   // branch flows and limit check when the row leaves (loading_out nullptr: off)
   int n_branch;
   const int* br_from;

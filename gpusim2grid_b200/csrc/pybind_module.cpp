@@ -500,6 +500,7 @@ PYBIND11_MODULE(_gs2g, m) {
   m.attr("START_ROWS") = GS2G_START_ROWS;
   m.attr("REFACTOR_EVERY") = GS2G_REFACTOR_EVERY;
   m.attr("REFACTOR_ADAPTIVE") = GS2G_REFACTOR_ADAPTIVE;
+  m.attr("REFACTOR_BASE_CHORD") = GS2G_REFACTOR_BASE_CHORD;
   m.def("version", &gs2g_version);
   m.def("max_edits_per_row", &gs2g_max_edits_per_row);
   m.def("acpf_nr", &acpf_nr);

@@ -111,6 +111,8 @@ struct gs2g_session {
   DevBuf d_ws, d_queue, d_phase;
   DevBuf d_multi;  // grid table of gs2g_run_multi (when this session leads)
   DevBuf d_row_map;  // rows of gs2g_run_subset
+  DevBuf d_base_ws;        // base case's factor for GS2G_REFACTOR_BASE_CHORD
+  int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
 
@@ -387,9 +389,12 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.status_out = out.status;
   a.iters_out = out.iters;
   a.pivot_floor = o.pivot_floor;
-  if (o.refactor_policy != GS2G_REFACTOR_EVERY && o.refactor_policy != GS2G_REFACTOR_ADAPTIVE)
-    throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY or GS2G_REFACTOR_ADAPTIVE");
+  if (o.refactor_policy != GS2G_REFACTOR_EVERY && o.refactor_policy != GS2G_REFACTOR_ADAPTIVE &&
+      o.refactor_policy != GS2G_REFACTOR_BASE_CHORD)
+    throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY, _ADAPTIVE or _BASE_CHORD");
   a.refactor_policy = o.refactor_policy;
+  if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD && use_rows && s->base_factor_prec == o.precision)
+    a.base_ws = s->d_base_ws.as<char>();
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
   a.factors_out = out.factors;
@@ -590,6 +595,7 @@ int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int
   s->plan = std::move(P);
   s->plan_bufs.clear();
   upload_plan(s);
+  s->base_factor_prec = -1;
   s->tm.plan_ms = s->plan.build_ms;
   GS2G_CATCH
 }
@@ -844,6 +850,7 @@ int gs2g_solve_base(gs2g_session* s, const gs2g_run_opts* o_, double* v_out, int
   s->d_basev.ensure(2 * n * sizeof(double));
   ck(cudaMemcpy(s->d_basev.p, s->b_v.p, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice), "keep base V");
   s->has_base = true;
+  s->base_factor_prec = -1;
   if (v_out) std::memcpy(v_out, s->base_v.data(), 2 * n * sizeof(double));
   if (status) *status = st;
   if (iters) *iters = it;
@@ -873,6 +880,7 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual) {
   ck(cudaMemcpy(&res, s->b_res.p, sizeof(double), cudaMemcpyDeviceToHost), "read residual");
   s->base_v.assign(v, v + 2 * n);
   s->has_base = true;
+  s->base_factor_prec = -1;
   if (residual) *residual = res;
   GS2G_CATCH
 }
@@ -888,7 +896,39 @@ struct RunPrep {
   OutBufs ob;
 };
 
+// Factor the base case's Jacobian (base V, base Ybus) once per precision
+// into the session's base workspace: one CTA in factor-only mode whose
+// workspace is that buffer.  GS2G_REFACTOR_BASE_CHORD rows start on it.
+void ensure_base_factor(gs2g_session* s, int prec) {
+  if (s->base_factor_prec == prec) return;
+  if (!s->has_base)
+    throw std::runtime_error("refactor policy BASE_CHORD needs a base case (solve_base or set_base_v first)");
+  const int n = s->n_bus;
+  const int64_t wsb = gs2g::workspace_bytes(s->dplan, prec);
+  s->d_base_ws.ensure((size_t)wsb);
+  s->b_v.ensure(2 * n * sizeof(double));
+  s->b_res.ensure(sizeof(double));
+  s->b_status.ensure(sizeof(int));
+  s->b_iters.ensure(sizeof(int));
+  gs2g_run_opts o{};
+  o.max_iter = 1;
+  o.precision = prec;
+  o.refactor_policy = GS2G_REFACTOR_EVERY;
+  OutBufs ob{s->b_v.as<double>(), s->b_res.as<double>(), s->b_status.as<int>(), s->b_iters.as<int>()};
+  gs2g::SweepArgs a = make_args(s, o, 1, s->d_basev.as<double>(), 0, s->d_sbus.as<double>(), 0, false, ob);
+  a.factor_only = 1;
+  s->d_queue.ensure(2 * sizeof(int));
+  a.queue = s->d_queue.as<int>();
+  a.workspace = s->d_base_ws.as<char>();
+  a.ws_stride = wsb;
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, prec, 1, s->stream), "base factor launch");
+  ck(cudaStreamSynchronize(s->stream), "base factor");
+  s->base_factor_prec = prec;
+}
+
 RunPrep prepare_rows(gs2g_session* s, const gs2g_run_opts& o) {
+  if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD) ensure_base_factor(s, o.precision);
   const int nr = s->n_rows;
   const int n = s->n_bus;
   const double* v0 = s->d_vinit.as<double>();

@@ -97,6 +97,12 @@ typedef struct gs2g_run_opts {
 
 #define GS2G_REFACTOR_EVERY 0
 #define GS2G_REFACTOR_ADAPTIVE 1
+/* As ADAPTIVE, but every row starts its chord steps on the base case's
+ * factor (its Jacobian at the base V; computed once per session and
+ * precision, shared read-only by all rows) and factors its own Jacobian only
+ * when a step stops contracting.  Needs a base case (solve_base or
+ * set_base_v). */
+#define GS2G_REFACTOR_BASE_CHORD 2
 
 /* mismatch, fill, head LU, Schur, dense LU, solve: head forward, tail forward,
  * dense tail, head backward; update */
