@@ -71,8 +71,9 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--strategy", choices=["adaptive", "refactor_every"], default="adaptive",
-                    help="linear-solve strategy of the measured arm (the FP64 comparison arm always refactors)")
+    ap.add_argument("--strategy", choices=["auto", "adaptive", "base_chord", "refactor_every"], default="auto",
+                    help="linear-solve strategy of the measured arm (the FP64 comparison arm always refactors); "
+                         "auto: base_chord for rows without tripped branches, adaptive otherwise")
     ap.add_argument("--cpu-sample-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
@@ -232,11 +233,17 @@ def _train_learned(g, args, device, n_rows=None):
     return ls, rep, mix
 
 
+def _strategy(args, trips):
+    if args.strategy != "auto":
+        return args.strategy
+    return "base_chord" if trips is None else "adaptive"
+
+
 def _facade(g, trips, p, q, args, local):
     """The reference-facing facade for the workload's rows (host inputs)."""
     from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, ScenarioSweepGPU
     kw = dict(init_from_n_powerflow=False, precision=args.precision, nb_iter=MAX_ITER, scheduling="continuous",
-              tol=TOL, start="flat", device=local, strategy=args.strategy)
+              tol=TOL, start="flat", device=local, strategy=_strategy(args, trips))
     if p is None:
         f = ContingencyAnalysisGPU(g.as_tuple(), **kw)
         f.set_branch_data(*g.branch_data())
@@ -280,7 +287,8 @@ def run_ours(args):
     learned = args.start == "learned"
     prec = lib.PREC_MIXED if args.precision == "mixed" else lib.PREC_FP64
     ca = _facade(g, trips, p, q, args, local)
-    strat = lib.REFACTOR_ADAPTIVE if args.strategy == "adaptive" else lib.REFACTOR_EVERY
+    strat = {"adaptive": lib.REFACTOR_ADAPTIVE, "base_chord": lib.REFACTOR_BASE_CHORD,
+             "refactor_every": lib.REFACTOR_EVERY}[_strategy(args, trips)]
     s = ca.session
     info = s.info()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -435,7 +443,7 @@ def run_ours(args):
         "dtype": "f64 mismatch/V, f32 J/LU, bf16 MLP" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": args.workload, "grid": gname, "rows": n, "start": args.start,
-                   "precision": args.precision, "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER,
+                   "precision": args.precision, "strategy": _strategy(args, trips), "tol_pu": TOL, "max_iter": MAX_ITER,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
         "rows_converged": n_conv, "rows_rescued": n_rescued, "rows_fp64_fallback": fallback_rows,
         "newton_iters_total": total_iters,
@@ -533,7 +541,8 @@ def run_ours_multi(args):
         if args.tune_rates:
             f.autotune(tuple(args.tune_rates), repeats=1)
     ratio, reuse = facades[0]._learned_opts if learned else (0.0, 0)
-    strat = lib.REFACTOR_ADAPTIVE if args.strategy == "adaptive" else lib.REFACTOR_EVERY
+    strat = {"adaptive": lib.REFACTOR_ADAPTIVE, "base_chord": lib.REFACTOR_BASE_CHORD,
+             "refactor_every": lib.REFACTOR_EVERY}[facades[0]._strategy]
     sessions = [f.session for f in facades]
     start_mode = lib.START_ROWS if learned else lib.START_VINIT
     ev0 = torch.cuda.Event(enable_timing=True)

@@ -120,7 +120,7 @@ class _BatchSweep:
             raise ValueError("start='learned' needs set_learned_start() first")
         self._start = value
 
-    def set_learned_start(self, learned, refactor_ratio=0.5, max_reuse=6):
+    def set_learned_start(self, learned, refactor_ratio=None, max_reuse=None):
         """Start every row from the voltages ``learned`` (a trained
         ``warmstart.LearnedStart`` of this grid) predicts for it, on the
         device, at every ``compute()``; switches ``start`` to 'learned'.
@@ -130,7 +130,11 @@ class _BatchSweep:
         if learned.grid.n_bus != self.n_bus:
             raise ValueError("the learned start belongs to a grid of another size")
         self._learned = learned
-        self._learned_opts = (float(refactor_ratio), int(max_reuse))
+        # on the shared base factor a step may contract more slowly before a
+        # row's own LU pays off
+        chord = self._strategy == "base_chord"
+        self._learned_opts = (float(refactor_ratio if refactor_ratio is not None else (0.7 if chord else 0.5)),
+                              int(max_reuse if max_reuse is not None else (8 if chord else 6)))
         self.start = "learned"
 
     def _row_defs(self):

@@ -414,8 +414,10 @@ struct PhaseProf {
 
 __host__ __device__ __forceinline__ int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
 
+constexpr int MAX_COMP = 16;  // compensated Jacobian positions per row (base_chord)
+
 struct WsLayout {
-  int64_t V, I, F, HV, S, y, total;
+  int64_t V, I, F, HV, S, y, Z, total;
 };
 
 template <typename T>
@@ -428,8 +430,56 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
   w.HV = o; o = align256(o + (int64_t)P.n_hv * sizeof(T));
   w.S = o; o = align256(o + (int64_t)P.nt * P.ld * sizeof(T));
   w.y = o; o = align256(o + (int64_t)P.dim * sizeof(T));
+  w.Z = o; o = align256(o + (int64_t)MAX_COMP * P.dim * sizeof(T));
   w.total = o;
   return w;
+}
+
+// y <- (LU)^-1 y with a factor (head values fHV, dense tail fS): forward
+// over the head levels, the tail rows against the head, the dense tail
+// forward + backward, backward over the head levels.
+template <typename T>
+__device__ __forceinline__ void apply_factor(const DevPlan& P, const T* fHV, const T* fS, T* y, T* s_blk, T* s_dense,
+                                             PhaseProf& prof) {
+  const int tid = threadIdx.x;
+  for (int lv = 0; lv < P.n_levels; ++lv) {
+    for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+      const int i = P.lev_piv[q0];
+      T acc = y[i];
+      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+  prof.mark(PH_SOLVE);
+  for (int ti = tid; ti < P.nt; ti += BS) {
+    const int i = P.p + ti;
+    T acc = y[i];
+    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
+    y[i] = acc;
+  }
+  __syncthreads();
+  prof.mark(PH_SOLVE_TAIL);
+  if (P.nt > 0)
+  {
+    // y tail in shared memory when it fits, the diagonal-block buffer after it
+    const bool y_in_smem = P.nt + 32 * stage_stride<T>() + 32 <= dense_smem_elems<T>();
+    T* ys = y_in_smem ? s_dense : y + P.p;
+    T* sbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
+    dense_solves<T>(fS, P.nt, P.ld, y + P.p, s_blk, ys, sbuf);
+  }
+  prof.mark(PH_SOLVE_DENSE);
+  for (int lv = P.n_levels - 1; lv >= 0; --lv) {
+    for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+      const int k = P.lev_piv[q0];
+      T acc = y[k];
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) acc -= fHV[P.bw_pos[q]] * y[P.bw_row[q]];
+      y[k] = acc / fHV[k];
+    }
+    __syncthreads();
+  }
+
+  prof.mark(PH_SOLVE_BACK);
 }
 
 // Shared-memory scratch of one CTA, handed to solve_row.
@@ -441,7 +491,188 @@ struct RowShared {
   double* s_red;
   T* s_blk;
   T* s_dense;
+  // outage compensation on the base factor (see setup_compensation)
+  int* s_cr;      // [1 + MAX_COMP]: r, then the compensated positions
+  double* s_cB;   // [MAX_COMP^2] Delta J on those positions (row-major)
+  double* s_cLU;  // [MAX_COMP^2] LU of I + W B (partial pivoting)
+  int* s_cpiv;    // [MAX_COMP]
+  double* s_cw;   // [MAX_COMP]
 };
+
+// One Jacobian entry pair of Ybus entry (i, j) with value yk at voltages
+// Vi, Vj and current Ii (the J-fill formulas): out = {dP/dtheta_j,
+// dP/dVm_j, dQ/dtheta_j, dQ/dVm_j}.
+__device__ __forceinline__ void jac_entry(bool diag, double2 yk, double2 Vi, double2 Vj, double2 Ii, double out[4]) {
+  double2 dVa, dVm;
+  if (diag) {
+    const double2 t = cmul(Vi, conj2(csub(Ii, cmul(yk, Vi))));
+    dVa = make_double2(-t.y, t.x);
+    const double inv = 1.0 / hypot(Vi.x, Vi.y);
+    const double2 vn = make_double2(Vi.x * inv, Vi.y * inv);
+    dVm = cadd(cmul(Vi, conj2(cmul(yk, vn))), cmul(conj2(Ii), vn));
+  } else {
+    const double2 t = cmul(Vi, conj2(cmul(yk, Vj)));
+    dVa = make_double2(t.y, -t.x);
+    const double inv = 1.0 / hypot(Vj.x, Vj.y);
+    const double2 vn = make_double2(Vj.x * inv, Vj.y * inv);
+    dVm = cmul(Vi, conj2(cmul(yk, vn)));
+  }
+  out[0] = dVa.x;
+  out[1] = dVm.x;
+  out[2] = dVa.y;
+  out[3] = dVm.y;
+}
+
+// Outage compensation (policy 2, rows with Ybus edits).  The chord matrix of
+// a row is its Jacobian at the base voltage Vb, M = M0 + E B E^T, where M0 is
+// the base factor and B = Delta J is confined to the P/Q rows and theta/Vm
+// columns of the buses the edits touch (positions R, r <= MAX_COMP).  With
+// Z = M0^-1 E (r solves) and W = E^T Z, Woodbury gives
+//   M^-1 F = x0 - Z B (I + W B)^-1 x0[R],   x0 = M0^-1 F.
+// Returns false (no compensation) when the row touches too many positions.
+template <typename T>
+__device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits ed, const double2* Y,
+                                                const double2* Vb, const T* bHV, const T* bS, T* y, T* Zc,
+                                                const RowShared<T> sh) {
+  const int tid = threadIdx.x;
+  PhaseProf prof;  // not profiled: its solves count with the row's setup
+  prof.init(false);
+  int* R = sh.s_cr + 1;
+  if (tid == 0) {
+    int r = 0;
+    bool ok = true;
+    auto add = [&](int pos) {
+      if (pos < 0) return;
+      for (int q = 0; q < r; ++q)
+        if (R[q] == pos) return;
+      if (r < MAX_COMP) R[r++] = pos;
+      else ok = false;
+    };
+    for (int e = 0; e < ed.n; ++e) {
+      const int k = ed.k[e];
+      const int i = P.y_row[k], j = P.y_indices[k];
+      add(P.fP[i]);
+      add(P.fQ[i]);
+      add(P.fP[j]);
+      add(P.fQ[j]);
+    }
+    sh.s_cr[0] = ok ? r : -1;
+    // B = J(Vb, Y_row) - J(Vb, Y_base) on R x R: rows of the edited buses
+    if (ok) {
+      for (int q = 0; q < r * r; ++q) sh.s_cB[q] = 0.0;
+      auto slot = [&](int pos) {
+        for (int q = 0; q < r; ++q)
+          if (R[q] == pos) return q;
+        return -1;
+      };
+      for (int e = 0; e < ed.n; ++e) {
+        const int i = P.y_row[ed.k[e]];
+        bool seen = false;
+        for (int e2 = 0; e2 < e; ++e2) seen |= P.y_row[ed.k[e2]] == i;
+        if (seen) continue;  // each edited row once
+        double2 Ib = make_double2(0.0, 0.0), Ir = make_double2(0.0, 0.0);
+        for (int k = P.y_indptr[i]; k < P.y_indptr[i + 1]; ++k) {
+          const double2 vj = Vb[P.y_indices[k]];
+          Ib = cadd(Ib, cmul(Y[k], vj));
+          Ir = cadd(Ir, cmul(ed.apply(k, Y[k]), vj));
+        }
+        const int rp = slot(P.fP[i]), rq = slot(P.fQ[i]);
+        for (int k = P.y_indptr[i]; k < P.y_indptr[i + 1]; ++k) {
+          const int j = P.y_indices[k];
+          const int cp = slot(P.fP[j]), cq = slot(P.fQ[j]);
+          if (cp < 0 && cq < 0) continue;
+          double jb[4], jr[4];
+          jac_entry(i == j, Y[k], Vb[i], Vb[j], Ib, jb);
+          jac_entry(i == j, ed.apply(k, Y[k]), Vb[i], Vb[j], Ir, jr);
+          const int rows[4] = {rp, rp, rq, rq}, cols[4] = {cp, cq, cp, cq};
+          for (int q = 0; q < 4; ++q)
+            if (rows[q] >= 0 && cols[q] >= 0) sh.s_cB[rows[q] * r + cols[q]] += jr[q] - jb[q];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const int r = sh.s_cr[0];
+  if (r <= 0) return false;
+  // Z = M0^-1 E, one solve per compensated position
+  for (int c = 0; c < r; ++c) {
+    const int pos = R[c];
+    for (int i = tid; i < P.dim; i += BS) y[i] = T(i == pos ? 1 : 0);
+    __syncthreads();
+    apply_factor<T>(P, bHV, bS, y, sh.s_blk, sh.s_dense, prof);
+    for (int i = tid; i < P.dim; i += BS) Zc[(int64_t)c * P.dim + i] = y[i];
+  }
+  __syncthreads();
+  // LU (partial pivoting) of C = I + W B, W[a][c] = Z_c[R[a]]
+  if (tid == 0) {
+    double* C = sh.s_cLU;
+    for (int i2 = 0; i2 < r; ++i2)
+      for (int j2 = 0; j2 < r; ++j2) {
+        double acc = i2 == j2 ? 1.0 : 0.0;
+        for (int c = 0; c < r; ++c) acc += (double)Zc[(int64_t)c * P.dim + R[i2]] * sh.s_cB[c * r + j2];
+        C[i2 * r + j2] = acc;
+      }
+    for (int k = 0; k < r; ++k) {
+      int pk = k;
+      for (int i2 = k + 1; i2 < r; ++i2)
+        if (fabs(C[i2 * r + k]) > fabs(C[pk * r + k])) pk = i2;
+      sh.s_cpiv[k] = pk;
+      if (pk != k)
+        for (int j2 = 0; j2 < r; ++j2) {
+          const double t = C[k * r + j2];
+          C[k * r + j2] = C[pk * r + j2];
+          C[pk * r + j2] = t;
+        }
+      const double d = C[k * r + k];
+      for (int i2 = k + 1; i2 < r; ++i2) {
+        const double l = C[i2 * r + k] / d;
+        C[i2 * r + k] = l;
+        for (int j2 = k + 1; j2 < r; ++j2) C[i2 * r + j2] -= l * C[k * r + j2];
+      }
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// y <- y - Z B (I + W B)^-1 y[R]  (see setup_compensation)
+template <typename T>
+__device__ __noinline__ void apply_compensation(int dim, T* y, const T* Zc, const RowShared<T> sh) {
+  const int tid = threadIdx.x;
+  const int r = sh.s_cr[0];
+  const int* R = sh.s_cr + 1;
+  if (tid == 0) {
+    double v[MAX_COMP];
+    for (int q = 0; q < r; ++q) v[q] = (double)y[R[q]];
+    const double* C = sh.s_cLU;
+    for (int k = 0; k < r; ++k) {  // P v, then L, then U
+      const int pk = sh.s_cpiv[k];
+      if (pk != k) {
+        const double t = v[k];
+        v[k] = v[pk];
+        v[pk] = t;
+      }
+    }
+    for (int i2 = 1; i2 < r; ++i2)
+      for (int k = 0; k < i2; ++k) v[i2] -= C[i2 * r + k] * v[k];
+    for (int i2 = r - 1; i2 >= 0; --i2) {
+      for (int k = i2 + 1; k < r; ++k) v[i2] -= C[i2 * r + k] * v[k];
+      v[i2] /= C[i2 * r + i2];
+    }
+    for (int q = 0; q < r; ++q) {  // w = B v
+      double acc = 0.0;
+      for (int c = 0; c < r; ++c) acc += sh.s_cB[q * r + c] * v[c];
+      sh.s_cw[q] = acc;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < dim; i += BS) {
+    T acc = T(0);
+    for (int c = 0; c < r; ++c) acc += Zc[(int64_t)c * dim + i] * (T)sh.s_cw[c];
+    y[i] -= acc;
+  }
+  __syncthreads();
+}
 
 // The whole Newton loop of one row of one grid, by the calling CTA: start
 // voltage, edits, mismatch / Jacobian / factorization / solves / update
@@ -458,6 +689,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
   T* HV = reinterpret_cast<T*>(ws + L.HV);
   T* S = reinterpret_cast<T*>(ws + L.S);
   T* y = reinterpret_cast<T*>(ws + L.y);
+  T* Zc = reinterpret_cast<T*>(ws + L.Z);
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const int n = P.n_bus;
   int& s_ne = *sh.s_ne;
@@ -517,6 +749,10 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     const T* fHV = on_base ? reinterpret_cast<const T*>(a.base_ws + L.HV) : HV;
     const T* fS = on_base ? reinterpret_cast<const T*>(a.base_ws + L.S) : S;
     bool have_factor = on_base;
+    // rows with tripped branches correct the base factor for their outage
+    bool comp_on = false;
+    if (on_base && ed.n > 0 && a.base_v != nullptr)
+      comp_on = setup_compensation<T>(P, ed, Y, reinterpret_cast<const double2*>(a.base_v), fHV, fS, y, Zc, sh);
     int since_factor = 0;
     double last_nrm = INFINITY;
     for (;;) {
@@ -661,6 +897,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
       fHV = HV;
       fS = S;
+      comp_on = false;
       }  // refactor
       ++since_factor;
       if (a.factor_only) break;
@@ -669,44 +906,8 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // ---- solves -----------------------------------------------------------
       for (int i = tid; i < P.dim; i += BS) y[i] = (T)F[i];
       __syncthreads();
-      for (int lv = 0; lv < P.n_levels; ++lv) {
-        for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
-          const int i = P.lev_piv[q0];
-          T acc = y[i];
-          for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
-          y[i] = acc;
-        }
-        __syncthreads();
-      }
-      prof.mark(PH_SOLVE);
-      for (int ti = tid; ti < P.nt; ti += BS) {
-        const int i = P.p + ti;
-        T acc = y[i];
-        for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) acc -= fHV[P.fw_pos[q]] * y[P.fw_col[q]];
-        y[i] = acc;
-      }
-      __syncthreads();
-      prof.mark(PH_SOLVE_TAIL);
-      if (P.nt > 0)
-      {
-        // y tail in shared memory when it fits, the diagonal-block buffer after it
-        const bool y_in_smem = P.nt + 32 * stage_stride<T>() + 32 <= dense_smem_elems<T>();
-        T* ys = y_in_smem ? s_dense : y + P.p;
-        T* sbuf = s_dense + (y_in_smem ? ((P.nt + 31) & ~31) : 0);
-        dense_solves<T>(fS, P.nt, P.ld, y + P.p, s_blk, ys, sbuf);
-      }
-      prof.mark(PH_SOLVE_DENSE);
-      for (int lv = P.n_levels - 1; lv >= 0; --lv) {
-        for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
-          const int k = P.lev_piv[q0];
-          T acc = y[k];
-          for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) acc -= fHV[P.bw_pos[q]] * y[P.bw_row[q]];
-          y[k] = acc / fHV[k];
-        }
-        __syncthreads();
-      }
-
-      prof.mark(PH_SOLVE_BACK);
+      apply_factor<T>(P, fHV, fS, y, s_blk, s_dense, prof);
+      if (comp_on) apply_compensation<T>(P.dim, y, Zc, sh);
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
         const int fp = P.fP[i], fq = P.fQ[i];
@@ -791,7 +992,13 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   __shared__ double2 s_ev[MAX_EDITS];
   __shared__ double s_red[NWARP];
   __shared__ T s_blk[64];
-  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw)};
+  __shared__ int s_cr[1 + MAX_COMP];
+  __shared__ double s_cB[MAX_COMP * MAX_COMP];
+  __shared__ double s_cLU[MAX_COMP * MAX_COMP];
+  __shared__ int s_cpiv[MAX_COMP];
+  __shared__ double s_cw[MAX_COMP];
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw), s_cr, s_cB, s_cLU, s_cpiv,
+                        s_cw};
   char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   PhaseProf prof;
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
@@ -824,7 +1031,13 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
   __shared__ double s_red[NWARP];
   __shared__ T s_blk[64];
   __shared__ __align__(16) GridEntry s_grid;
-  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw)};
+  __shared__ int s_cr[1 + MAX_COMP];
+  __shared__ double s_cB[MAX_COMP * MAX_COMP];
+  __shared__ double s_cLU[MAX_COMP * MAX_COMP];
+  __shared__ int s_cpiv[MAX_COMP];
+  __shared__ double s_cw[MAX_COMP];
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw), s_cr, s_cB, s_cLU, s_cpiv,
+                        s_cw};
   char* ws = workspace + (int64_t)blockIdx.x * ws_stride;
   PhaseProf prof;
   prof.init(phase_cycles != nullptr && threadIdx.x == 0);

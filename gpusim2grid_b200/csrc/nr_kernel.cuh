@@ -79,6 +79,7 @@ struct SweepArgs {
   // base case's factor, shared read-only by every CTA; factor_only: factor
   // the Jacobian at the start voltage into the CTA's workspace and stop
   const char* base_ws;
+  const double* base_v;  // complex [n_bus]: the voltage the base factor was taken at
   int factor_only;
   // branch flows and limit check when the row leaves (loading_out nullptr: off)
   int n_branch;

@@ -393,8 +393,10 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
       o.refactor_policy != GS2G_REFACTOR_BASE_CHORD)
     throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY, _ADAPTIVE or _BASE_CHORD");
   a.refactor_policy = o.refactor_policy;
-  if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD && use_rows && s->base_factor_prec == o.precision)
+  if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD && use_rows && s->base_factor_prec == o.precision) {
     a.base_ws = s->d_base_ws.as<char>();
+    a.base_v = s->d_basev.as<double>();
+  }
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
   a.factors_out = out.factors;
