@@ -73,7 +73,10 @@ def _args():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--strategy", choices=["auto", "adaptive", "base_chord", "refactor_every"], default="auto",
                     help="linear-solve strategy of the measured arm (the FP64 comparison arm always refactors); "
-                         "auto: base_chord for rows without tripped branches, adaptive otherwise")
+                         "auto: base_chord (rows chord on the base case's factor, outages by Woodbury compensation)")
+    ap.add_argument("--refactor-ratio", type=float, default=None,
+                    help="contraction ratio above which a row factors its own Jacobian (default: the facade's)")
+    ap.add_argument("--max-reuse", type=int, default=None, help="chord steps on one factor at most (default: the facade's)")
     ap.add_argument("--cpu-sample-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
@@ -236,7 +239,7 @@ def _train_learned(g, args, device, n_rows=None):
 def _strategy(args, trips):
     if args.strategy != "auto":
         return args.strategy
-    return "base_chord" if trips is None else "adaptive"
+    return "base_chord"
 
 
 def _facade(g, trips, p, q, args, local):
@@ -310,7 +313,7 @@ def run_ours(args):
                  "val_mse": round(rep["val"][-1], 5) if rep["val"] else None,
                  "note": "untimed: training rows are seeded synthetic operating points (load scaling, single "
                          "outages) solved by this engine in FP64, drawn with another seed than the timed rows"}
-        ca.set_learned_start(ls)
+        ca.set_learned_start(ls, args.refactor_ratio, args.max_reuse)
         ratio, reuse = ca._learned_opts
     # one-time plan choice (untimed, like the symbolic analysis): the
     # head/tail split that solves these rows fastest in the measured arm
@@ -535,7 +538,7 @@ def run_ours_multi(args):
             train.append({"grid": g.name, "rows": rep["n_rows"], "unconverged_dropped": rep["n_unconverged"],
                           "t_total_s": round(time.perf_counter() - t0, 2),
                           "val_mse": round(rep["val"][-1], 5) if rep["val"] else None})
-            f.set_learned_start(ls)
+            f.set_learned_start(ls, args.refactor_ratio, args.max_reuse)
     for f in facades:
         f.start = "learned" if learned else "flat"
         if args.tune_rates:

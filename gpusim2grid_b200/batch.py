@@ -130,16 +130,44 @@ class _BatchSweep:
         if learned.grid.n_bus != self.n_bus:
             raise ValueError("the learned start belongs to a grid of another size")
         self._learned = learned
-        # on the shared base factor a step may contract more slowly before a
-        # row's own LU pays off
-        chord = self._strategy == "base_chord"
-        self._learned_opts = (float(refactor_ratio if refactor_ratio is not None else (0.7 if chord else 0.5)),
-                              int(max_reuse if max_reuse is not None else (8 if chord else 6)))
+        self._learned_override = (refactor_ratio, max_reuse)
         self.start = "learned"
+
+    @property
+    def _learned_opts(self):
+        """(refactor_ratio, max_reuse) of learned runs.  On the shared base
+        factor (base_chord) injection rows keep chording longer (0.7 / 8):
+        their Jacobian stays close to the base one.  Rows with tripped
+        branches, whose flows move further, factor their own Jacobian as
+        soon as a step contracts by less than 0.5 (at most 6 steps on one
+        factor), as under the adaptive strategy."""
+        r, m = getattr(self, "_learned_override", (None, None))
+        long_chord = self._strategy == "base_chord" and not self._rows_have_trips()
+        return (float(r if r is not None else (0.7 if long_chord else 0.5)),
+                int(m if m is not None else (8 if long_chord else 6)))
+
+    def _rows_have_trips(self):
+        return False
 
     def _row_defs(self):
         """(sbus_rows or None, trips CSR or None, n_rows) of the current rows."""
         raise NotImplementedError
+
+    def _device_row_defs(self):
+        """The current rows as ``_row_defs`` gives them, but read from the
+        session's own device copies (no host round trip): Sbus rows as a
+        (rows, n_bus) complex128 tensor, trips as a device CSR (ptr, ids)."""
+        import torch
+        sb, tp, ti = (self._s.device_rows(w) for w in ("sbus", "trip_ptr", "trip_ids"))
+        sbus = torch.from_dlpack(sb) if sb is not None else None
+        trips = (torch.from_dlpack(tp), torch.from_dlpack(ti)) if tp is not None else None
+        if sbus is not None:
+            n = sbus.shape[0]
+        elif trips is not None:
+            n = trips[0].numel() - 1
+        else:
+            n = self._row_defs()[2]
+        return sbus, trips, n
 
     def autotune(self, dense_rates=(40.0, 80.0, 160.0, 320.0, 640.0), repeats=2, batch_size=512):
         """Pick the symbolic plan that solves the current rows fastest.  Each
@@ -243,7 +271,7 @@ class _BatchSweep:
         rescue = self._start in ("rows", "learned")
         if self._start == "learned":
             import torch
-            sbus, trips, n = self._row_defs()
+            sbus, trips, n = self._device_row_defs()
             # V0 is written in place into the session's start-row buffer on
             # torch's stream, which must be done before the session's launch
             self._learned.start_voltages(sbus, trips, n, out_ptr=self._s.start_rows_buffer(n))
@@ -378,6 +406,9 @@ class ContingencyAnalysisGPU(_BatchSweep):
     def _row_defs(self):
         return None, self._ctg_csr, len(self._ctg)
 
+    def _rows_have_trips(self):
+        return True
+
     @property
     def n_contingencies(self):
         return len(self._ctg)
@@ -435,6 +466,9 @@ class ScenarioSweepGPU(InjectionSweepGPU):
         p, q, sn = self._inj
         return (p + 1j * q) / sn, (self._topo_csr if self._topo is not None else None), self._n_scen
 
+    def _rows_have_trips(self):
+        return self._topo is not None
+
     def get_disconnected(self):
         """(n_rows,) bool: rows whose topology islands the grid (never solved)."""
         return self.get_row_status() == RowStatus.NOT_SIMULATED
@@ -466,7 +500,7 @@ def compute_many(sweeps, batch_size=0):
     if start == "learned":
         import torch
         for f in sweeps:
-            sbus, trips, n = f._row_defs()
+            sbus, trips, n = f._device_row_defs()
             f._learned.start_voltages(sbus, trips, n, out_ptr=f._s.start_rows_buffer(n))
         torch.cuda.current_stream().synchronize()
         for f in sweeps:

@@ -417,7 +417,7 @@ __host__ __device__ __forceinline__ int64_t align256(int64_t x) { return (x + 25
 constexpr int MAX_COMP = 16;  // compensated Jacobian positions per row (base_chord)
 
 struct WsLayout {
-  int64_t V, I, F, HV, S, y, Z, total;
+  int64_t V, I, F, HV, S, y, total;
 };
 
 template <typename T>
@@ -430,7 +430,6 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
   w.HV = o; o = align256(o + (int64_t)P.n_hv * sizeof(T));
   w.S = o; o = align256(o + (int64_t)P.nt * P.ld * sizeof(T));
   w.y = o; o = align256(o + (int64_t)P.dim * sizeof(T));
-  w.Z = o; o = align256(o + (int64_t)MAX_COMP * P.dim * sizeof(T));
   w.total = o;
   return w;
 }
@@ -527,16 +526,14 @@ __device__ __forceinline__ void jac_entry(bool diag, double2 yk, double2 Vi, dou
 // a row is its Jacobian at the base voltage Vb, M = M0 + E B E^T, where M0 is
 // the base factor and B = Delta J is confined to the P/Q rows and theta/Vm
 // columns of the buses the edits touch (positions R, r <= MAX_COMP).  With
-// Z = M0^-1 E (r solves) and W = E^T Z, Woodbury gives
+// Z = M0^-1 E -- columns R of the base inverse Minv, computed once per
+// session (inverse mode of the sweep) -- and W = E^T Z, Woodbury gives
 //   M^-1 F = x0 - Z B (I + W B)^-1 x0[R],   x0 = M0^-1 F.
 // Returns false (no compensation) when the row touches too many positions.
 template <typename T>
 __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits ed, const double2* Y,
-                                                const double2* Vb, const T* bHV, const T* bS, T* y, T* Zc,
-                                                const RowShared<T> sh) {
+                                                const double2* Vb, const T* Minv, const RowShared<T> sh) {
   const int tid = threadIdx.x;
-  PhaseProf prof;  // not profiled: its solves count with the row's setup
-  prof.init(false);
   int* R = sh.s_cr + 1;
   if (tid == 0) {
     int r = 0;
@@ -594,24 +591,17 @@ __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits 
   __syncthreads();
   const int r = sh.s_cr[0];
   if (r <= 0) return false;
-  // Z = M0^-1 E, one solve per compensated position
-  for (int c = 0; c < r; ++c) {
-    const int pos = R[c];
-    for (int i = tid; i < P.dim; i += BS) y[i] = T(i == pos ? 1 : 0);
-    __syncthreads();
-    apply_factor<T>(P, bHV, bS, y, sh.s_blk, sh.s_dense, prof);
-    for (int i = tid; i < P.dim; i += BS) Zc[(int64_t)c * P.dim + i] = y[i];
+  // C = I + W B, W[a][c] = Z_c[R[a]] = Minv[R[c]][R[a]], one entry per thread
+  double* C = sh.s_cLU;
+  for (int q = tid; q < r * r; q += BS) {
+    const int i2 = q / r, j2 = q % r;
+    double acc = i2 == j2 ? 1.0 : 0.0;
+    for (int c = 0; c < r; ++c) acc += (double)Minv[(int64_t)R[c] * P.dim + R[i2]] * sh.s_cB[c * r + j2];
+    C[q] = acc;
   }
   __syncthreads();
-  // LU (partial pivoting) of C = I + W B, W[a][c] = Z_c[R[a]]
+  // its LU with partial pivoting
   if (tid == 0) {
-    double* C = sh.s_cLU;
-    for (int i2 = 0; i2 < r; ++i2)
-      for (int j2 = 0; j2 < r; ++j2) {
-        double acc = i2 == j2 ? 1.0 : 0.0;
-        for (int c = 0; c < r; ++c) acc += (double)Zc[(int64_t)c * P.dim + R[i2]] * sh.s_cB[c * r + j2];
-        C[i2 * r + j2] = acc;
-      }
     for (int k = 0; k < r; ++k) {
       int pk = k;
       for (int i2 = k + 1; i2 < r; ++i2)
@@ -637,7 +627,7 @@ __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits 
 
 // y <- y - Z B (I + W B)^-1 y[R]  (see setup_compensation)
 template <typename T>
-__device__ __noinline__ void apply_compensation(int dim, T* y, const T* Zc, const RowShared<T> sh) {
+__device__ __noinline__ void apply_compensation(int dim, T* y, const T* Minv, const RowShared<T> sh) {
   const int tid = threadIdx.x;
   const int r = sh.s_cr[0];
   const int* R = sh.s_cr + 1;
@@ -668,7 +658,7 @@ __device__ __noinline__ void apply_compensation(int dim, T* y, const T* Zc, cons
   __syncthreads();
   for (int i = tid; i < dim; i += BS) {
     T acc = T(0);
-    for (int c = 0; c < r; ++c) acc += Zc[(int64_t)c * dim + i] * (T)sh.s_cw[c];
+    for (int c = 0; c < r; ++c) acc += Minv[(int64_t)R[c] * dim + i] * (T)sh.s_cw[c];
     y[i] -= acc;
   }
   __syncthreads();
@@ -689,7 +679,6 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
   T* HV = reinterpret_cast<T*>(ws + L.HV);
   T* S = reinterpret_cast<T*>(ws + L.S);
   T* y = reinterpret_cast<T*>(ws + L.y);
-  T* Zc = reinterpret_cast<T*>(ws + L.Z);
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const int n = P.n_bus;
   int& s_ne = *sh.s_ne;
@@ -698,6 +687,17 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
   double* s_red = sh.s_red;
   T* s_blk = sh.s_blk;
   T* s_dense = sh.s_dense;
+  if (a.inverse_out != nullptr) {
+    // inverse mode: column `row` of the base factor's inverse (policy 2)
+    for (int i = tid; i < P.dim; i += BS) y[i] = T(i == row ? 1 : 0);
+    __syncthreads();
+    apply_factor<T>(P, reinterpret_cast<const T*>(a.base_ws + L.HV), reinterpret_cast<const T*>(a.base_ws + L.S), y,
+                    s_blk, s_dense, prof);
+    T* col = reinterpret_cast<T*>(a.inverse_out) + (int64_t)row * P.dim;
+    for (int i = tid; i < P.dim; i += BS) col[i] = y[i];
+    __syncthreads();
+    return;
+  }
     double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
 
     if (a.row_skip != nullptr && a.row_skip[row]) {
@@ -751,8 +751,9 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     bool have_factor = on_base;
     // rows with tripped branches correct the base factor for their outage
     bool comp_on = false;
-    if (on_base && ed.n > 0 && a.base_v != nullptr)
-      comp_on = setup_compensation<T>(P, ed, Y, reinterpret_cast<const double2*>(a.base_v), fHV, fS, y, Zc, sh);
+    const T* Minv = reinterpret_cast<const T*>(a.base_inv);
+    if (on_base && ed.n > 0 && a.base_v != nullptr && Minv != nullptr)
+      comp_on = setup_compensation<T>(P, ed, Y, reinterpret_cast<const double2*>(a.base_v), Minv, sh);
     int since_factor = 0;
     double last_nrm = INFINITY;
     for (;;) {
@@ -907,7 +908,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       for (int i = tid; i < P.dim; i += BS) y[i] = (T)F[i];
       __syncthreads();
       apply_factor<T>(P, fHV, fS, y, s_blk, s_dense, prof);
-      if (comp_on) apply_compensation<T>(P.dim, y, Zc, sh);
+      if (comp_on) apply_compensation<T>(P.dim, y, Minv, sh);
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
         const int fp = P.fP[i], fq = P.fQ[i];

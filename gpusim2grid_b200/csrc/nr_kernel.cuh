@@ -80,6 +80,8 @@ struct SweepArgs {
   // the Jacobian at the start voltage into the CTA's workspace and stop
   const char* base_ws;
   const double* base_v;  // complex [n_bus]: the voltage the base factor was taken at
+  const char* base_inv;  // [dim x dim] of the sweep's type: column c = M0^-1 e_c (outage compensation)
+  char* inverse_out;     // inverse mode: row r of the launch writes column r of M0^-1 here
   int factor_only;
   // branch flows and limit check when the row leaves (loading_out nullptr: off)
   int n_branch;

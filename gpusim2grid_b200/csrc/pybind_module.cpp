@@ -343,6 +343,25 @@ class Session {
     throw py::value_error("unknown result '" + what + "'");
   }
 
+  // DLPack capsules of the current rows on the device: "sbus" (n_rows, n_bus)
+  // complex128, "trip_ptr" (n_rows + 1,) / "trip_ids" (n_ids,) int32; None
+  // when the rows have no such definition.
+  py::object device_rows(const std::string& what) {
+    int nr = 0;
+    const double* sb = nullptr;
+    const int *tp = nullptr, *ti = nullptr;
+    int64_t nid = 0;
+    check(gs2g_get_device_rows(h(), &nr, &sb, &tp, &ti, &nid));
+    int dev = 0;
+    check(gs2g_get_device(h(), &dev));
+    if (what == "sbus") return sb ? py::object(make_dlpack(const_cast<double*>(sb), dev, 2, nr, n_bus_, kDLComplex_, 128)) : py::none();
+    if (what == "trip_ptr") return tp ? py::object(make_dlpack(const_cast<int*>(tp), dev, 1, nr + 1, 0, kDLInt_, 32)) : py::none();
+    if (what == "trip_ids")
+      return ti ? py::object(make_dlpack(const_cast<int*>(ti), dev, 1, std::max<int64_t>(nid, 0), 0, kDLInt_, 32))
+                : py::none();
+    throw py::value_error("unknown row definition '" + what + "'");
+  }
+
   py::dict timings() const {
     gs2g_timings t{};
     check(gs2g_get_timings(h(), &t));
@@ -545,6 +564,7 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("results", &Session::results)
       .def("device_results", &Session::device_results)
       .def("dlpack", &Session::dlpack)
+      .def("device_rows", &Session::device_rows)
       .def("timings", &Session::timings)
       .def("sync", &Session::sync);
 }

@@ -97,8 +97,7 @@ struct gs2g_session {
   // row definitions
   int n_ctg = 0;
   std::vector<int> ctg_ptr, ctg_ids;
-  int n_inj = 0;
-  std::vector<double> inj_sbus;  // [n_inj * n_bus] complex
+  int n_inj = 0;  // injection rows, already in d_sbus_rows (set_injections uploads them)
   int n_start = 0;
   DevBuf d_v0rows;
   bool rows_dirty = true;
@@ -112,6 +111,7 @@ struct gs2g_session {
   DevBuf d_multi;  // grid table of gs2g_run_multi (when this session leads)
   DevBuf d_row_map;  // rows of gs2g_run_subset
   DevBuf d_base_ws;        // base case's factor for GS2G_REFACTOR_BASE_CHORD
+  DevBuf d_base_inv;       // its inverse, column c = M0^-1 e_c (outage compensation)
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -279,11 +279,6 @@ void assemble_rows(gs2g_session* s) {
     s->rows_dirty = false;
     return;
   }
-  if (s->rows_have_sbus) {
-    s->d_sbus_rows.ensure(s->inj_sbus.size() * sizeof(double));
-    ck(cudaMemcpy(s->d_sbus_rows.p, s->inj_sbus.data(), s->inj_sbus.size() * sizeof(double), cudaMemcpyHostToDevice),
-       "upload sbus rows");
-  }
   if (s->rows_have_edits) {
     s->d_trip_ptr.ensure((nr + 1) * sizeof(int));
     s->d_trip_ids.ensure(std::max<size_t>(s->ctg_ids.size(), 1) * sizeof(int));
@@ -396,6 +391,7 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD && use_rows && s->base_factor_prec == o.precision) {
     a.base_ws = s->d_base_ws.as<char>();
     a.base_v = s->d_basev.as<double>();
+    a.base_inv = s->d_base_inv.as<char>();
   }
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
@@ -756,21 +752,57 @@ int gs2g_set_contingencies(gs2g_session* s, int n_rows, const int* ptr, const in
   GS2G_CATCH
 }
 
+extern "C++" {
+namespace {
+constexpr size_t kStageChunk = size_t(8) << 20;
+// the session's pinned double buffer for large copies, made on first use
+void ensure_stage(const gs2g_session* s) {
+  if (!s->h_stage) {
+    ck(cudaMallocHost(&s->h_stage, 2 * kStageChunk), "pinned staging buffer");
+    for (cudaEvent_t& e : s->ev_stage) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  }
+}
+// Large host-to-device uploads of generated data: `fill(dst, off, len)`
+// writes bytes [off, off + len) of the payload into a pinned chunk, which is
+// copied to the device while the next chunk is filled.  `len` is a multiple
+// of 16 bytes except for the last chunk.
+template <typename Fill>
+void h2d_staged(const gs2g_session* s, void* dst, size_t bytes, Fill fill) {
+  ensure_stage(s);
+  char* buf[2] = {static_cast<char*>(s->h_stage), static_cast<char*>(s->h_stage) + kStageChunk};
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  for (size_t i = 0; i < nch; ++i) {
+    const size_t off = i * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    if (i >= 2) ck(cudaEventSynchronize(s->ev_stage[i & 1]), "upload rows");  // buffer free again
+    fill(reinterpret_cast<double*>(buf[i & 1]), off, len);
+    ck(cudaMemcpyAsync(static_cast<char*>(dst) + off, buf[i & 1], len, cudaMemcpyHostToDevice, s->stream),
+       "upload rows");
+    ck(cudaEventRecord(s->ev_stage[i & 1], s->stream), "event");
+  }
+  ck(cudaStreamSynchronize(s->stream), "upload rows");
+}
+}  // namespace
+}  // extern "C++"
+
 int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const double* q_mvar, double sn_mva) {
   GS2G_TRY
   if (!s || n_rows < 0) throw std::invalid_argument("set_injections: bad arguments");
   if (n_rows > 0) {
     if (!p_mw || !q_mvar) throw std::invalid_argument("set_injections: p_mw / q_mvar must not be NULL");
     if (!(sn_mva > 0)) throw std::invalid_argument("set_injections: sn_mva must be positive");
-    const int n = s->n_bus;
-    s->inj_sbus.resize((size_t)2 * n_rows * n);
+    DeviceGuard g(s->device);
+    const size_t m = (size_t)n_rows * s->n_bus;
+    s->d_sbus_rows.ensure(m * 2 * sizeof(double));
+    // Sbus = (p + jq) / sn_mva, interleaved straight into pinned chunks that
+    // are copied to the device while the next chunk is converted
     const double inv = 1.0 / sn_mva;
-    for (size_t q = 0; q < (size_t)n_rows * n; ++q) {
-      s->inj_sbus[2 * q] = p_mw[q] * inv;
-      s->inj_sbus[2 * q + 1] = q_mvar[q] * inv;
-    }
-  } else {
-    s->inj_sbus.clear();
+    h2d_staged(s, s->d_sbus_rows.p, m * 2 * sizeof(double), [&](double* dst, size_t off, size_t len) {
+      const size_t q0 = off / (2 * sizeof(double)), nq = len / (2 * sizeof(double));
+      for (size_t q = 0; q < nq; ++q) {
+        dst[2 * q] = p_mw[q0 + q] * inv;
+        dst[2 * q + 1] = q_mvar[q0 + q] * inv;
+      }
+    });
   }
   s->n_inj = n_rows;
   s->rows_dirty = true;
@@ -925,6 +957,20 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   a.ws_stride = wsb;
   ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
   ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, prec, 1, s->stream), "base factor launch");
+  // its inverse, one column per row of an inverse-mode sweep over all CTAs
+  const int dim = s->dplan.dim;
+  const size_t elem = prec == GS2G_PREC_FP64 ? sizeof(double) : sizeof(float);
+  s->d_base_inv.ensure((size_t)dim * dim * elem);
+  int n_ctas = std::max(1, std::min(gs2g::sweep_ctas(prec, s->device), dim));
+  s->d_ws.ensure((size_t)wsb * n_ctas);
+  gs2g::SweepArgs ai = a;
+  ai.factor_only = 0;
+  ai.n_rows = dim;
+  ai.base_ws = s->d_base_ws.as<char>();
+  ai.inverse_out = s->d_base_inv.as<char>();
+  ai.workspace = s->d_ws.as<char>();
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck((cudaError_t)gs2g::launch_sweep(s->dplan, ai, prec, n_ctas, s->stream), "base inverse launch");
   ck(cudaStreamSynchronize(s->stream), "base factor");
   s->base_factor_prec = prec;
 }
@@ -1104,15 +1150,12 @@ namespace {
 // a pinned double buffer of the session: chunk i+1 is in flight while chunk
 // i is copied out on the host.
 void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes) {
-  constexpr size_t kChunk = size_t(8) << 20;
+  constexpr size_t kChunk = kStageChunk;
   if (bytes < 2 * kChunk) {
     ck(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "read results");
     return;
   }
-  if (!s->h_stage) {
-    ck(cudaMallocHost(&s->h_stage, 2 * kChunk), "pinned staging buffer");
-    for (cudaEvent_t& e : s->ev_stage) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-  }
+  ensure_stage(s);
   char* buf[2] = {static_cast<char*>(s->h_stage), static_cast<char*>(s->h_stage) + kChunk};
   const size_t nch = (bytes + kChunk - 1) / kChunk;
   auto issue = [&](size_t i) {
@@ -1192,6 +1235,20 @@ int gs2g_get_device_results(const gs2g_session* s, double** v, double** residual
   if (residuals) *residuals = s->d_res.as<double>();
   if (status) *status = s->d_status.as<int>();
   if (iters) *iters = s->d_iters.as<int>();
+  GS2G_CATCH
+}
+
+int gs2g_get_device_rows(gs2g_session* s, int* n_rows, const double** sbus_rows, const int** trip_ptr,
+                         const int** trip_ids, int64_t* n_trip_ids) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  DeviceGuard g(s->device);
+  assemble_rows(s);
+  if (n_rows) *n_rows = s->n_rows;
+  if (sbus_rows) *sbus_rows = s->rows_have_sbus ? s->d_sbus_rows.as<double>() : nullptr;
+  if (trip_ptr) *trip_ptr = s->rows_have_edits ? s->d_trip_ptr.as<int>() : nullptr;
+  if (trip_ids) *trip_ids = s->rows_have_edits ? s->d_trip_ids.as<int>() : nullptr;
+  if (n_trip_ids) *n_trip_ids = s->rows_have_edits ? (int64_t)s->ctg_ids.size() : 0;
   GS2G_CATCH
 }
 

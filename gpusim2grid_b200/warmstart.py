@@ -420,7 +420,7 @@ class LearnedStart:
         """Raw features (rows, n_in) fp32 on the device.  ``sbus_rows``:
         (rows, n_bus) complex per unit (device tensor or array; None: base
         injections).  ``trips``: list of tripped-branch lists or a CSR
-        (ptr, ids) pair (None: no trips)."""
+        (ptr, ids) pair of arrays or device tensors (None: no trips)."""
         if n_rows is None:
             n_rows = sbus_rows.shape[0] if sbus_rows is not None else (
                 len(trips[0]) - 1 if isinstance(trips, tuple) else len(trips))
@@ -433,9 +433,15 @@ class LearnedStart:
         if trips is not None:
             ptr, ids = trips if isinstance(trips, tuple) else _csr(trips)
             if len(ids):
-                rows = np.repeat(np.arange(n_rows, dtype=np.int64), np.diff(ptr))
-                r = torch.as_tensor(rows, device=self.device)
-                b = torch.as_tensor(np.asarray(ids, dtype=np.int64), device=self.device)
+                if isinstance(ptr, torch.Tensor):  # device CSR (e.g. a session's own row definitions)
+                    pt = ptr.to(device=self.device, dtype=torch.int64)
+                    r = torch.repeat_interleave(torch.arange(n_rows, device=self.device), pt[1:] - pt[:-1],
+                                                output_size=len(ids))
+                    b = ids.to(device=self.device, dtype=torch.int64)
+                else:
+                    rows = np.repeat(np.arange(n_rows, dtype=np.int64), np.diff(ptr))
+                    r = torch.as_tensor(rows, device=self.device)
+                    b = torch.as_tensor(np.asarray(ids, dtype=np.int64), device=self.device)
                 cols = self._br_cols.index_select(0, b)
                 vals = self._br_vals.index_select(0, b)
                 F.index_put_((r[:, None].expand(-1, 4), cols), vals, accumulate=True)

@@ -217,6 +217,14 @@ int gs2g_set_branch_limits(gs2g_session* s, int n_branch, const double* rate_mva
 int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violations, float* max_loading);
 /* Device pointers of the last run's results (valid until the next run or destroy). */
 int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
+/* Device copies of the current row definitions (uploaded first if they
+ * changed): sbus_rows [n_rows x n_bus] complex per unit (NULL: the rows use
+ * the base injections), trip_ptr [n_rows + 1] / trip_ids [n_trip_ids] CSR of
+ * tripped branches (NULL: no trips).  Valid until the rows change.  A
+ * device-resident caller (e.g. a learned start) reads them instead of
+ * shipping the rows again. */
+int gs2g_get_device_rows(gs2g_session* s, int* n_rows, const double** sbus_rows, const int** trip_ptr,
+                         const int** trip_ids, int64_t* n_trip_ids);
 int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
 /* Synchronise the session stream. */
 int gs2g_sync(gs2g_session* s);

@@ -46,3 +46,25 @@ def test_base_chord_injections(g118):
     np.testing.assert_array_equal(b.get_row_status(), a.get_row_status())
     ok = a.get_row_status() == RowStatus.CONVERGED
     assert np.abs(a.V_results[ok] - b.V_results[ok]).max() < TOL_V_MIXED
+
+
+def test_device_rows_match_host_definitions(g118):
+    """gs2g_get_device_rows hands out the session's device copies of the
+    rows: Sbus = (p + jq) / sn_mva (uploaded through the pinned staging
+    chunks, several of them at this size) and the trip CSR."""
+    import torch
+    from gpusim2grid_b200 import ScenarioSweepGPU
+    n = 2 * (8 << 20) // (16 * g118.n_bus) + 7  # more than two 8 MiB chunks of complex rows
+    p, q = injection_scenarios(g118, n, seed=3)
+    trips = [[int(b)] if r % 3 else [] for r, b in enumerate(np.resize(n1_branches(g118), n))]
+    sw = ScenarioSweepGPU(g118.as_tuple(), init_from_n_powerflow=False, precision="mixed", nb_iter=10,
+                          scheduling="continuous", tol=1e-8)
+    sw.set_branch_data(*g118.branch_data())
+    sw.set_injections(p, q, g118.sn_mva)
+    sw.set_topology(trips)
+    sbus, (ptr, ids), nr = sw._device_row_defs()
+    assert nr == n and sbus.shape == (n, g118.n_bus)
+    np.testing.assert_array_equal(sbus.cpu().numpy(), (p + 1j * q) / g118.sn_mva)
+    np.testing.assert_array_equal(ptr.cpu().numpy(), np.cumsum([0] + [len(t) for t in trips]))
+    np.testing.assert_array_equal(ids.cpu().numpy(), [b for t in trips for b in t])
+    assert isinstance(sbus, torch.Tensor) and sbus.is_cuda
