@@ -419,8 +419,6 @@ def run_ours(args):
                          [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
     n_ids = sum(len(r_) for r_ in trips) if trips is not None else 0
     h2d = (4 * (n + 1) + 4 * n_ids if trips is not None else 0) + (2 * p.nbytes if p is not None else 0)
-    if learned:
-        h2d += 16 * n_ids + (0 if p is None else n * g.n_bus * 16)
     d2h = V.nbytes + stt.nbytes + r.nbytes
 
     w = 4 if args.precision == "mixed" else 8
@@ -550,6 +548,7 @@ def run_ours_multi(args):
     start_mode = lib.START_ROWS if learned else lib.START_VINIT
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    sweeps = []
 
     def step():
         pre_ms = 0.0
@@ -562,10 +561,11 @@ def run_ours_multi(args):
             ev1.synchronize()
             pre_ms = ev0.elapsed_time(ev1)
         lib.run_multi(sessions, MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, False, strat, ratio, reuse, learned)
-        ms = sessions[0].timings()["kernel_ms"]
+        ms = sweep_ms = sessions[0].timings()["kernel_ms"]
         for f in facades:
             f._ran = True
             ms += f.fp64_fallback()
+        sweeps.append(sweep_ms)
         return pre_ms, ms
 
     for _ in range(args.warmup):
@@ -591,6 +591,17 @@ def run_ours_multi(args):
     iters = np.concatenate([r[3] for r in res])
     n_total = int(sum(n_rows))
     value = world * n_conv * args.steps / (total_ms / 1e3)
+    # roofline of the multi-grid sweep launch: each grid's algorithmic bytes
+    # per LU and per Newton step times its rows' counts in the last step
+    w = 4 if args.precision == "mixed" else 8
+    launch_bytes = 0
+    for s_, (g_, _, _, _), r_ in zip(sessions, parts, res):
+        b_fact, b_iter = algorithmic_bytes(s_.info(), w)
+        b_iter += 16 * g_.n_bus  # each step reads the row's Sbus
+        launch_bytes += b_fact * int(s_.factor_counts().sum()) + b_iter * int(r_[3].sum())
+    sweep_ms = float(np.mean(sweeps[-args.steps:]))
+    achieved_gbs = launch_bytes / (sweep_ms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
 
     def flat_arm(p_, strat_):
         lib.run_multi(sessions, MAX_ITER, TOL, False, p_, lib.START_VINIT, 0.0, 0, False, strat_)
@@ -628,8 +639,6 @@ def run_ours_multi(args):
     n_conv_e2e = sum(int((o[1] == 0).sum()) for o in outs)
     e2e_value = world * n_conv_e2e / float(np.mean(e2e_s))
     h2d = sum(2 * p.nbytes + 4 * (len(t) + 1) + 4 * sum(len(x) for x in t) for _, t, p, _ in parts)
-    if learned:
-        h2d += sum(p.shape[0] * g.n_bus * 16 + 16 * sum(len(x) for x in t) for g, t, p, _ in parts)
     d2h = sum(o[0].nbytes + o[1].nbytes + o[2].nbytes for o in outs)
 
     per_step_launches = 1 + (sum(ls.launches_per_call(n) for ls, n in zip(learners, n_rows)) if learned else 0)
@@ -653,6 +662,11 @@ def run_ours_multi(args):
         "agreement_with_fp64": {"max_abs_dv_pu": agree, "same_convergence_flags": same, "flag_differences": mism},
         "training": train,
         "plan_tails": [s.info()["tail_dim"] for s in sessions],
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_gbs / peak, 4), "traffic": None,
+                     "note": f"multi-grid sweep kernel ({round(sweep_ms, 3)} ms per launch); peak {peak_kind}; "
+                             f"algorithmic bytes per launch = sum over grids of bytes per LU x LUs + bytes per "
+                             f"Newton step x steps = {launch_bytes}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": args.steps * per_step_launches,

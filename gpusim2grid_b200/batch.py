@@ -17,8 +17,10 @@ default).  Rows start from the converged base case as the reference's batch
 sources do (``start='base'``), or from ``Vinit`` (``start='flat'``), or from
 per-row voltages (``set_start_voltages``), or from voltages a trained
 network predicts for each row (``set_learned_start``, ``start='learned'``;
-see ``warmstart.py``).  Rows given a start of their own that fail from it
-restart once from ``Vinit`` inside the same launch.
+see ``warmstart.py``).  A row given a start of their own begins from the
+base case instead when that has the smaller mismatch, and a row that fails
+from its start restarts once from the base case (``Vinit`` without one)
+inside the same launch.
 """
 
 from __future__ import annotations
@@ -194,7 +196,8 @@ class _BatchSweep:
     @property
     def warm_report(self):
         """Timings of the last learned start: predict_ms (features, network
-        and V0 on the device, wall), n_rescued (rows restarted from Vinit)."""
+        and V0 on the device, wall), n_rescued (rows restarted), n_base_start
+        (rows that began from the base case: its mismatch was the smaller)."""
         return dict(self._warm)
 
     @property
@@ -284,6 +287,7 @@ class _BatchSweep:
         tm = self._s.timings()
         if self._start == "learned":
             self._warm["n_rescued"] = int(tm["n_rescued"])
+            self._warm["n_base_start"] = int(tm["n_base_start"])
         kernel_ms = tm["kernel_ms"]
         kernel_ms += self.fp64_fallback(n_ctas)
         tm = dict(tm, kernel_ms=kernel_ms)

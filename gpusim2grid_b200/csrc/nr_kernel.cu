@@ -522,6 +522,26 @@ __device__ __forceinline__ void jac_entry(bool diag, double2 yk, double2 Vi, dou
   out[3] = dVm.y;
 }
 
+// ||F||inf of the row (row-patched Ybus, its Sbus) at voltage Vx, NaN-sticky,
+// without touching the row's workspace
+__device__ __noinline__ double mismatch_norm(const DevPlan P, const RowEdits ed, const double2* Y, const double2* Vx,
+                                             const double2* sb, double* s_red) {
+  double lmax = 0.0;
+  for (int i = threadIdx.x; i < P.n_bus; i += BS) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = P.y_indptr[i]; k < P.y_indptr[i + 1]; ++k) {
+      const double2 yk = ed.apply(k, Y[k]);
+      const double2 vj = Vx[P.y_indices[k]];
+      acc.x = fma(yk.x, vj.x, fma(-yk.y, vj.y, acc.x));
+      acc.y = fma(yk.x, vj.y, fma(yk.y, vj.x, acc.y));
+    }
+    const double2 s = csub(cmul(Vx[i], conj2(acc)), sb[i]);
+    if (P.fP[i] >= 0) lmax = (isnan(s.x) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.x));
+    if (P.fQ[i] >= 0) lmax = (isnan(s.y) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.y));
+  }
+  return block_nanmax(lmax, s_red);
+}
+
 // Outage compensation (policy 2, rows with Ybus edits).  The chord matrix of
 // a row is its Jacobian at the base voltage Vb, M = M0 + E B E^T, where M0 is
 // the base factor and B = Delta J is confined to the P/Q rows and theta/Vm
@@ -738,6 +758,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
 
     int it_total = 0, status = ROW_MAX_ITER, n_factor = 0;
     double nrm = NAN;
+    bool check_alt = a.alt_v0 != nullptr && !a.fixed_iters && !a.factor_only;
     // attempt 0 starts from the row's own start voltage; with a rescue
     // voltage, a row that ends unconverged there gets one more attempt from
     // it, with a fresh Newton budget (iterations and factorizations add up)
@@ -786,6 +807,19 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
         }
       }
       nrm = block_nanmax(lmax, s_red);
+      if (check_alt) {
+        // the row's own start stands only if its mismatch is below the
+        // alternative start's (a NaN start never stands)
+        check_alt = false;
+        const double2* va = reinterpret_cast<const double2*>(a.alt_v0);
+        const double na = mismatch_norm(P, ed, Y, va, sb, s_red);
+        if (!(nrm < na) && isfinite(na)) {
+          for (int i = tid; i < n; i += BS) V[i] = va[i];
+          if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
+          __syncthreads();
+          continue;  // mismatch again at the new start
+        }
+      }
       prof.mark(PH_MISMATCH);
       const bool finite = isfinite(nrm);
       if (a.factor_only) {

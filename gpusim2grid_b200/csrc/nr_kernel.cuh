@@ -75,6 +75,11 @@ struct SweepArgs {
   // the restarts (nullptr: not counted)
   const double* rescue_v0;
   int* n_rescued;
+  // start selection: a row whose first mismatch at its own start is not
+  // below the mismatch at this complex [n_bus] voltage (the base case) starts
+  // from it instead (nullptr: off); n_alt_start counts those rows
+  const double* alt_v0;
+  int* n_alt_start;
   // policy 2: workspace (ws_layout of this plan and precision) holding the
   // base case's factor, shared read-only by every CTA; factor_only: factor
   // the Jacobian at the start voltage into the CTA's workspace and stop

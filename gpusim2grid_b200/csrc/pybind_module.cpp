@@ -379,6 +379,7 @@ class Session {
     d["phase_cycles"] = pc;
     d["phase_share"] = ps;
     d["n_rescued"] = t.n_rescued;
+    d["n_base_start"] = t.n_base_start;
     return d;
   }
 

@@ -396,8 +396,13 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
   a.factors_out = out.factors;
+  // rescue (per-row starts, continuous schedule): with a base case the row
+  // starts from the base V when that has the smaller mismatch, and an
+  // unconverged row restarts from the base V (from Vinit without one)
   const bool rescue = o.rescue != 0 && v0_stride != 0 && !o.fixed_iters;
-  a.rescue_v0 = rescue ? s->d_vinit.as<double>() : nullptr;
+  const bool base = rescue && s->has_base && use_rows;
+  a.rescue_v0 = rescue ? (base ? s->d_basev.as<double>() : s->d_vinit.as<double>()) : nullptr;
+  a.alt_v0 = base ? s->d_basev.as<double>() : nullptr;
   a.phase_cycles = nullptr;
   if (use_rows && s->limits_on) {
     const size_t nr = (size_t)std::max(n_rows, 1);
@@ -425,17 +430,18 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
   s->d_ws.ensure((size_t)wsb * n_ctas);
-  s->d_queue.ensure(2 * sizeof(int));  // [0] row queue, [1] rescue count
+  s->d_queue.ensure(3 * sizeof(int));  // [0] row queue, [1] rescue count, [2] alternative starts
   a.queue = s->d_queue.as<int>();
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
   a.n_rescued = s->d_queue.as<int>() + 1;
+  a.n_alt_start = s->d_queue.as<int>() + 2;
   if (o.profile_phases) {
     s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
     ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
     a.phase_cycles = s->d_phase.as<unsigned long long>();
   }
-  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");
@@ -444,6 +450,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
   for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
   ck(cudaMemcpy(&s->tm.n_rescued, s->d_queue.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost), "rescue count");
+  ck(cudaMemcpy(&s->tm.n_base_start, s->d_queue.as<int>() + 2, sizeof(int), cudaMemcpyDeviceToHost), "start count");
   if (o.profile_phases) {
     unsigned long long c[gs2g::N_PHASES];
     ck(cudaMemcpy(c, s->d_phase.p, sizeof(c), cudaMemcpyDeviceToHost), "read phases");
@@ -951,11 +958,11 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   OutBufs ob{s->b_v.as<double>(), s->b_res.as<double>(), s->b_status.as<int>(), s->b_iters.as<int>()};
   gs2g::SweepArgs a = make_args(s, o, 1, s->d_basev.as<double>(), 0, s->d_sbus.as<double>(), 0, false, ob);
   a.factor_only = 1;
-  s->d_queue.ensure(2 * sizeof(int));
+  s->d_queue.ensure(3 * sizeof(int));
   a.queue = s->d_queue.as<int>();
   a.workspace = s->d_base_ws.as<char>();
   a.ws_stride = wsb;
-  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, prec, 1, s->stream), "base factor launch");
   // its inverse, one column per row of an inverse-mode sweep over all CTAs
   const int dim = s->dplan.dim;
@@ -969,7 +976,7 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   ai.base_ws = s->d_base_ws.as<char>();
   ai.inverse_out = s->d_base_inv.as<char>();
   ai.workspace = s->d_ws.as<char>();
-  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck((cudaError_t)gs2g::launch_sweep(s->dplan, ai, prec, n_ctas, s->stream), "base inverse launch");
   ck(cudaStreamSynchronize(s->stream), "base factor");
   s->base_factor_prec = prec;
@@ -1045,12 +1052,12 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   n_ctas = std::max(1, std::min(n_ctas, std::max(n_sub, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
   s->d_ws.ensure((size_t)wsb * n_ctas);
-  s->d_queue.ensure(2 * sizeof(int));
+  s->d_queue.ensure(3 * sizeof(int));
   a.queue = s->d_queue.as<int>();
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
   a.n_rescued = s->d_queue.as<int>() + 1;
-  ck(cudaMemsetAsync(s->d_queue.p, 0, 2 * sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_sub > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "subset launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");
@@ -1080,7 +1087,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   std::vector<gs2g::GridEntry> ge(n_sessions);
   std::vector<int> begin(n_sessions + 1, 0);
   int64_t wsb = 0;
-  s0->d_queue.ensure(2 * sizeof(int));
+  s0->d_queue.ensure(3 * sizeof(int));
   for (int i = 0; i < n_sessions; ++i) {
     gs2g_session* s = sessions[i];
     assemble_rows(s);
@@ -1088,6 +1095,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
     ge[i].P = s->dplan;
     ge[i].a = make_args(s, o, rp.nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
     ge[i].a.n_rescued = s0->d_queue.as<int>() + 1;
+    ge[i].a.n_alt_start = s0->d_queue.as<int>() + 2;
     begin[i + 1] = begin[i] + rp.nr;
     wsb = std::max(wsb, gs2g::workspace_bytes(s->dplan, o.precision));
   }
@@ -1107,7 +1115,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
     ck(cudaMemsetAsync(s0->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s0->stream), "phase reset");
     phase = s0->d_phase.as<unsigned long long>();
   }
-  ck(cudaMemsetAsync(s0->d_queue.p, 0, 2 * sizeof(int), s0->stream), "queue reset");
+  ck(cudaMemsetAsync(s0->d_queue.p, 0, 3 * sizeof(int), s0->stream), "queue reset");
   ck(cudaEventRecord(s0->ev0, s0->stream), "event");
   if (total > 0)
     ck((cudaError_t)gs2g::launch_sweep_multi(reinterpret_cast<const gs2g::GridEntry*>(s0->d_multi.p), n_sessions,
@@ -1118,8 +1126,8 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   ck(cudaStreamSynchronize(s0->stream), "multi-grid sweep");
   float ms = 0;
   ck(cudaEventElapsedTime(&ms, s0->ev0, s0->ev1), "event time");
-  int rescued = 0;
-  ck(cudaMemcpy(&rescued, s0->d_queue.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost), "rescue count");
+  int counts[2] = {0, 0};
+  ck(cudaMemcpy(counts, s0->d_queue.as<int>() + 1, sizeof(counts), cudaMemcpyDeviceToHost), "rescue count");
   for (int i = 0; i < n_sessions; ++i) {
     gs2g_session* s = sessions[i];
     s->last_rows_run = begin[i + 1] - begin[i];
@@ -1127,7 +1135,8 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
     s->tm.upload_ms = upload_ms;
     s->tm.total_ms = ms_since(t0);
     s->tm.total_iters = -1;
-    s->tm.n_rescued = i == 0 ? rescued : 0;
+    s->tm.n_rescued = i == 0 ? counts[0] : 0;
+    s->tm.n_base_start = i == 0 ? counts[1] : 0;
     for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
   }
   if (o.profile_phases) {

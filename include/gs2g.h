@@ -86,12 +86,14 @@ typedef struct gs2g_run_opts {
   int refactor_policy;
   double refactor_ratio; /* adaptive: <= 0 selects 0.3 */
   int max_reuse;         /* adaptive: <= 0 selects 3 */
-  /* 1: with GS2G_START_ROWS and the continuous schedule, a row that ends
-   * unconverged (MAX_ITER or DIVERGED) from its given start restarts once
-   * from Vinit inside the same launch, with a fresh max_iter budget and a
-   * new LU every step; its iteration and factorization counts include both
-   * attempts.  Guards a learned or otherwise predicted start against a bad
-   * prediction. */
+  /* 1: with GS2G_START_ROWS and the continuous schedule, guard each row's
+   * given start (a learned or otherwise predicted one) against a bad
+   * prediction.  With a base case, a row whose mismatch at its given start
+   * is not below its mismatch at the base V starts from the base V instead.
+   * A row that ends unconverged (MAX_ITER or DIVERGED) restarts once, inside
+   * the same launch, from the base V (from Vinit without a base case), with
+   * a fresh max_iter budget and a new LU every step; its iteration and
+   * factorization counts include both attempts. */
   int rescue;
 } gs2g_run_opts;
 
@@ -118,7 +120,8 @@ typedef struct gs2g_timings {
    * phase's share of their total */
   double phase_cycles[GS2G_N_PHASES];
   double phase_share[GS2G_N_PHASES];
-  int n_rescued; /* rows of the last run restarted from Vinit (gs2g_run_opts.rescue) */
+  int n_rescued;    /* rows of the last run restarted (gs2g_run_opts.rescue) */
+  int n_base_start; /* rows of the last run that began from the base V instead of their given start */
 } gs2g_timings;
 
 const char* gs2g_last_error(void);

@@ -78,22 +78,66 @@ def test_learned_start_injection_rows(g118, learned118):
     assert warm.get_row_iterations().sum() < flat.get_row_iterations().sum()
 
 
-def test_failed_start_rows_are_rescued_from_vinit(g118):
-    """Half the rows get a NaN start (their mismatch is NaN, so they end
-    DIVERGED at step 0); the kernel restarts exactly those from Vinit in the
-    same launch, and every row matches the flat-start run."""
+def test_failed_start_rows_are_rescued(g118):
+    """Half the rows get a NaN start, the others Vinit.  (1) With a (solved)
+    base case every row begins from the base V instead -- its mismatch is
+    below both -- and runs exactly as a base-start row.  (2) On a session
+    without a base case the NaN rows end DIVERGED at step 0 and restart from
+    Vinit in the same launch, matching the flat-start run."""
+    from gpusim2grid_b200._common import grid_arrays, make_session
+    from gpusim2grid_b200._native import lib
     p, q = injection_scenarios(g118, 64, seed=4)
-    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", start="flat")
-    flat = InjectionSweepGPU(g118.as_tuple(), **kw)
-    flat.set_injections(p, q, g118.sn_mva)
-    flat.compute()
-    sw = InjectionSweepGPU(g118.as_tuple(), **kw)
-    sw.set_injections(p, q, g118.sn_mva)
     V0 = np.tile(g118.vinit(), (64, 1))
     V0[::2] = np.nan
+    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous")
+    base = InjectionSweepGPU(g118.as_tuple(), start="base", **kw)
+    base.set_injections(p, q, g118.sn_mva)
+    base.compute()
+    sw = InjectionSweepGPU(g118.as_tuple(), start="flat", **kw)
+    sw.set_injections(p, q, g118.sn_mva)
     sw.set_start_voltages(V0)
     sw.compute()
-    assert sw.session.timings()["n_rescued"] == 32
+    t = sw.session.timings()
+    assert t["n_base_start"] == 64 and t["n_rescued"] == 0
     assert np.all(sw.get_row_status() == RowStatus.CONVERGED)
-    np.testing.assert_array_equal(sw.get_row_iterations(), flat.get_row_iterations())
-    assert np.abs(sw.V_results - flat.V_results).max() < TOL_V_MIXED
+    np.testing.assert_array_equal(sw.get_row_iterations(), base.get_row_iterations())
+    assert np.abs(sw.V_results - base.V_results).max() < TOL_V_MIXED
+
+    s = make_session(grid_arrays(g118.as_tuple()), None)
+    s.set_injections(p, q, g118.sn_mva)
+    s.run(10, 1e-8, False, lib.PREC_MIXED, lib.START_VINIT, 0.0, 0, False, lib.REFACTOR_EVERY, 0.3, 3, False)
+    Vf, _, stf, itf = s.results()
+    assert np.all(stf == RowStatus.CONVERGED)
+    s.set_start_rows(V0)
+    s.run(10, 1e-8, False, lib.PREC_MIXED, lib.START_ROWS, 0.0, 0, False, lib.REFACTOR_EVERY, 0.3, 3, True)
+    t = s.timings()
+    assert t["n_rescued"] == 32 and t["n_base_start"] == 0
+    V, _, st, it = s.results()
+    assert np.all(st == RowStatus.CONVERGED)
+    np.testing.assert_array_equal(it, itf)
+    assert np.abs(V - Vf).max() < TOL_V_MIXED
+
+
+def test_given_start_worse_than_base_begins_from_base(g118):
+    """With a base case, a row whose given start has a larger mismatch than
+    the base V begins from the base V (and then runs exactly as a base-start
+    row); a better given start stands."""
+    p, q = injection_scenarios(g118, 64, seed=6)
+    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous",
+              strategy="base_chord")
+    base = InjectionSweepGPU(g118.as_tuple(), start="base", **kw)
+    base.set_injections(p, q, g118.sn_mva)
+    base.compute()
+    assert np.all(base.get_row_status() == RowStatus.CONVERGED)
+    sw = InjectionSweepGPU(g118.as_tuple(), start="flat", **kw)
+    sw.set_injections(p, q, g118.sn_mva)
+    V0 = base.V_results.copy()       # the solutions themselves: better than the base V
+    V0[::2] = 0.7 * g118.vinit()     # far worse than the base V
+    sw.set_start_voltages(V0)
+    sw.compute()
+    t = sw.session.timings()
+    assert t["n_base_start"] == 32 and t["n_rescued"] == 0
+    assert np.all(sw.get_row_status() == RowStatus.CONVERGED)
+    np.testing.assert_array_equal(sw.get_row_iterations()[::2], base.get_row_iterations()[::2])
+    assert np.all(sw.get_row_iterations()[1::2] <= 1)
+    assert np.abs(sw.V_results - base.V_results).max() < TOL_V_MIXED
