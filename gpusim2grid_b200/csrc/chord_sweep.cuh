@@ -1,0 +1,457 @@
+// Chord sweep: several rows per CTA stepping in lockstep on the shared base
+// factor (refactor policy 2, continuous schedule).
+//
+// Under policy 2 most Newton steps of most rows apply the same factor -- the
+// base case's Jacobian, shared read-only by every CTA and resident in L2 --
+// so a step is bound by the latency and the L2 bandwidth of streaming that
+// factor, not by arithmetic.  Here each CTA holds CK rows ("slots") and every
+// read of a factor entry or index serves all of them: the right-hand sides
+// are stored interleaved (CK values per unknown, one vector load), the head
+// levels and the tail rows are swept once for all slots, and the dense tail
+// is one product of the tail block of the base inverse (the inverse of the
+// dense Schur complement) with CK columns.  Every barrier is shared by the
+// slots as well.
+//
+// A slot leaves the chord kernel when its row converges (outputs written
+// here, branch flows included) or when the row needs more than the base
+// factor can give: the step stopped contracting (ratio test or max_reuse),
+// the mismatch is not finite, or the iteration budget is spent while a rescue
+// voltage is set.  Those rows are handed off -- current V in v_out, steps so
+// far in iters_out, row id in a device list -- to the single-row sweep
+// kernel, which continues them with their own factor (policy 1) and, where
+// needed, the rescue attempt.  The decisions are the single-row kernel's:
+// the same ratio test, the same counters, the same statuses.
+//
+// Included by nr_kernel.cu inside its anonymous namespace (it uses that
+// file's helpers).
+
+constexpr int CK = 4;  // rows per CTA
+
+template <typename T>
+struct alignas(4 * sizeof(T)) Vec4 {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ void fms4(Vec4<T>& acc, T a, const Vec4<T>& b) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
+}
+
+// Workspace of one chord CTA: V [n] and F [dim] per slot, then the
+// interleaved right-hand sides y [dim] x CK.
+struct ChordWs {
+  int64_t V, F, y, total;
+};
+
+template <typename T>
+__host__ __device__ ChordWs chord_ws(const DevPlan& P) {
+  ChordWs w;
+  int64_t o = 0;
+  w.V = o; o = align256(o + (int64_t)CK * P.n_bus * 16);
+  w.F = o; o = align256(o + (int64_t)CK * P.dim * 8);
+  w.y = o; o = align256(o + (int64_t)P.dim * sizeof(Vec4<T>));
+  w.total = o;
+  return w;
+}
+
+// Per-slot state, in shared memory; written by thread 0 between barriers.
+struct ChordSlot {
+  int row;    // session row, -1: empty
+  int it;     // Newton steps taken
+  int since;  // steps on the factor since the last (here: base) factorization
+  int fresh;  // first mismatch still to be compared with the alternative start
+  int comp;   // outage compensation set up
+  int act;    // this round: 1 solve, 2 converged, 3 diverged, 4 budget spent, 5 hand off
+  double nrm, last;
+};
+
+// NaN-sticky block max of four values at once (one pair of barriers).
+__device__ __forceinline__ void block_nanmax4(double v[4], double* s_red4) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_xor_sync(0xffffffffu, v[s], o);
+      v[s] = (isnan(w) || isnan(v[s])) ? NAN : fmax(v[s], w);
+    }
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) s_red4[warp * 4 + s] = v[s];
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double r = s_red4[s];
+    for (int w = 1; w < NWARP; ++w) {
+      const double x = s_red4[w * 4 + s];
+      r = (isnan(x) || isnan(r)) ? NAN : fmax(r, x);
+    }
+    v[s] = r;
+  }
+  __syncthreads();
+}
+
+// F and ||F||inf of the slots in `mask` (bit s: slot s): one sweep over the
+// Ybus rows, each entry read once for all slots.  Row edits are applied as
+// corrections on the buses of the edited Ybus rows (edits subtract ev[e]
+// from Y at entry ek[e]).
+__device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, const unsigned mask,
+                                            const ChordSlot* sl, const int* s_ne, const int (*s_ek)[MAX_EDITS],
+                                            const double2 (*s_ev)[MAX_EDITS], const double2* Vs, double* Fs,
+                                            double* nrm_out, double* s_red4) {
+  const int n = P.n_bus;
+  const double2* Y = reinterpret_cast<const double2*>(a.ybus);
+  const double2* sb[CK];
+#pragma unroll
+  for (int s = 0; s < CK; ++s)
+    sb[s] = reinterpret_cast<const double2*>(a.sbus) + (int64_t)(sl[s].row < 0 ? 0 : sl[s].row) * a.sbus_stride;
+  double lmax[CK] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += BS) {
+    double2 acc[CK];
+#pragma unroll
+    for (int s = 0; s < CK; ++s) acc[s] = make_double2(0.0, 0.0);
+    for (int k = P.y_indptr[i]; k < P.y_indptr[i + 1]; ++k) {
+      const double2 yk = Y[k];
+      const int j = P.y_indices[k];
+#pragma unroll
+      for (int s = 0; s < CK; ++s) {
+        if (!(mask >> s & 1)) continue;
+        const double2 vj = Vs[(int64_t)s * n + j];
+        acc[s].x = fma(yk.x, vj.x, fma(-yk.y, vj.y, acc[s].x));
+        acc[s].y = fma(yk.x, vj.y, fma(yk.y, vj.x, acc[s].y));
+      }
+    }
+    const int fp = P.fP[i], fq = P.fQ[i];
+#pragma unroll
+    for (int s = 0; s < CK; ++s) {
+      if (!(mask >> s & 1)) continue;
+      const double2* V = Vs + (int64_t)s * n;
+      for (int e = 0; e < s_ne[s]; ++e) {
+        const int k = s_ek[s][e];
+        if (P.y_row[k] != i) continue;
+        const double2 vj = V[P.y_indices[k]];
+        acc[s] = csub(acc[s], cmul(s_ev[s][e], vj));
+      }
+      const double2 sv = csub(cmul(V[i], conj2(acc[s])), sb[s][i]);
+      double* F = Fs + (int64_t)s * P.dim;
+      if (fp >= 0) {
+        F[fp] = -sv.x;
+        lmax[s] = (isnan(sv.x) || isnan(lmax[s])) ? NAN : fmax(lmax[s], fabs(sv.x));
+      }
+      if (fq >= 0) {
+        F[fq] = -sv.y;
+        lmax[s] = (isnan(sv.y) || isnan(lmax[s])) ? NAN : fmax(lmax[s], fabs(sv.y));
+      }
+    }
+  }
+  block_nanmax4(lmax, s_red4);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int s = 0; s < CK; ++s)
+      if (mask >> s & 1) nrm_out[s] = lmax[s];
+  __syncthreads();
+}
+
+// Forward over the head levels, all slots at once.
+template <typename T>
+__device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+  for (int lv = 0; lv < P.n_levels; ++lv) {
+    for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+      const int i = P.lev_piv[q0];
+      Vec4<T> acc = y[i];
+      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms4(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+      y[i] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// The tail rows against the head.
+template <typename T>
+__device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+  for (int ti = threadIdx.x; ti < P.nt; ti += BS) {
+    const int i = P.p + ti;
+    Vec4<T> acc = y[i];
+    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms4(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+    y[i] = acc;
+  }
+  __syncthreads();
+}
+
+// y_t <- Sinv y_t for all slots: the tail block of the base inverse (column j
+// at Minv + (p + j) * dim + p) times the CK columns held in shared memory.
+// Each thread owns up to four tail rows per pass; for each column a warp
+// reads 32 consecutive entries.
+template <typename T>
+__device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ Minv, Vec4<T>* y, Vec4<T>* ys) {
+  const int tid = threadIdx.x, nt = P.nt;
+  for (int i = tid; i < nt; i += BS) ys[i] = y[P.p + i];
+  __syncthreads();
+  const T* Sinv = Minv + (int64_t)P.p * P.dim + P.p;
+  for (int r0 = 0; r0 < nt; r0 += 4 * BS) {
+    Vec4<T> acc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc[u].v[s] = T(0);
+    const int nr = min(4, (nt - r0 - tid + BS - 1) / BS);  // rows of this thread in the pass (may be <= 0)
+    const T* base = Sinv + r0 + tid;
+#pragma unroll 2
+    for (int j = 0; j < nt; ++j) {
+      const Vec4<T> yj = ys[j];
+      const T* col = base + (int64_t)j * P.dim;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (u < nr) fms4(acc[u], -col[u * BS], yj);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u < nr) y[P.p + r0 + tid + u * BS] = acc[u];
+  }
+  __syncthreads();
+}
+
+// Backward over the head levels.
+template <typename T>
+__device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+  for (int lv = P.n_levels - 1; lv >= 0; --lv) {
+    for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
+      const int k = P.lev_piv[q0];
+      Vec4<T> acc = y[k];
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms4(acc, fHV[P.bw_pos[q]], y[P.bw_row[q]]);
+      const T d = fHV[k];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc.v[s] = acc.v[s] / d;
+      y[k] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Outputs of a slot's row as it leaves: V, and either the final status
+// (flows included) or the hand-off to the single-row kernel.
+__device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, const double2* V, const int n,
+                                         double* s_red) {
+  const int tid = threadIdx.x;
+  const int row = sl.row;
+  double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
+  for (int i = tid; i < n; i += BS) vout[i] = V[i];
+  if (sl.act == 5) {
+    if (tid == 0) {
+      a.iters_out[row] = sl.it;
+      a.handoff[atomicAdd(a.n_handoff, 1)] = row;
+    }
+    __syncthreads();
+    return;
+  }
+  const int status = sl.act == 2 ? ROW_CONVERGED : (sl.act == 3 ? ROW_DIVERGED : ROW_MAX_ITER);
+  if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
+  if (tid == 0) {
+    a.res_out[row] = sl.nrm;
+    a.status_out[row] = status;
+    a.iters_out[row] = sl.it;
+    if (a.factors_out != nullptr) a.factors_out[row] = 0;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const SweepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ ChordSlot sl[CK];
+  __shared__ int s_pull, s_more;
+  __shared__ int s_ne[CK];
+  __shared__ int s_ek[CK][MAX_EDITS];
+  __shared__ double2 s_ev[CK][MAX_EDITS];
+  __shared__ double s_red[NWARP];
+  __shared__ double s_red4[NWARP * 4];
+  __shared__ double s_nrm[CK];
+  __shared__ int s_cr[CK][1 + MAX_COMP];
+  __shared__ double s_cB[CK][MAX_COMP * MAX_COMP];
+  __shared__ double s_cLU[CK][MAX_COMP * MAX_COMP];
+  __shared__ int s_cpiv[CK][MAX_COMP];
+  __shared__ double s_cw[CK][MAX_COMP];
+  const int tid = threadIdx.x;
+  const int n = P.n_bus;
+  const ChordWs L = chord_ws<T>(P);
+  char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
+  double2* Vs = reinterpret_cast<double2*>(ws + L.V);
+  double* Fs = reinterpret_cast<double*>(ws + L.F);
+  Vec4<T>* y = reinterpret_cast<Vec4<T>*>(ws + L.y);
+  Vec4<T>* ys = reinterpret_cast<Vec4<T>*>(smem_raw);
+  const WsLayout BL = ws_layout<T>(P);  // layout of the base factor's workspace
+  const T* fHV = reinterpret_cast<const T*>(a.base_ws + BL.HV);
+  const T* Minv = reinterpret_cast<const T*>(a.base_inv);
+  const double2* Y = reinterpret_cast<const double2*>(a.ybus);
+  const double2* Vbase = reinterpret_cast<const double2*>(a.base_v);
+  auto shs = [&](int s) {
+    return RowShared<T>{&s_ne[s], s_ek[s], s_ev[s], s_red, nullptr, nullptr, s_cr[s], s_cB[s], s_cLU[s], s_cpiv[s],
+                        s_cw[s]};
+  };
+  PhaseProf prof;
+  prof.init(a.phase_cycles != nullptr && tid == 0);
+  if (tid == 0) {
+    for (int s = 0; s < CK; ++s) sl[s].row = -1;
+    s_more = 1;
+  }
+  __syncthreads();
+  for (;;) {
+    // ---- refill empty slots from the row queue ----------------------------
+    for (int s = 0; s < CK; ++s) {
+      if (sl[s].row >= 0) continue;
+      for (;;) {
+        // every thread reads the flag before thread 0 may pull (and clear it)
+        const int more = s_more;
+        __syncthreads();
+        if (!more) break;
+        if (tid == 0) {
+          const int q = atomicAdd(a.queue, 1);
+          s_pull = q < a.n_rows ? (a.row_map != nullptr ? a.row_map[q] : q) : -1;
+          if (q >= a.n_rows) s_more = 0;
+        }
+        __syncthreads();
+        const int row = s_pull;
+        if (row < 0) break;
+        if (a.row_skip != nullptr && a.row_skip[row]) {
+          skip_row_outputs(a, row, n);
+          continue;
+        }
+        if (tid == 0) {
+          int ne = 0;
+          if (a.edit_ptr != nullptr) {
+            const int e0 = a.edit_ptr[row], e1 = a.edit_ptr[row + 1];
+            ne = min(e1 - e0, MAX_EDITS);
+            for (int e = 0; e < ne; ++e) {
+              s_ek[s][e] = a.edit_k[e0 + e];
+              s_ev[s][e] = reinterpret_cast<const double2*>(a.edit_val)[e0 + e];
+            }
+          }
+          s_ne[s] = ne;
+          sl[s].row = row;
+          sl[s].it = 0;
+          sl[s].since = 0;
+          sl[s].fresh = a.alt_v0 != nullptr;
+          sl[s].comp = 0;
+          sl[s].act = 0;
+          sl[s].last = INFINITY;
+        }
+        const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
+        for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = v0[i];
+        __syncthreads();
+        const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
+        bool c = false;
+        if (ed.n > 0 && Minv != nullptr && Vbase != nullptr) c = setup_compensation<T>(P, ed, Y, Vbase, Minv, shs(s));
+        if (tid == 0) sl[s].comp = c;
+        __syncthreads();
+        break;
+      }
+    }
+    unsigned active = 0;
+    for (int s = 0; s < CK; ++s) active |= (sl[s].row >= 0 ? 1u : 0u) << s;
+    if (active == 0) break;
+
+    // ---- mismatch of every slot, start selection for new rows --------------
+    chord_mismatch(P, a, active, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red4);
+    for (int s = 0; s < CK; ++s) {
+      if (!(active >> s & 1) || !sl[s].fresh) continue;
+      const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
+      const double2* va = reinterpret_cast<const double2*>(a.alt_v0);
+      const double2* sb = reinterpret_cast<const double2*>(a.sbus) + (int64_t)sl[s].row * a.sbus_stride;
+      const double na = a.alt_s != nullptr
+                            ? alt_mismatch_norm(P, ed, va, reinterpret_cast<const double2*>(a.alt_s), sb, s_red)
+                            : mismatch_norm(P, ed, Y, va, sb, s_red);
+      const bool sw = !(s_nrm[s] < na) && isfinite(na);
+      __syncthreads();
+      if (tid == 0) sl[s].fresh = 0;
+      if (sw) {
+        for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = va[i];
+        if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
+        __syncthreads();
+        chord_mismatch(P, a, 1u << s, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red4);
+      }
+    }
+    prof.mark(PH_MISMATCH);
+
+    // ---- per-slot decisions (the single-row kernel's, in its order) ---------
+    if (tid == 0) {
+      const bool rescue = a.rescue_v0 != nullptr;
+      for (int s = 0; s < CK; ++s) {
+        if (!(active >> s & 1)) continue;
+        ChordSlot& q = sl[s];
+        q.nrm = s_nrm[s];
+        if (!isfinite(q.nrm)) q.act = rescue ? 5 : 3;
+        else if (q.nrm < a.tol) q.act = 2;
+        else if (q.it >= a.max_iter) q.act = rescue ? 5 : 4;
+        else if (!(q.nrm <= a.refactor_ratio * q.last) || q.since >= a.max_reuse) q.act = 5;  // needs its own LU
+        else q.act = 1;
+      }
+    }
+    __syncthreads();
+    unsigned solve = 0;
+    for (int s = 0; s < CK; ++s) {
+      if (!(active >> s & 1)) continue;
+      if (sl[s].act == 1) {
+        solve |= 1u << s;
+        continue;
+      }
+      chord_leave(a, sl[s], Vs + (int64_t)s * n, n, s_red);
+      if (tid == 0) sl[s].row = -1;
+      __syncthreads();
+    }
+    if (solve == 0) continue;
+
+    // ---- one solve on the base factor for every remaining slot -------------
+    for (int i = tid; i < P.dim; i += BS) {
+      Vec4<T> r;
+#pragma unroll
+      for (int s = 0; s < CK; ++s) r.v[s] = (solve >> s & 1) ? (T)Fs[(int64_t)s * P.dim + i] : T(0);
+      y[i] = r;
+    }
+    __syncthreads();
+    chord_head_fw<T>(P, fHV, y);
+    prof.mark(PH_SOLVE);
+    chord_tail_fw<T>(P, fHV, y);
+    prof.mark(PH_SOLVE_TAIL);
+    if (P.nt > 0) chord_dense<T>(P, Minv, y, ys);
+    prof.mark(PH_SOLVE_DENSE);
+    chord_head_bw<T>(P, fHV, y);
+    for (int s = 0; s < CK; ++s)
+      if ((solve >> s & 1) && sl[s].comp) apply_compensation<T>(P.dim, &y[0].v[s], Minv, shs(s), CK);
+    prof.mark(PH_SOLVE_BACK);
+
+    // ---- V update (FP64, polar) ---------------------------------------------
+    for (int i = tid; i < n; i += BS) {
+      const int fp = P.fP[i], fq = P.fQ[i];
+      if (fp < 0 && fq < 0) continue;
+      const Vec4<T> ya = fp >= 0 ? y[fp] : Vec4<T>{};
+      const Vec4<T> ym = fq >= 0 ? y[fq] : Vec4<T>{};
+#pragma unroll
+      for (int s = 0; s < CK; ++s) {
+        if (!(solve >> s & 1)) continue;
+        double2* V = Vs + (int64_t)s * n;
+        const double2 v = V[i];
+        const double vm = hypot(v.x, v.y) + (fq >= 0 ? (double)ym.v[s] : 0.0);
+        const double va = atan2(v.y, v.x) + (fp >= 0 ? (double)ya.v[s] : 0.0);
+        double sn, cs;
+        sincos(va, &sn, &cs);
+        V[i] = make_double2(vm * cs, vm * sn);
+      }
+    }
+    if (tid == 0)
+      for (int s = 0; s < CK; ++s)
+        if (solve >> s & 1) {
+          sl[s].last = sl[s].nrm;
+          ++sl[s].since;
+          ++sl[s].it;
+        }
+    __syncthreads();
+    prof.mark(PH_UPDATE);
+  }
+  prof.flush(a.phase_cycles);
+}
+
+template <typename T>
+int chord_smem_bytes(const DevPlan& P) {
+  return (int)(sizeof(Vec4<T>) * (size_t)(P.nt > 0 ? P.nt : 1));
+}

@@ -434,12 +434,41 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
   return w;
 }
 
+// y_t <- Sinv y_t with an explicit inverse of the dense tail, column j at
+// Sinv + j * ld (nt rows): one parallel product instead of the serial block
+// chain of the triangular solves.  ys holds the input copy of y_t (shared
+// memory); each thread owns up to four rows per pass, and for each column a
+// warp reads 32 consecutive entries.
+template <typename T>
+__device__ __forceinline__ void tail_inverse_product(const T* Sinv, int64_t ld, int nt, const T* ys, T* yt) {
+  const int tid = threadIdx.x;
+  for (int r0 = 0; r0 < nt; r0 += 4 * BS) {
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    const T* base = Sinv + r0 + tid;
+    const int nr = min(4, (nt - r0 - tid + BS - 1) / BS);  // rows of this thread in the pass (may be <= 0)
+#pragma unroll 4
+    for (int j = 0; j < nt; ++j) {
+      const T yj = ys[j];
+      const T* col = base + (int64_t)j * ld;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (u < nr) acc[u] = fma(col[u * BS], yj, acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u < nr) yt[r0 + tid + u * BS] = acc[u];
+  }
+}
+
 // y <- (LU)^-1 y with a factor (head values fHV, dense tail fS): forward
 // over the head levels, the tail rows against the head, the dense tail
-// forward + backward, backward over the head levels.
+// forward + backward, backward over the head levels.  With Minv (the
+// factor's explicit inverse, column c at Minv + c * dim, in the plan's
+// ordering) the dense tail is applied as a product with its tail block,
+// which is the inverse of the dense Schur complement.
 template <typename T>
 __device__ __forceinline__ void apply_factor(const DevPlan& P, const T* fHV, const T* fS, T* y, T* s_blk, T* s_dense,
-                                             PhaseProf& prof) {
+                                             PhaseProf& prof, const T* Minv = nullptr) {
   const int tid = threadIdx.x;
   for (int lv = 0; lv < P.n_levels; ++lv) {
     for (int q0 = P.lev_piv_ptr[lv] + tid; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
@@ -459,7 +488,12 @@ __device__ __forceinline__ void apply_factor(const DevPlan& P, const T* fHV, con
   }
   __syncthreads();
   prof.mark(PH_SOLVE_TAIL);
-  if (P.nt > 0)
+  if (P.nt > 0 && Minv != nullptr && P.nt <= dense_smem_elems<T>()) {
+    for (int i = tid; i < P.nt; i += BS) s_dense[i] = y[P.p + i];
+    __syncthreads();
+    tail_inverse_product<T>(Minv + (int64_t)P.p * P.dim + P.p, P.dim, P.nt, s_dense, y + P.p);
+    __syncthreads();
+  } else if (P.nt > 0)
   {
     // y tail in shared memory when it fits, the diagonal-block buffer after it
     const bool y_in_smem = P.nt + 32 * stage_stride<T>() + 32 <= dense_smem_elems<T>();
@@ -536,6 +570,27 @@ __device__ __noinline__ double mismatch_norm(const DevPlan P, const RowEdits ed,
       acc.y = fma(yk.x, vj.y, fma(yk.y, vj.x, acc.y));
     }
     const double2 s = csub(cmul(Vx[i], conj2(acc)), sb[i]);
+    if (P.fP[i] >= 0) lmax = (isnan(s.x) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.x));
+    if (P.fQ[i] >= 0) lmax = (isnan(s.y) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.y));
+  }
+  return block_nanmax(lmax, s_red);
+}
+
+// The same norm at the alternative start Va without a sparse product: Sa =
+// Va conj(Y Va) on the unedited Ybus is shared by all rows, and a row's
+// edits change S only at the buses of the edited Ybus rows, by
+// Va_i conj(dY_k Va_j) per edited entry k = (i, j).
+__device__ __noinline__ double alt_mismatch_norm(const DevPlan P, const RowEdits ed, const double2* Va,
+                                                 const double2* Sa, const double2* sb, double* s_red) {
+  double lmax = 0.0;
+  for (int i = threadIdx.x; i < P.n_bus; i += BS) {
+    double2 s = csub(Sa[i], sb[i]);
+    for (int e = 0; e < ed.n; ++e) {
+      const int k = ed.k[e];
+      if (P.y_row[k] != i) continue;
+      // edits subtract ed.v[e] from Y_k
+      s = csub(s, cmul(Va[i], conj2(cmul(ed.v[e], Va[P.y_indices[k]]))));
+    }
     if (P.fP[i] >= 0) lmax = (isnan(s.x) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.x));
     if (P.fQ[i] >= 0) lmax = (isnan(s.y) || isnan(lmax)) ? NAN : fmax(lmax, fabs(s.y));
   }
@@ -647,13 +702,14 @@ __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits 
 
 // y <- y - Z B (I + W B)^-1 y[R]  (see setup_compensation)
 template <typename T>
-__device__ __noinline__ void apply_compensation(int dim, T* y, const T* Minv, const RowShared<T> sh) {
+__device__ __noinline__ void apply_compensation(int dim, T* y, const T* Minv, const RowShared<T> sh,
+                                                const int stride = 1) {
   const int tid = threadIdx.x;
   const int r = sh.s_cr[0];
   const int* R = sh.s_cr + 1;
   if (tid == 0) {
     double v[MAX_COMP];
-    for (int q = 0; q < r; ++q) v[q] = (double)y[R[q]];
+    for (int q = 0; q < r; ++q) v[q] = (double)y[(int64_t)R[q] * stride];
     const double* C = sh.s_cLU;
     for (int k = 0; k < r; ++k) {  // P v, then L, then U
       const int pk = sh.s_cpiv[k];
@@ -679,7 +735,67 @@ __device__ __noinline__ void apply_compensation(int dim, T* y, const T* Minv, co
   for (int i = tid; i < dim; i += BS) {
     T acc = T(0);
     for (int c = 0; c < r; ++c) acc += Minv[(int64_t)R[c] * dim + i] * (T)sh.s_cw[c];
-    y[i] -= acc;
+    y[(int64_t)i * stride] -= acc;
+  }
+  __syncthreads();
+}
+
+// Branch flows and the limit check of one row as it leaves, by the row's
+// own CTA on the V it still holds (the reference's compute_branch_flows +
+// check_limit_violations passes): per branch loading = max(|S_from|, |S_to|)
+// / rate (0 for tripped or unlimited branches, NaN when not converged), the
+// number of branches above 1 and the largest loading.
+__device__ __noinline__ void row_flows(const SweepArgs a, const int row, const double2* V, const bool ok,
+                                       double* s_red) {
+  const int tid = threadIdx.x;
+  const int q0 = a.trip_ptr != nullptr ? a.trip_ptr[row] : 0;
+  const int q1 = a.trip_ptr != nullptr ? a.trip_ptr[row + 1] : 0;
+  double lmax = 0.0;
+  int nv = 0;
+  for (int l = tid; l < a.n_branch; l += BS) {
+    float ld = NAN;
+    if (ok) {
+      bool tripped = false;
+      for (int q = q0; q < q1; ++q) tripped |= a.trip_ids[q] == l;
+      ld = 0.f;
+      if (!tripped && a.br_rate[l] > 0.0) {
+        const double2* yb = reinterpret_cast<const double2*>(a.br_y) + 4 * (int64_t)l;
+        const double2 Vf = V[a.br_from[l]], Vt = V[a.br_to[l]];
+        const double2 Sf = cmul(Vf, conj2(cadd(cmul(yb[0], Vf), cmul(yb[1], Vt))));
+        const double2 St = cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt))));
+        const double r = fmax(hypot(Sf.x, Sf.y), hypot(St.x, St.y)) / a.br_rate[l];
+        ld = (float)r;
+        lmax = fmax(lmax, r);
+        nv += r > 1.0;
+      }
+    }
+    a.loading_out[(int64_t)row * a.n_branch + l] = ld;
+  }
+  lmax = block_nanmax(lmax, s_red);
+  const double nv_all = block_sum(double(nv), s_red);
+  if (tid == 0) {
+    a.nviol_out[row] = ok ? (int)nv_all : -1;
+    a.maxload_out[row] = ok ? (float)lmax : NAN;
+  }
+}
+
+// Outputs of a row that is not simulated (its outage islands the grid).
+__device__ __noinline__ void skip_row_outputs(const SweepArgs a, const int row, const int n) {
+  const int tid = threadIdx.x;
+  double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
+  for (int i = tid; i < n; i += BS) vout[i] = make_double2(NAN, NAN);
+  if (a.loading_out != nullptr) {
+    for (int l = tid; l < a.n_branch; l += BS) a.loading_out[(int64_t)row * a.n_branch + l] = NAN;
+    if (tid == 0) {
+      a.nviol_out[row] = -1;
+      a.maxload_out[row] = NAN;
+    }
+  }
+  if (tid == 0) {
+    a.res_out[row] = NAN;
+    a.status_out[row] = ROW_NOT_SIMULATED;
+    a.iters_out[row] = 0;
+    if (a.factors_out != nullptr) a.factors_out[row] = 0;
   }
   __syncthreads();
 }
@@ -721,20 +837,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
 
     if (a.row_skip != nullptr && a.row_skip[row]) {
-      for (int i = tid; i < n; i += BS) vout[i] = make_double2(NAN, NAN);
-      if (a.loading_out != nullptr) {
-        for (int l = tid; l < a.n_branch; l += BS) a.loading_out[(int64_t)row * a.n_branch + l] = NAN;
-        if (tid == 0) {
-          a.nviol_out[row] = -1;
-          a.maxload_out[row] = NAN;
-        }
-      }
-      if (tid == 0) {
-        a.res_out[row] = NAN;
-        a.status_out[row] = ROW_NOT_SIMULATED;
-        a.iters_out[row] = 0;
-      }
-      __syncthreads();
+      skip_row_outputs(a, row, n);
       return;
     }
     if (tid == 0) {
@@ -763,7 +866,8 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     // voltage, a row that ends unconverged there gets one more attempt from
     // it, with a fresh Newton budget (iterations and factorizations add up)
     for (int attempt = 0;; ++attempt) {
-    int it = 0;
+    // a row continued from another launch keeps counting its Newton steps
+    int it = (attempt == 0 && a.iters_in != nullptr) ? a.iters_in[row] : 0;
     // policy 2 starts on the base case's factor (shared by every CTA, read
     // only) and moves to the row's own factor at its first refactor
     const bool on_base = a.refactor_policy == 2 && a.base_ws != nullptr && attempt == 0 && !a.factor_only;
@@ -812,7 +916,9 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
         // alternative start's (a NaN start never stands)
         check_alt = false;
         const double2* va = reinterpret_cast<const double2*>(a.alt_v0);
-        const double na = mismatch_norm(P, ed, Y, va, sb, s_red);
+        const double na = a.alt_s != nullptr
+                              ? alt_mismatch_norm(P, ed, va, reinterpret_cast<const double2*>(a.alt_s), sb, s_red)
+                              : mismatch_norm(P, ed, Y, va, sb, s_red);
         if (!(nrm < na) && isfinite(na)) {
           for (int i = tid; i < n; i += BS) V[i] = va[i];
           if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
@@ -941,7 +1047,8 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // ---- solves -----------------------------------------------------------
       for (int i = tid; i < P.dim; i += BS) y[i] = (T)F[i];
       __syncthreads();
-      apply_factor<T>(P, fHV, fS, y, s_blk, s_dense, prof);
+      // rows still on the base factor apply its dense tail through the base inverse
+      apply_factor<T>(P, fHV, fS, y, s_blk, s_dense, prof, fHV != HV ? Minv : nullptr);
       if (comp_on) apply_compensation<T>(P.dim, y, Minv, sh);
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
@@ -970,40 +1077,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     }  // attempts
 
     // ---- branch flows and limit check as the row leaves --------------------
-    // (the reference's compute_branch_flows + check_limit_violations passes,
-    // done by the row's own CTA on the V it still holds)
-    if (a.loading_out != nullptr) {
-      const bool ok = status == ROW_CONVERGED;
-      const int q0 = a.trip_ptr != nullptr ? a.trip_ptr[row] : 0;
-      const int q1 = a.trip_ptr != nullptr ? a.trip_ptr[row + 1] : 0;
-      double lmax = 0.0;
-      int nv = 0;
-      for (int l = tid; l < a.n_branch; l += BS) {
-        float ld = NAN;
-        if (ok) {
-          bool tripped = false;
-          for (int q = q0; q < q1; ++q) tripped |= a.trip_ids[q] == l;
-          ld = 0.f;
-          if (!tripped && a.br_rate[l] > 0.0) {
-            const double2* yb = reinterpret_cast<const double2*>(a.br_y) + 4 * (int64_t)l;
-            const double2 Vf = V[a.br_from[l]], Vt = V[a.br_to[l]];
-            const double2 Sf = cmul(Vf, conj2(cadd(cmul(yb[0], Vf), cmul(yb[1], Vt))));
-            const double2 St = cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt))));
-            const double r = fmax(hypot(Sf.x, Sf.y), hypot(St.x, St.y)) / a.br_rate[l];
-            ld = (float)r;
-            lmax = fmax(lmax, r);
-            nv += r > 1.0;
-          }
-        }
-        a.loading_out[(int64_t)row * a.n_branch + l] = ld;
-      }
-      lmax = block_nanmax(lmax, s_red);
-      const double nv_all = block_sum(double(nv), s_red);
-      if (tid == 0) {
-        a.nviol_out[row] = ok ? (int)nv_all : -1;
-        a.maxload_out[row] = ok ? (float)lmax : NAN;
-      }
-    }
+    if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
 
     for (int i = tid; i < n; i += BS) vout[i] = V[i];
     if (tid == 0) {
@@ -1037,11 +1111,12 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   PhaseProf prof;
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
+  const int n_rows = a.n_rows_dev != nullptr ? *a.n_rows_dev : a.n_rows;
   for (;;) {
     if (threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
     __syncthreads();
     const int q = s_row;
-    if (q >= a.n_rows) {
+    if (q >= n_rows) {
       prof.flush(a.phase_cycles);
       return;
     }
@@ -1099,6 +1174,8 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
   }
 }
 
+#include "chord_sweep.cuh"
+
 template <typename T>
 int smem_bytes() {
   return sizeof(T) == 4 ? gs2g::dense32::Smem::bytes : dense::Smem<T>::bytes;
@@ -1153,6 +1230,48 @@ int launch_sweep_multi(const GridEntry* d_grids, int n_grids, const int* d_row_b
   else
     sweep_kernel_multi<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(d_grids, n_grids, d_row_begin, n_rows,
                                                                          queue, workspace, ws_stride, phase_cycles);
+  return (int)cudaGetLastError();
+}
+
+int64_t chord_workspace_bytes(const DevPlan& P, int prec) {
+  return prec == 1 ? chord_ws<float>(P).total : chord_ws<double>(P).total;
+}
+
+int chord_rows_per_cta() { return CK; }
+
+namespace {
+template <typename T>
+cudaError_t chord_opt_in(const DevPlan& P) {
+  return cudaFuncSetAttribute(chord_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, chord_smem_bytes<T>(P));
+}
+}  // namespace
+
+int chord_ctas(const DevPlan& P, int prec, int device) {
+  int n_sm = 0;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
+  int per_sm = 0;
+  if (prec == 1) {
+    chord_opt_in<float>(P);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chord_kernel<float>, BS, chord_smem_bytes<float>(P));
+  } else {
+    chord_opt_in<double>(P);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chord_kernel<double>, BS, chord_smem_bytes<double>(P));
+  }
+  if (per_sm < 1) per_sm = 1;
+  return n_sm * per_sm;
+}
+
+int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0 || a.base_ws == nullptr || a.base_inv == nullptr || a.handoff == nullptr ||
+      a.n_handoff == nullptr || a.fixed_iters)
+    return (int)cudaErrorInvalidValue;
+  cudaError_t e = prec == 1 ? chord_opt_in<float>(P) : chord_opt_in<double>(P);
+  if (e != cudaSuccess) return (int)e;
+  if (prec == 1)
+    chord_kernel<float><<<n_ctas, BS, chord_smem_bytes<float>(P), st>>>(P, a);
+  else
+    chord_kernel<double><<<n_ctas, BS, chord_smem_bytes<double>(P), st>>>(P, a);
   return (int)cudaGetLastError();
 }
 

@@ -79,6 +79,17 @@ struct SweepArgs {
   // below the mismatch at this complex [n_bus] voltage (the base case) starts
   // from it instead (nullptr: off); n_alt_start counts those rows
   const double* alt_v0;
+  // per-row Newton steps already taken by another launch (nullptr: none);
+  // may alias iters_out (read at the row's start, written at its end)
+  const int* iters_in;
+  // chord sweep (see launch_chord): rows it hands to the single-row kernel
+  // are appended to handoff ([n_rows]) and counted in *n_handoff
+  int* handoff;
+  int* n_handoff;
+  // when set, the launch's row count is read here on the device (a launch
+  // that follows the chord sweep on the same stream takes its hand-offs)
+  const int* n_rows_dev;
+  const double* alt_s;  // complex [n_bus] V conj(Y V) at alt_v0 on the unedited Ybus (nullptr: evaluate in full)
   int* n_alt_start;
   // policy 2: workspace (ws_layout of this plan and precision) holding the
   // base case's factor, shared read-only by every CTA; factor_only: factor
@@ -135,6 +146,16 @@ int64_t workspace_bytes(const DevPlan& P, int prec);
 // Launch the sweep on `stream` with `n_ctas` CTAs (<= 0: one wave at full
 // occupancy).  Returns the cudaError_t as int.
 int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream);
+
+// Chord sweep (policy 2, continuous schedule): chord_rows_per_cta() rows per
+// CTA step in lockstep on the base factor (a.base_ws) with its inverse
+// (a.base_inv); converged rows are finished, the others are handed off to a
+// following single-row launch (a.handoff / a.n_handoff, their V in v_out and
+// steps in iters_out).  Workspace per CTA: chord_workspace_bytes.
+int64_t chord_workspace_bytes(const DevPlan& P, int prec);
+int chord_rows_per_cta();
+int chord_ctas(const DevPlan& P, int prec, int device);
+int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream);
 
 // CTAs that fit at once for `prec` (for sizing the workspace).
 int sweep_ctas(int prec, int device);

@@ -80,6 +80,7 @@ struct gs2g_session {
   std::vector<double> vinit, sbus, base_v;
   bool has_base = false;
   DevBuf d_ybus, d_vinit, d_sbus, d_basev;
+  DevBuf d_bases;  // complex [n_bus] Vb conj(Y Vb): the power the base V draws on the unedited Ybus
 
   // branch data
   int n_branch = 0;
@@ -112,6 +113,8 @@ struct gs2g_session {
   DevBuf d_row_map;  // rows of gs2g_run_subset
   DevBuf d_base_ws;        // base case's factor for GS2G_REFACTOR_BASE_CHORD
   DevBuf d_base_inv;       // its inverse, column c = M0^-1 e_c (outage compensation)
+  DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
+  bool chord = true;       // policy 2 runs start with the multi-row chord sweep
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -403,6 +406,7 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   const bool base = rescue && s->has_base && use_rows;
   a.rescue_v0 = rescue ? (base ? s->d_basev.as<double>() : s->d_vinit.as<double>()) : nullptr;
   a.alt_v0 = base ? s->d_basev.as<double>() : nullptr;
+  a.alt_s = base ? s->d_bases.as<double>() : nullptr;
   a.phase_cycles = nullptr;
   if (use_rows && s->limits_on) {
     const size_t nr = (size_t)std::max(n_rows, 1);
@@ -429,8 +433,22 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   int n_ctas = n_ctas_req > 0 ? n_ctas_req : gs2g::sweep_ctas(o.precision, s->device);
   n_ctas = std::max(1, std::min(n_ctas, std::max(n_rows, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
-  s->d_ws.ensure((size_t)wsb * n_ctas);
-  s->d_queue.ensure(3 * sizeof(int));  // [0] row queue, [1] rescue count, [2] alternative starts
+  s->d_queue.ensure(4 * sizeof(int));  // [0] row queue, [1] rescue count, [2] alternative starts, [3] hand-offs
+  // policy 2 (continuous): the chord sweep takes every row first, several
+  // per CTA on the base factor, and hands the rows that need their own LU
+  // (or the rescue) to the single-row sweep that follows on the stream
+  const bool chord = s->chord && use_rows && n_rows > 0 && o.refactor_policy == GS2G_REFACTOR_BASE_CHORD &&
+                     a.base_ws != nullptr && a.base_inv != nullptr && !o.fixed_iters;
+  int n_chord = 0;
+  int64_t cwsb = 0;
+  if (chord) {
+    n_chord = n_ctas_req > 0 ? n_ctas_req : gs2g::chord_ctas(s->dplan, o.precision, s->device);
+    const int per = gs2g::chord_rows_per_cta();
+    n_chord = std::max(1, std::min(n_chord, (n_rows + per - 1) / per));
+    cwsb = gs2g::chord_workspace_bytes(s->dplan, o.precision);
+    s->d_handoff.ensure((size_t)n_rows * sizeof(int));
+  }
+  s->d_ws.ensure(std::max((size_t)wsb * n_ctas, (size_t)cwsb * n_chord));
   a.queue = s->d_queue.as<int>();
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
@@ -441,8 +459,29 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
     a.phase_cycles = s->d_phase.as<unsigned long long>();
   }
-  ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
+  ck(cudaMemsetAsync(s->d_queue.p, 0, 4 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
+  if (chord) {
+    gs2g::SweepArgs c = a;
+    c.ws_stride = cwsb;
+    c.handoff = s->d_handoff.as<int>();
+    c.n_handoff = s->d_queue.as<int>() + 3;
+    ck((cudaError_t)gs2g::launch_chord(s->dplan, c, o.precision, n_chord, s->stream), "chord sweep launch");
+    ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
+    // the hand-offs continue from where the chord sweep left them: their V
+    // (v_out) and step count (iters_out), on their own factor (policy 1)
+    a.row_map = s->d_handoff.as<int>();
+    a.n_rows_dev = s->d_queue.as<int>() + 3;
+    a.v0 = out.v;
+    a.v0_stride = s->n_bus;
+    a.iters_in = out.iters;
+    a.refactor_policy = GS2G_REFACTOR_ADAPTIVE;
+    a.base_ws = nullptr;
+    a.base_v = nullptr;
+    a.base_inv = nullptr;
+    a.alt_v0 = nullptr;
+    a.alt_s = nullptr;
+  }
   if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");
   ck(cudaStreamSynchronize(s->stream), "sweep");
@@ -581,6 +620,13 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
   s->d_sbus.ensure(2 * n_bus * sizeof(double));
   ck(cudaMemcpy(s->d_sbus.p, sbus, 2 * n_bus * sizeof(double), cudaMemcpyHostToDevice), "upload Sbus");
   *out = s.release();
+  GS2G_CATCH
+}
+
+int gs2g_session_set_chord(gs2g_session* s, int on) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_set_chord: NULL session");
+  s->chord = on != 0;
   GS2G_CATCH
 }
 
@@ -867,6 +913,29 @@ int gs2g_set_vinit(gs2g_session* s, const double* vinit) {
   GS2G_CATCH
 }
 
+namespace {
+// Vb conj(Y Vb) per bus for the current base V (host, once per base case),
+// so that a row's mismatch at the base V needs no sparse product
+void upload_base_power(gs2g_session* s) {
+  const int n = s->n_bus;
+  std::vector<double> S(2 * n);
+  for (int i = 0; i < n; ++i) {
+    double ir = 0, ii = 0;
+    for (int k = s->y_ip[i]; k < s->y_ip[i + 1]; ++k) {
+      const double yr = s->ybus[2 * k], yi = s->ybus[2 * k + 1];
+      const double vr = s->base_v[2 * s->y_ix[k]], vi = s->base_v[2 * s->y_ix[k] + 1];
+      ir += yr * vr - yi * vi;
+      ii += yr * vi + yi * vr;
+    }
+    const double vr = s->base_v[2 * i], vi = s->base_v[2 * i + 1];
+    S[2 * i] = vr * ir + vi * ii;  // V conj(I)
+    S[2 * i + 1] = vi * ir - vr * ii;
+  }
+  s->d_bases.ensure(2 * n * sizeof(double));
+  ck(cudaMemcpy(s->d_bases.p, S.data(), 2 * n * sizeof(double), cudaMemcpyHostToDevice), "upload base power");
+}
+}  // namespace
+
 int gs2g_solve_base(gs2g_session* s, const gs2g_run_opts* o_, double* v_out, int* status, int* iters,
                     double* residual) {
   GS2G_TRY
@@ -892,6 +961,7 @@ int gs2g_solve_base(gs2g_session* s, const gs2g_run_opts* o_, double* v_out, int
   ck(cudaMemcpy(s->d_basev.p, s->b_v.p, 2 * n * sizeof(double), cudaMemcpyDeviceToDevice), "keep base V");
   s->has_base = true;
   s->base_factor_prec = -1;
+  upload_base_power(s);
   if (v_out) std::memcpy(v_out, s->base_v.data(), 2 * n * sizeof(double));
   if (status) *status = st;
   if (iters) *iters = it;
@@ -922,6 +992,7 @@ int gs2g_set_base_v(gs2g_session* s, const double* v, double* residual) {
   s->base_v.assign(v, v + 2 * n);
   s->has_base = true;
   s->base_factor_prec = -1;
+  upload_base_power(s);
   if (residual) *residual = res;
   GS2G_CATCH
 }
