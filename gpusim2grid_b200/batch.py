@@ -138,13 +138,15 @@ class _BatchSweep:
     @property
     def _learned_opts(self):
         """(refactor_ratio, max_reuse) of learned runs.  On the shared base
-        factor (base_chord) injection rows keep chording longer (0.7 / 8):
-        their Jacobian stays close to the base one.  Rows with tripped
-        branches, whose flows move further, factor their own Jacobian as
-        soon as a step contracts by less than 0.5 (at most 6 steps on one
-        factor), as under the adaptive strategy."""
+        factor (base_chord) a chord step is cheap -- several rows share each
+        factor read -- so rows keep chording while a step contracts by 0.7 or
+        better, for at most 8 steps (the kernel also leaves the chord when
+        the remaining step budget could not reach tol at the observed rate).
+        Under the adaptive strategy a row factors its own Jacobian as soon as
+        a step contracts by less than 0.5, for at most 6 steps on one
+        factor."""
         r, m = getattr(self, "_learned_override", (None, None))
-        long_chord = self._strategy == "base_chord" and not self._rows_have_trips()
+        long_chord = self._strategy == "base_chord"
         return (float(r if r is not None else (0.7 if long_chord else 0.5)),
                 int(m if m is not None else (8 if long_chord else 6)))
 

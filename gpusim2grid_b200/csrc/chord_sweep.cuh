@@ -383,7 +383,8 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
         if (!isfinite(q.nrm)) q.act = rescue ? 5 : 3;
         else if (q.nrm < a.tol) q.act = 2;
         else if (q.it >= a.max_iter) q.act = rescue ? 5 : 4;
-        else if (!(q.nrm <= a.refactor_ratio * q.last) || q.since >= a.max_reuse) q.act = 5;  // needs its own LU
+        else if (!keep_factor(q.nrm, q.last, a.refactor_ratio, q.since, a.max_reuse, q.it, a.max_iter, a.tol))
+          q.act = 5;  // needs its own LU
         else q.act = 1;
       }
     }

@@ -383,6 +383,26 @@ __device__ __noinline__ void dense_solves(const T* __restrict__ A, int n, int ld
   }
 }
 
+// Whether a row keeps its current factor (an earlier iterate's, or the base
+// case's) for one more step: the mismatch must contract by at least `ratio`
+// per step and the factor must have served fewer than max_reuse steps.  Once
+// BUDGET_STEPS or fewer steps are left (Newton from a near iterate needs
+// about that many), the observed contraction rate -- settled by then -- held
+// for the remaining steps must also reach tol: a chord that cannot converge
+// in time is left for the row's own LU now, rather than after the budget is
+// spent and the row has to be rescued.
+constexpr int BUDGET_STEPS = 3;
+
+__device__ __forceinline__ bool keep_factor(double nrm, double last, double ratio, int since, int max_reuse, int it,
+                                            int max_iter, double tol) {
+  if (!(nrm <= ratio * last) || since >= max_reuse) return false;
+  if (max_iter - it <= BUDGET_STEPS && last < INFINITY && last > 0.0) {
+    const double rho = nrm / last;
+    if (rho > 0.0 && nrm * pow(rho, (double)(max_iter - it)) > tol) return false;
+  }
+  return true;
+}
+
 // Per-phase SM cycles, recorded by thread 0 of each CTA at the block-wide
 // barriers that separate the phases, summed over CTAs at exit.
 struct PhaseProf {
@@ -950,7 +970,8 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // (the rescue attempt restarts from Vinit, far from the solution: full
       // Newton there)
       const bool refactor = a.factor_only || !have_factor || a.refactor_policy == 0 || attempt > 0 ||
-                            !(nrm <= a.refactor_ratio * last_nrm) || since_factor >= a.max_reuse;
+                            !keep_factor(nrm, last_nrm, a.refactor_ratio, since_factor, a.max_reuse, it, a.max_iter,
+                                         a.tol);
       last_nrm = nrm;
       if (refactor) {
         have_factor = true;
