@@ -58,10 +58,13 @@ WORKLOADS = {
 }
 MAX_ITER, TOL = 10, 1e-8
 METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
-# DRAM bytes (read + write) of one sweep-kernel launch, from the ncu capture
-# summarised in profiles/sweep_kernel_full_n1_case2000_learned.md (same
-# workload, 3203 LUs and 14023 Newton steps in that launch)
-NCU_TRAFFIC = {"n1_sweep_case2000_synth": (69.64e9, 3203, 14023)}
+# DRAM bytes (read + write) of one timed step's sweep launches (chord sweep +
+# single-row sweep), from the ncu capture summarised in the profile named by
+# "source", with that step's counts of LUs, Newton steps and steps on the
+# shared base factor (same workload and command line as the default run)
+NCU_TRAFFIC = {"n1_sweep_case2000_synth": {
+    "dram_bytes": 2.0939e9 + 1.8876e9, "lus": 129, "steps": 13780, "chord_steps": 13633,
+    "source": "profiles/chord_kernel_full_n1_case2000_learned.md (20k training rows; same sweep workload)"}}
 
 
 def _args():
@@ -335,13 +338,16 @@ def run_ours(args):
             ev1.synchronize()
             pre_ms = ev0.elapsed_time(ev1)
         s.run(MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, False, strat, ratio, reuse, learned)
-        ms = s.timings()["kernel_ms"]
+        tm = s.timings()
+        ms = tm["kernel_ms"]
+        sweep_log.append((ms, int(tm["chord_steps"])))
         # rows left unconverged are re-solved in plain FP64 (part of the timed work)
         return pre_ms, ms + ca.fp64_fallback()
 
     def barrier():
         replicas.barrier()
 
+    sweep_log = []  # (sweep-launch ms, Newton steps on the shared base factor) per step
     for _ in range(args.warmup):
         step()
     clk = ClockSampler(local)
@@ -425,15 +431,21 @@ def run_ours(args):
     b_fact, b_iter = algorithmic_bytes(info, w)
     if p is not None:
         b_iter += 16 * info["n_bus"]  # each step reads the row's Sbus
-    launch_bytes = b_fact * total_factors + b_iter * total_iters
-    kernel_ms = float(np.mean(ker))
+    # a step on the shared base factor reads no factor of its own: that
+    # factor is shared structure, amortised to zero like the plan
+    b_iter_shared = b_iter - w * info["nnz_lu"]
+    chord_steps = sweep_log[-1][1]
+    launch_bytes = b_fact * total_factors + b_iter_shared * chord_steps + b_iter * (total_iters - chord_steps)
+    kernel_ms = float(np.mean([x[0] for x in sweep_log[-args.steps:]]))
     achieved_gbs = launch_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
     f_fact, f_iter = algorithmic_flops(info)
     launch_flops = f_fact * total_factors + f_iter * total_iters
     achieved_tflops = launch_flops / (kernel_ms / 1e3) / 1e12
     fma_peak = 71.4 if args.precision == "mixed" else 37.1
-    per_step_launches = 1 + (ls.launches_per_call(n) if learned else 0)
+    # base_chord: the chord sweep, then the single-row sweep for its hand-offs
+    sweep_launches = 2 if strat == lib.REFACTOR_BASE_CHORD else 1
+    per_step_launches = sweep_launches + (ls.launches_per_call(n) if learned else 0) + (1 if fallback_rows else 0)
     gname = WORKLOADS[args.workload][0]
 
     line = {
@@ -464,12 +476,16 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4),
                      "traffic": None if args.workload not in NCU_TRAFFIC else {
-                         "dram_bytes_per_launch": NCU_TRAFFIC[args.workload][0],
-                         "algorithmic_bytes_same_launch": b_fact * NCU_TRAFFIC[args.workload][1]
-                         + b_iter * NCU_TRAFFIC[args.workload][2],
-                         "source": "ncu capture, profiles/sweep_kernel_full_n1_case2000_learned.md"},
-                     "note": f"sweep kernel; peak {peak_kind}; algorithmic bytes per launch = {b_fact} per LU x "
-                             f"{total_factors} LUs + {b_iter} per Newton step x {total_iters} steps"},
+                         "dram_bytes_per_step": NCU_TRAFFIC[args.workload]["dram_bytes"],
+                         "algorithmic_bytes_same_step": b_fact * NCU_TRAFFIC[args.workload]["lus"]
+                         + b_iter_shared * NCU_TRAFFIC[args.workload]["chord_steps"]
+                         + b_iter * (NCU_TRAFFIC[args.workload]["steps"] - NCU_TRAFFIC[args.workload]["chord_steps"]),
+                         "source": NCU_TRAFFIC[args.workload]["source"]},
+                     "note": f"sweep launches of one step ({sweep_launches}); peak {peak_kind}; algorithmic bytes = "
+                             f"{b_fact} per LU x {total_factors} LUs + {b_iter_shared} per step on the shared base "
+                             f"factor x {chord_steps} + {b_iter} per step on a row's own factor x "
+                             f"{total_iters - chord_steps}; the shared factor is served from L2, so the sweep is "
+                             f"bound by L2 latency and bandwidth rather than HBM"},
         "fma_roofline": {"achieved": round(achieved_tflops, 3), "peak": fma_peak, "unit": "TFLOP/s",
                          "frac": round(achieved_tflops / fma_peak, 4),
                          "note": "FP64 (or FP32) FMA pipe; peak measured by a DFMA/FFMA loop on this pool"},

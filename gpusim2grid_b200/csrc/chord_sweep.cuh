@@ -237,6 +237,7 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   const int row = sl.row;
   double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
   for (int i = tid; i < n; i += BS) vout[i] = V[i];
+  if (tid == 0 && a.n_chord_steps != nullptr) atomicAdd(a.n_chord_steps, (unsigned long long)sl.it);
   if (sl.act == 5) {
     if (tid == 0) {
       a.iters_out[row] = sl.it;

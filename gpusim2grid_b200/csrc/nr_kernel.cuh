@@ -91,6 +91,8 @@ struct SweepArgs {
   const int* n_rows_dev;
   const double* alt_s;  // complex [n_bus] V conj(Y V) at alt_v0 on the unedited Ybus (nullptr: evaluate in full)
   int* n_alt_start;
+  // chord sweep: Newton steps taken on the shared base factor, summed over rows
+  unsigned long long* n_chord_steps;
   // policy 2: workspace (ws_layout of this plan and precision) holding the
   // base case's factor, shared read-only by every CTA; factor_only: factor
   // the Jacobian at the start voltage into the CTA's workspace and stop

@@ -382,6 +382,7 @@ class Session {
     d["phase_share"] = ps;
     d["n_rescued"] = t.n_rescued;
     d["n_base_start"] = t.n_base_start;
+    d["chord_steps"] = t.chord_steps;
     return d;
   }
 

@@ -114,6 +114,7 @@ struct gs2g_session {
   DevBuf d_base_ws;        // base case's factor for GS2G_REFACTOR_BASE_CHORD
   DevBuf d_base_inv;       // its inverse, column c = M0^-1 e_c (outage compensation)
   DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
+  DevBuf d_chord_steps;    // Newton steps the last chord sweep took on the base factor
   bool chord = true;       // policy 2 runs start with the multi-row chord sweep
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
@@ -460,12 +461,15 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.phase_cycles = s->d_phase.as<unsigned long long>();
   }
   ck(cudaMemsetAsync(s->d_queue.p, 0, 4 * sizeof(int), s->stream), "queue reset");
+  s->d_chord_steps.ensure(sizeof(unsigned long long));
+  ck(cudaMemsetAsync(s->d_chord_steps.p, 0, sizeof(unsigned long long), s->stream), "step count reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (chord) {
     gs2g::SweepArgs c = a;
     c.ws_stride = cwsb;
     c.handoff = s->d_handoff.as<int>();
     c.n_handoff = s->d_queue.as<int>() + 3;
+    c.n_chord_steps = s->d_chord_steps.as<unsigned long long>();
     ck((cudaError_t)gs2g::launch_chord(s->dplan, c, o.precision, n_chord, s->stream), "chord sweep launch");
     ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
     // the hand-offs continue from where the chord sweep left them: their V
@@ -490,6 +494,9 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
   ck(cudaMemcpy(&s->tm.n_rescued, s->d_queue.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost), "rescue count");
   ck(cudaMemcpy(&s->tm.n_base_start, s->d_queue.as<int>() + 2, sizeof(int), cudaMemcpyDeviceToHost), "start count");
+  unsigned long long cs = 0;
+  ck(cudaMemcpy(&cs, s->d_chord_steps.p, sizeof(cs), cudaMemcpyDeviceToHost), "step count");
+  s->tm.chord_steps = (int64_t)cs;
   if (o.profile_phases) {
     unsigned long long c[gs2g::N_PHASES];
     ck(cudaMemcpy(c, s->d_phase.p, sizeof(c), cudaMemcpyDeviceToHost), "read phases");
@@ -1208,6 +1215,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
     s->tm.total_iters = -1;
     s->tm.n_rescued = i == 0 ? counts[0] : 0;
     s->tm.n_base_start = i == 0 ? counts[1] : 0;
+    s->tm.chord_steps = 0;
     for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
   }
   if (o.profile_phases) {

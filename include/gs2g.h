@@ -122,6 +122,7 @@ typedef struct gs2g_timings {
   double phase_share[GS2G_N_PHASES];
   int n_rescued;    /* rows of the last run restarted (gs2g_run_opts.rescue) */
   int n_base_start; /* rows of the last run that began from the base V instead of their given start */
+  int64_t chord_steps; /* Newton steps of the last run taken in the chord sweep on the shared base factor */
 } gs2g_timings;
 
 const char* gs2g_last_error(void);
