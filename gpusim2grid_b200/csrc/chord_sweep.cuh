@@ -22,10 +22,23 @@
 // needed, the rescue attempt.  The decisions are the single-row kernel's:
 // the same ratio test, the same counters, the same statuses.
 //
+// With a.broyden set, the chord steps are Broyden's "good" method instead:
+// the base factor (with the row's outage compensation) is the initial
+// inverse Jacobian H0, and each step corrects H0 F by the rank-one updates
+// of the steps taken so far, in the storage-efficient form of C. T. Kelley
+// ("Iterative Methods for Linear and Nonlinear Equations", SIAM 1995, the
+// brsol algorithm): with steps s_0..s_n stored,
+//   z = H0 F;  z += s_{j+1} (s_j . z) / |s_j|^2  for j < n;
+//   s_{n+1} = z / (1 - (s_n . z) / |s_n|^2),
+// so a step costs one base solve plus a few dot products, and converges
+// superlinearly where the plain chord converges linearly.  The same
+// contraction, budget and hand-off tests apply to its steps.
+//
 // Included by nr_kernel.cu inside its anonymous namespace (it uses that
 // file's helpers).
 
-constexpr int CK = 4;  // rows per CTA
+constexpr int CK = 4;      // rows per CTA
+constexpr int CB_MAX = 10;  // Broyden steps kept per row (the memory restarts beyond)
 
 template <typename T>
 struct alignas(4 * sizeof(T)) Vec4 {
@@ -38,10 +51,10 @@ __device__ __forceinline__ void fms4(Vec4<T>& acc, T a, const Vec4<T>& b) {
   for (int s = 0; s < 4; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
 }
 
-// Workspace of one chord CTA: V [n] and F [dim] per slot, then the
-// interleaved right-hand sides y [dim] x CK.
+// Workspace of one chord CTA: V [n] and F [dim] per slot, the interleaved
+// right-hand sides y [dim] x CK, then the Broyden steps [CK][CB_MAX][dim].
 struct ChordWs {
-  int64_t V, F, y, total;
+  int64_t V, F, y, S, total;
 };
 
 template <typename T>
@@ -51,6 +64,7 @@ __host__ __device__ ChordWs chord_ws(const DevPlan& P) {
   w.V = o; o = align256(o + (int64_t)CK * P.n_bus * 16);
   w.F = o; o = align256(o + (int64_t)CK * P.dim * 8);
   w.y = o; o = align256(o + (int64_t)P.dim * sizeof(Vec4<T>));
+  w.S = o; o = align256(o + (int64_t)CK * CB_MAX * P.dim * sizeof(T));
   w.total = o;
   return w;
 }
@@ -63,6 +77,7 @@ struct ChordSlot {
   int fresh;  // first mismatch still to be compared with the alternative start
   int comp;   // outage compensation set up
   int act;    // this round: 1 solve, 2 converged, 3 diverged, 4 budget spent, 5 hand off
+  int nb;     // Broyden steps stored
   double nrm, last;
 };
 
@@ -89,6 +104,112 @@ __device__ __forceinline__ void block_nanmax4(double v[4], double* s_red4) {
     }
     v[s] = r;
   }
+  __syncthreads();
+}
+
+// Block sum of four values at once (one pair of barriers).
+__device__ __forceinline__ void block_sum4(double v[4], double* s_red4) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+    for (int o = 16; o > 0; o >>= 1) v[s] += __shfl_xor_sync(0xffffffffu, v[s], o);
+  if (lane == 0)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) s_red4[warp * 4 + s] = v[s];
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double r = 0.0;
+    for (int w = 0; w < NWARP; ++w) r += s_red4[w * 4 + s];
+    v[s] = r;
+  }
+  __syncthreads();
+}
+
+// Broyden correction of the slots in `mask`: y holds z = H0 F per slot on
+// entry and the step s_{nb} on exit, which is also stored as the slot's
+// next Broyden step (with its squared norm).  St: the CTA's steps
+// [CK][CB_MAX][dim]; s_ss: their squared norms.
+template <typename T>
+__device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, ChordSlot* sl, Vec4<T>* y, T* St,
+                                           double (*s_ss)[CB_MAX], double* s_red4) {
+  const int tid = threadIdx.x;
+  int nb[CK];
+  int maxnb = 0;
+#pragma unroll
+  for (int s = 0; s < CK; ++s) {
+    nb[s] = (mask >> s & 1) ? sl[s].nb : 0;
+    if (nb[s] >= CB_MAX) nb[s] = 0;  // memory full: restart from H0
+    maxnb = max(maxnb, nb[s]);
+  }
+  auto step = [&](int s, int j) { return St + ((int64_t)s * CB_MAX + j) * dim; };
+  for (int j = 0; j + 1 < maxnb; ++j) {
+    double d[CK] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = tid; i < dim; i += BS) {
+      const Vec4<T> z = y[i];
+#pragma unroll
+      for (int s = 0; s < CK; ++s)
+        if (j + 1 < nb[s]) d[s] += (double)step(s, j)[i] * (double)z.v[s];
+    }
+    block_sum4(d, s_red4);
+    T cf[CK];
+#pragma unroll
+    for (int s = 0; s < CK; ++s) {
+      const double ss = s_ss[s][j];
+      cf[s] = (j + 1 < nb[s] && ss > 0.0) ? (T)(d[s] / ss) : T(0);
+    }
+    for (int i = tid; i < dim; i += BS) {
+      Vec4<T> z = y[i];
+#pragma unroll
+      for (int s = 0; s < CK; ++s)
+        if (j + 1 < nb[s]) z.v[s] = fma(cf[s], step(s, j + 1)[i], z.v[s]);
+      y[i] = z;
+    }
+    __syncthreads();
+  }
+  // s_{nb} = z / (1 - (s_{nb-1} . z) / |s_{nb-1}|^2); a vanishing denominator
+  // (the update breaks down) restarts the memory with the plain step z
+  double d[CK] = {0.0, 0.0, 0.0, 0.0};
+  if (maxnb > 0) {
+    for (int i = tid; i < dim; i += BS) {
+      const Vec4<T> z = y[i];
+#pragma unroll
+      for (int s = 0; s < CK; ++s)
+        if (nb[s] > 0) d[s] += (double)step(s, nb[s] - 1)[i] * (double)z.v[s];
+    }
+    block_sum4(d, s_red4);
+  }
+  T sc[CK];
+#pragma unroll
+  for (int s = 0; s < CK; ++s) {
+    sc[s] = T(1);
+    if (nb[s] > 0) {
+      const double ss = s_ss[s][nb[s] - 1];
+      const double den = ss > 0.0 ? 1.0 - d[s] / ss : 0.0;
+      if (fabs(den) > 1e-6) sc[s] = (T)(1.0 / den);
+      else nb[s] = 0;
+    }
+  }
+  double q[CK] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = tid; i < dim; i += BS) {
+    Vec4<T> z = y[i];
+#pragma unroll
+    for (int s = 0; s < CK; ++s) {
+      if (!(mask >> s & 1)) continue;
+      z.v[s] *= sc[s];
+      step(s, nb[s])[i] = z.v[s];
+      q[s] += (double)z.v[s] * (double)z.v[s];
+    }
+    y[i] = z;
+  }
+  block_sum4(q, s_red4);
+  if (tid == 0)
+#pragma unroll
+    for (int s = 0; s < CK; ++s)
+      if (mask >> s & 1) {
+        s_ss[s][nb[s]] = q[s];
+        sl[s].nb = nb[s] + 1;
+      }
   __syncthreads();
 }
 
@@ -273,6 +394,7 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
   __shared__ double s_cLU[CK][MAX_COMP * MAX_COMP];
   __shared__ int s_cpiv[CK][MAX_COMP];
   __shared__ double s_cw[CK][MAX_COMP];
+  __shared__ double s_ss[CK][CB_MAX];
   const int tid = threadIdx.x;
   const int n = P.n_bus;
   const ChordWs L = chord_ws<T>(P);
@@ -280,6 +402,7 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
   double2* Vs = reinterpret_cast<double2*>(ws + L.V);
   double* Fs = reinterpret_cast<double*>(ws + L.F);
   Vec4<T>* y = reinterpret_cast<Vec4<T>*>(ws + L.y);
+  T* St = reinterpret_cast<T*>(ws + L.S);
   Vec4<T>* ys = reinterpret_cast<Vec4<T>*>(smem_raw);
   const WsLayout BL = ws_layout<T>(P);  // layout of the base factor's workspace
   const T* fHV = reinterpret_cast<const T*>(a.base_ws + BL.HV);
@@ -335,6 +458,7 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
           sl[s].fresh = a.alt_v0 != nullptr;
           sl[s].comp = 0;
           sl[s].act = 0;
+          sl[s].nb = 0;
           sl[s].last = INFINITY;
         }
         const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
@@ -420,6 +544,7 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
     chord_head_bw<T>(P, fHV, y);
     for (int s = 0; s < CK; ++s)
       if ((solve >> s & 1) && sl[s].comp) apply_compensation<T>(P.dim, &y[0].v[s], Minv, shs(s), CK);
+    if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red4);
     prof.mark(PH_SOLVE_BACK);
 
     // ---- V update (FP64, polar) ---------------------------------------------

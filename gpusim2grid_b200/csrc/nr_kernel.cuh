@@ -93,6 +93,8 @@ struct SweepArgs {
   int* n_alt_start;
   // chord sweep: Newton steps taken on the shared base factor, summed over rows
   unsigned long long* n_chord_steps;
+  // chord sweep: Broyden updates of the base factor's steps (see chord_sweep.cuh)
+  int broyden;
   // policy 2: workspace (ws_layout of this plan and precision) holding the
   // base case's factor, shared read-only by every CTA; factor_only: factor
   // the Jacobian at the start voltage into the CTA's workspace and stop

@@ -222,7 +222,7 @@ class Session {
     check(gs2g_session_replan(h(), tail_policy, dense_rate, force_tau));
   }
 
-  void set_chord(bool on) { check(gs2g_session_set_chord(h(), on ? 1 : 0)); }
+  void set_chord(int mode) { check(gs2g_session_set_chord(h(), mode)); }
 
   uintptr_t start_rows_buffer(int n_rows) {
     double* p = nullptr;
@@ -553,7 +553,7 @@ PYBIND11_MODULE(_gs2g, m) {
            py::arg("n_ctas") = 0, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
            py::arg("rescue") = false)
       .def("branch_loading", &Session::branch_loading)
-      .def("set_chord", &Session::set_chord, py::arg("on"))
+      .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)

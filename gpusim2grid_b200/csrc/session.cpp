@@ -115,7 +115,7 @@ struct gs2g_session {
   DevBuf d_base_inv;       // its inverse, column c = M0^-1 e_c (outage compensation)
   DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
   DevBuf d_chord_steps;    // Newton steps the last chord sweep took on the base factor
-  bool chord = true;       // policy 2 runs start with the multi-row chord sweep
+  int chord = 2;           // policy 2: 0 single-row sweep, 1 chord sweep, 2 chord sweep with Broyden steps
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -438,7 +438,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   // policy 2 (continuous): the chord sweep takes every row first, several
   // per CTA on the base factor, and hands the rows that need their own LU
   // (or the rescue) to the single-row sweep that follows on the stream
-  const bool chord = s->chord && use_rows && n_rows > 0 && o.refactor_policy == GS2G_REFACTOR_BASE_CHORD &&
+  const bool chord = s->chord > 0 && use_rows && n_rows > 0 && o.refactor_policy == GS2G_REFACTOR_BASE_CHORD &&
                      a.base_ws != nullptr && a.base_inv != nullptr && !o.fixed_iters;
   int n_chord = 0;
   int64_t cwsb = 0;
@@ -470,6 +470,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     c.handoff = s->d_handoff.as<int>();
     c.n_handoff = s->d_queue.as<int>() + 3;
     c.n_chord_steps = s->d_chord_steps.as<unsigned long long>();
+    c.broyden = s->chord == 2;
     ck((cudaError_t)gs2g::launch_chord(s->dplan, c, o.precision, n_chord, s->stream), "chord sweep launch");
     ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
     // the hand-offs continue from where the chord sweep left them: their V
@@ -630,10 +631,11 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
   GS2G_CATCH
 }
 
-int gs2g_session_set_chord(gs2g_session* s, int on) {
+int gs2g_session_set_chord(gs2g_session* s, int mode) {
   GS2G_TRY
   if (!s) throw std::invalid_argument("session_set_chord: NULL session");
-  s->chord = on != 0;
+  if (mode < 0 || mode > 2) throw std::invalid_argument("session_set_chord: mode must be 0, 1 or 2");
+  s->chord = mode;
   GS2G_CATCH
 }
 

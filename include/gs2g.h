@@ -144,13 +144,15 @@ int gs2g_session_destroy(gs2g_session* s);
  * facades' autotuner, which times candidate plans on the caller's rows
  * (the reference's lu_plan builds one plan; no counterpart). */
 int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int force_tau);
-/* GS2G_REFACTOR_BASE_CHORD with the continuous schedule runs in two launches
- * by default: a chord sweep that steps several rows per CTA in lockstep on
- * the shared base factor (every factor read serves all of them), then the
- * single-row sweep for the rows that need their own LU or the rescue,
- * continued from where the chord sweep left them.  on = 0 keeps every row in
- * the single-row sweep (same decisions; for comparison). */
-int gs2g_session_set_chord(gs2g_session* s, int on);
+/* GS2G_REFACTOR_BASE_CHORD with the continuous schedule runs in two launches:
+ * a chord sweep that steps several rows per CTA in lockstep on the shared
+ * base factor (every factor read serves all of them), then the single-row
+ * sweep for the rows that need their own LU or the rescue, continued from
+ * where the chord sweep left them.  mode 2 (default): the chord steps are
+ * Broyden steps on the base factor (superlinear instead of linear
+ * convergence); mode 1: plain chord steps, the same decisions as the
+ * single-row sweep; mode 0: every row in the single-row sweep. */
+int gs2g_session_set_chord(gs2g_session* s, int mode);
 int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
 int gs2g_get_device(const gs2g_session* s, int* device);
 

@@ -1,9 +1,11 @@
 """The chord sweep (several rows per CTA in lockstep on the shared base
 factor, hand-off of the rows that need their own LU to the single-row
-sweep) must take the single-row sweep's decisions: the same statuses, Newton
-steps and factorizations per row, and the same voltages within the mixed-
-precision bar.  Covers the hand-off, islanded rows, branch loading at
-eviction and fewer rows than slots."""
+sweep) with plain chord steps must take the single-row sweep's decisions:
+the same statuses, Newton steps and factorizations per row, and the same
+voltages within the mixed-precision bar.  Covers the hand-off, islanded
+rows, branch loading at eviction and fewer rows than slots.  With Broyden
+steps (the default) the rows converge to the same solutions as plain FP64
+Newton, with the same statuses, in no more Newton steps than the chord."""
 
 import numpy as np
 import pytest
@@ -15,14 +17,17 @@ from gpusim2grid_b200.synthetic import injection_scenarios, n1_branches, scenari
 pytestmark = pytest.mark.gpu
 
 
+CHORD, SINGLE, BROYDEN = 1, 0, 2
+
+
 def _both(f):
-    """(chord, single-row) results of the facade's current rows."""
+    """(plain chord, single-row) results of the facade's current rows."""
     out = []
-    for on in (True, False):
-        f.session.set_chord(on)
+    for mode in (CHORD, SINGLE):
+        f.session.set_chord(mode)
         f.compute()
         out.append((f.V_results, f.get_row_status(), f.get_row_iterations(), f.get_row_factorizations()))
-    f.session.set_chord(True)
+    f.session.set_chord(BROYDEN)
     return out
 
 
@@ -59,8 +64,8 @@ def test_chord_injections_and_outages_with_flows(g118):
     sw.set_topology(scenario_outages(g118, 301, max_trips=2, seed=10))
     sw.set_branch_limits(rng.uniform(50.0, 300.0, g118.n_branch), g118.sn_mva)
     out = []
-    for on in (True, False):
-        sw.session.set_chord(on)
+    for mode in (CHORD, SINGLE):
+        sw.session.set_chord(mode)
         sw.compute()
         out.append((sw.V_results, sw.get_row_status(), sw.get_row_iterations(), sw.get_row_factorizations(),
                     sw.branch_loading()))
@@ -96,8 +101,8 @@ def test_chord_learned_like_starts_and_rescue(g118):
     V0[::3] = np.nan
     sw.set_start_voltages(V0)
     out, rescued = [], []
-    for on in (True, False):
-        sw.session.set_chord(on)
+    for mode in (CHORD, SINGLE):
+        sw.session.set_chord(mode)
         sw.compute()
         out.append((sw.V_results, sw.get_row_status(), sw.get_row_iterations(), sw.get_row_factorizations()))
         t = sw.session.timings()
@@ -105,3 +110,29 @@ def test_chord_learned_like_starts_and_rescue(g118):
         rescued.append(t["n_rescued"])
     _same(out[0], out[1], TOL_V_MIXED)
     assert rescued[0] == rescued[1] > 0
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_broyden_steps_reach_the_fp64_solutions(g118, precision):
+    """Broyden steps on the base factor: N-1 rows and injection + outage rows
+    converge to plain FP64 Newton's solutions with the same statuses, in
+    fewer Newton steps than the plain chord."""
+    ref = ContingencyAnalysisGPU(g118.as_tuple(), init_from_n_powerflow=False, precision="fp64", nb_iter=10,
+                                 scheduling="continuous", tol=1e-8, start="flat", strategy="refactor_every")
+    ca = ContingencyAnalysisGPU(g118.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
+                                scheduling="continuous", tol=1e-8, start="base", strategy="base_chord")
+    rows = [[b] for b in range(g118.n_branch)]
+    for f in (ref, ca):
+        f.set_branch_data(*g118.branch_data())
+        f.add_contingencies_by_branch_id(rows)
+    ref.compute()
+    its = {}
+    for mode in (CHORD, BROYDEN):
+        ca.session.set_chord(mode)
+        ca.compute()
+        np.testing.assert_array_equal(ca.get_row_status(), ref.get_row_status())
+        ok = ref.get_row_status() == RowStatus.CONVERGED
+        # another iteration stopped at the same ||F|| tolerance: the |dV| bar of the metric
+        assert np.abs(ca.V_results[ok] - ref.V_results[ok]).max() < TOL_V_MIXED
+        its[mode] = ca.get_row_iterations()[ok].sum()
+    assert its[BROYDEN] < its[CHORD]
