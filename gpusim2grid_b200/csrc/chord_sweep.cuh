@@ -362,7 +362,7 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   if (sl.act == 5) {
     if (tid == 0) {
       a.iters_out[row] = sl.it;
-      a.handoff[atomicAdd(a.n_handoff, 1)] = row;
+      a.handoff[atomicAdd(a.n_handoff, 1)] = a.handoff_base + row;
     }
     __syncthreads();
     return;
@@ -378,8 +378,11 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   __syncthreads();
 }
 
+// The chord loop over the rows of one grid (queue a.queue, a.n_rows), until
+// that queue is exhausted and every slot has left.  Called by the
+// single-grid kernel once and by the multi-grid kernel once per grid.
 template <typename T>
-__global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const SweepArgs a) {
+__device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a, PhaseProf& prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChordSlot sl[CK];
   __shared__ int s_pull, s_more;
@@ -413,8 +416,6 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
     return RowShared<T>{&s_ne[s], s_ek[s], s_ev[s], s_red, nullptr, nullptr, s_cr[s], s_cB[s], s_cLU[s], s_cpiv[s],
                         s_cw[s]};
   };
-  PhaseProf prof;
-  prof.init(a.phase_cycles != nullptr && tid == 0);
   if (tid == 0) {
     for (int s = 0; s < CK; ++s) sl[s].row = -1;
     s_more = 1;
@@ -575,7 +576,37 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
     __syncthreads();
     prof.mark(PH_UPDATE);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const SweepArgs a) {
+  PhaseProf prof;
+  prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
+  chord_body<T>(P, a, prof);
   prof.flush(a.phase_cycles);
+}
+
+// Multi-grid chord sweep: a CTA binds its slots to one grid at a time (the
+// slots share that grid's base factor), draining the grids' own queues in
+// cyclic order from grid blockIdx.x % n_grids, so the CTAs spread over the
+// grids and move on as queues run dry.  The grid's plan and arguments are
+// copied into shared memory while the CTA works on it.
+template <typename T>
+__global__ void __launch_bounds__(BS, 2)
+    chord_kernel_multi(const GridEntry* __restrict__ grids, int n_grids, unsigned long long* phase_cycles) {
+  __shared__ __align__(16) GridEntry s_grid;
+  PhaseProf prof;
+  prof.init(phase_cycles != nullptr && threadIdx.x == 0);
+  for (int k = 0; k < n_grids; ++k) {
+    const int g = (blockIdx.x + k) % n_grids;
+    const int* src = reinterpret_cast<const int*>(grids + g);
+    int* dst = reinterpret_cast<int*>(&s_grid);
+    for (int i = threadIdx.x; i < (int)(sizeof(GridEntry) / sizeof(int)); i += BS) dst[i] = src[i];
+    __syncthreads();
+    chord_body<T>(s_grid.P, s_grid.a, prof);
+    __syncthreads();  // every thread is done with this grid's entry before the next copy
+  }
+  prof.flush(phase_cycles);
 }
 
 template <typename T>

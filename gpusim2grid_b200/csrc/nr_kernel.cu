@@ -1153,7 +1153,8 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
 template <typename T>
 __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
     sweep_kernel_multi(const GridEntry* __restrict__ grids, int n_grids, const int* __restrict__ row_begin,
-                       int n_rows, int* queue, char* workspace, int64_t ws_stride, unsigned long long* phase_cycles) {
+                       int n_rows, int* queue, char* workspace, int64_t ws_stride, unsigned long long* phase_cycles,
+                       const int* __restrict__ row_list, const int* __restrict__ n_rows_dev) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_row;
   __shared__ int s_ne;
@@ -1173,14 +1174,18 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
   PhaseProf prof;
   prof.init(phase_cycles != nullptr && threadIdx.x == 0);
   int cur = -1;
+  // with row_list, queue entry q solves global row row_list[q], and the
+  // number of entries is read on the device (hand-offs of a chord sweep)
+  const int n_entries = n_rows_dev != nullptr ? *n_rows_dev : n_rows;
   for (;;) {
     if (threadIdx.x == 0) s_row = atomicAdd(queue, 1);
     __syncthreads();
-    const int row = s_row;
-    if (row >= n_rows) {
+    const int q = s_row;
+    if (q >= n_entries) {
       prof.flush(phase_cycles);
       return;
     }
+    const int row = row_list != nullptr ? row_list[q] : q;
     int g = 0;
     while (g + 1 < n_grids && row >= row_begin[g + 1]) ++g;
     if (g != cur) {
@@ -1240,17 +1245,17 @@ int sweep_ctas(int prec, int device) {
 
 int launch_sweep_multi(const GridEntry* d_grids, int n_grids, const int* d_row_begin, int n_rows, int* queue,
                        char* workspace, int64_t ws_stride, unsigned long long* phase_cycles, int prec, int n_ctas,
-                       void* stream) {
+                       void* stream, const int* row_list, const int* n_rows_dev) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n_ctas <= 0 || n_grids <= 0 || n_grids > MAX_GRIDS) return (int)cudaErrorInvalidValue;
   const cudaError_t e = opt_in_smem();
   if (e != cudaSuccess) return (int)e;
   if (prec == 1)
-    sweep_kernel_multi<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(d_grids, n_grids, d_row_begin, n_rows, queue,
-                                                                       workspace, ws_stride, phase_cycles);
+    sweep_kernel_multi<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(
+        d_grids, n_grids, d_row_begin, n_rows, queue, workspace, ws_stride, phase_cycles, row_list, n_rows_dev);
   else
-    sweep_kernel_multi<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(d_grids, n_grids, d_row_begin, n_rows,
-                                                                         queue, workspace, ws_stride, phase_cycles);
+    sweep_kernel_multi<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(
+        d_grids, n_grids, d_row_begin, n_rows, queue, workspace, ws_stride, phase_cycles, row_list, n_rows_dev);
   return (int)cudaGetLastError();
 }
 
@@ -1295,6 +1300,24 @@ int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
     chord_kernel<double><<<n_ctas, BS, chord_smem_bytes<double>(P), st>>>(P, a);
   return (int)cudaGetLastError();
 }
+
+int launch_chord_multi(const GridEntry* d_grids, int n_grids, int smem, unsigned long long* phase_cycles, int prec,
+                       int n_ctas, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0 || n_grids <= 0 || n_grids > MAX_GRIDS || smem <= 0) return (int)cudaErrorInvalidValue;
+  cudaError_t e = prec == 1 ? cudaFuncSetAttribute(chord_kernel_multi<float>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                            : cudaFuncSetAttribute(chord_kernel_multi<double>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  if (prec == 1)
+    chord_kernel_multi<float><<<n_ctas, BS, smem, st>>>(d_grids, n_grids, phase_cycles);
+  else
+    chord_kernel_multi<double><<<n_ctas, BS, smem, st>>>(d_grids, n_grids, phase_cycles);
+  return (int)cudaGetLastError();
+}
+
+int chord_smem(const DevPlan& P, int prec) { return prec == 1 ? chord_smem_bytes<float>(P) : chord_smem_bytes<double>(P); }
 
 int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -86,6 +86,7 @@ struct SweepArgs {
   // are appended to handoff ([n_rows]) and counted in *n_handoff
   int* handoff;
   int* n_handoff;
+  int handoff_base;  // added to the row id in handoff (multi-grid: the grid's first global row)
   // when set, the launch's row count is read here on the device (a launch
   // that follows the chord sweep on the same stream takes its hand-offs)
   const int* n_rows_dev;
@@ -176,9 +177,18 @@ struct GridEntry {
 // d_grids [n_grids] and d_row_begin [n_grids + 1] in device memory; queue
 // zeroed by the caller; workspace n_ctas * ws_stride bytes, ws_stride >=
 // workspace_bytes of every grid.
+// With row_list, queue entry q solves global row row_list[q] and the entry
+// count is read from *n_rows_dev (the hand-offs of a multi-grid chord sweep).
 int launch_sweep_multi(const GridEntry* d_grids, int n_grids, const int* d_row_begin, int n_rows, int* queue,
                        char* workspace, int64_t ws_stride, unsigned long long* phase_cycles, int prec, int n_ctas,
-                       void* stream);
+                       void* stream, const int* row_list = nullptr, const int* n_rows_dev = nullptr);
+// Multi-grid chord sweep over d_grids (policy 2, every grid with its base
+// factor and inverse; each grid's a.queue its own zeroed counter; a.handoff
+// one list for all grids, a.handoff_base the grid's first global row).
+// smem: the largest chord_smem of the grids.
+int launch_chord_multi(const GridEntry* d_grids, int n_grids, int smem, unsigned long long* phase_cycles, int prec,
+                       int n_ctas, void* stream);
+int chord_smem(const DevPlan& P, int prec);
 
 // Size of the file-scope device array the allocation-free sweep uses as its
 // scratch (row queue + per-CTA workspaces).

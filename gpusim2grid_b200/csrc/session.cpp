@@ -1167,7 +1167,9 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   std::vector<gs2g::GridEntry> ge(n_sessions);
   std::vector<int> begin(n_sessions + 1, 0);
   int64_t wsb = 0;
-  s0->d_queue.ensure(3 * sizeof(int));
+  // [0] row queue, [1] rescue count, [2] alternative starts, [3] hand-offs,
+  // [4 + i] chord queue of grid i
+  s0->d_queue.ensure((4 + n_sessions) * sizeof(int));
   for (int i = 0; i < n_sessions; ++i) {
     gs2g_session* s = sessions[i];
     assemble_rows(s);
@@ -1183,24 +1185,80 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   const int total = begin[n_sessions];
   int n_ctas = o.n_ctas > 0 ? o.n_ctas : gs2g::sweep_ctas(o.precision, s0->device);
   n_ctas = std::max(1, std::min(n_ctas, std::max(total, 1)));
+  // policy 2 (continuous): a multi-grid chord sweep first (several rows per
+  // CTA on each grid's base factor), then the single-row sweep continues the
+  // rows it hands off, from v_out / iters_out on their own factors
+  bool chord = s0->chord > 0 && total > 0 && o.refactor_policy == GS2G_REFACTOR_BASE_CHORD && !o.fixed_iters;
+  for (int i = 0; i < n_sessions; ++i) chord = chord && ge[i].a.base_ws != nullptr && ge[i].a.base_inv != nullptr;
+  std::vector<gs2g::GridEntry> gc;
+  int64_t cwsb = 0;
+  int csmem = 0, n_chord = 0;
+  if (chord) {
+    const int per = gs2g::chord_rows_per_cta();
+    int big = 0;
+    for (int i = 0; i < n_sessions; ++i) {
+      cwsb = std::max(cwsb, gs2g::chord_workspace_bytes(sessions[i]->dplan, o.precision));
+      const int sm = gs2g::chord_smem(sessions[i]->dplan, o.precision);
+      if (sm > csmem) {
+        csmem = sm;
+        big = i;
+      }
+    }
+    n_chord = o.n_ctas > 0 ? o.n_ctas : gs2g::chord_ctas(sessions[big]->dplan, o.precision, s0->device);
+    n_chord = std::max(1, std::min(n_chord, (total + per - 1) / per));
+    s0->d_handoff.ensure((size_t)total * sizeof(int));
+    s0->d_chord_steps.ensure(sizeof(unsigned long long));
+    gc = ge;
+    for (int i = 0; i < n_sessions; ++i) {
+      gs2g::SweepArgs& a = gc[i].a;
+      a.queue = s0->d_queue.as<int>() + 4 + i;
+      a.ws_stride = cwsb;
+      a.handoff = s0->d_handoff.as<int>();
+      a.n_handoff = s0->d_queue.as<int>() + 3;
+      a.handoff_base = begin[i];
+      a.n_chord_steps = s0->d_chord_steps.as<unsigned long long>();
+      a.broyden = s0->chord == 2;
+      // the hand-offs continue from where the chord sweep left them
+      gs2g::SweepArgs& b = ge[i].a;
+      b.v0 = b.v_out;
+      b.v0_stride = sessions[i]->n_bus;
+      b.iters_in = b.iters_out;
+      b.refactor_policy = GS2G_REFACTOR_ADAPTIVE;
+      b.base_ws = nullptr;
+      b.base_v = nullptr;
+      b.base_inv = nullptr;
+      b.alt_v0 = nullptr;
+      b.alt_s = nullptr;
+    }
+  }
+  s0->d_ws.ensure(std::max((size_t)wsb * n_ctas, (size_t)cwsb * n_chord));
+  for (auto& e : gc) e.a.workspace = s0->d_ws.as<char>();
   const size_t ge_bytes = sizeof(gs2g::GridEntry) * n_sessions;
-  s0->d_multi.ensure(ge_bytes + sizeof(int) * (n_sessions + 1));
+  s0->d_multi.ensure(2 * ge_bytes + sizeof(int) * (n_sessions + 1));
   ck(cudaMemcpy(s0->d_multi.p, ge.data(), ge_bytes, cudaMemcpyHostToDevice), "upload grids");
-  int* d_begin = reinterpret_cast<int*>(s0->d_multi.as<char>() + ge_bytes);
+  if (chord) ck(cudaMemcpy(s0->d_multi.as<char>() + ge_bytes, gc.data(), ge_bytes, cudaMemcpyHostToDevice), "upload grids");
+  int* d_begin = reinterpret_cast<int*>(s0->d_multi.as<char>() + 2 * ge_bytes);
   ck(cudaMemcpy(d_begin, begin.data(), sizeof(int) * (n_sessions + 1), cudaMemcpyHostToDevice), "upload grids");
-  s0->d_ws.ensure((size_t)wsb * n_ctas);
   unsigned long long* phase = nullptr;
   if (o.profile_phases) {
     s0->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
     ck(cudaMemsetAsync(s0->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s0->stream), "phase reset");
     phase = s0->d_phase.as<unsigned long long>();
   }
-  ck(cudaMemsetAsync(s0->d_queue.p, 0, 3 * sizeof(int), s0->stream), "queue reset");
+  ck(cudaMemsetAsync(s0->d_queue.p, 0, (4 + n_sessions) * sizeof(int), s0->stream), "queue reset");
+  if (chord) ck(cudaMemsetAsync(s0->d_chord_steps.p, 0, sizeof(unsigned long long), s0->stream), "step count reset");
   ck(cudaEventRecord(s0->ev0, s0->stream), "event");
+  if (chord)
+    ck((cudaError_t)gs2g::launch_chord_multi(
+           reinterpret_cast<const gs2g::GridEntry*>(s0->d_multi.as<char>() + ge_bytes), n_sessions, csmem, phase,
+           o.precision, n_chord, s0->stream),
+       "multi-grid chord sweep launch");
   if (total > 0)
     ck((cudaError_t)gs2g::launch_sweep_multi(reinterpret_cast<const gs2g::GridEntry*>(s0->d_multi.p), n_sessions,
                                              d_begin, total, s0->d_queue.as<int>(), s0->d_ws.as<char>(), wsb, phase,
-                                             o.precision, n_ctas, s0->stream),
+                                             o.precision, n_ctas, s0->stream,
+                                             chord ? s0->d_handoff.as<int>() : nullptr,
+                                             chord ? s0->d_queue.as<int>() + 3 : nullptr),
        "multi-grid sweep launch");
   ck(cudaEventRecord(s0->ev1, s0->stream), "event");
   ck(cudaStreamSynchronize(s0->stream), "multi-grid sweep");
@@ -1218,6 +1276,11 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
     s->tm.n_rescued = i == 0 ? counts[0] : 0;
     s->tm.n_base_start = i == 0 ? counts[1] : 0;
     s->tm.chord_steps = 0;
+    if (i == 0 && chord) {
+      unsigned long long cs = 0;
+      ck(cudaMemcpy(&cs, s0->d_chord_steps.p, sizeof(cs), cudaMemcpyDeviceToHost), "step count");
+      s->tm.chord_steps = (int64_t)cs;
+    }
     for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
   }
   if (o.profile_phases) {

@@ -14,9 +14,10 @@ from oracle import nr_oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _sweep(g, n_rows, precision, seed):
+def _sweep(g, n_rows, precision, seed, strategy="adaptive"):
+    start = "base" if strategy == "base_chord" else "flat"
     sw = ScenarioSweepGPU(g.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
-                          scheduling="continuous", start="flat", strategy="adaptive")
+                          scheduling="continuous", start=start, strategy=strategy)
     sw.set_branch_data(*g.branch_data())
     p, q = injection_scenarios(g, n_rows, seed=seed)
     sw.set_injections(p, q, g.sn_mva)
@@ -24,18 +25,22 @@ def _sweep(g, n_rows, precision, seed):
     return sw, p, q
 
 
+@pytest.mark.parametrize("strategy", ["adaptive", "base_chord"])
 @pytest.mark.parametrize("precision,tol_v", [("fp64", TOL_V_FP64), ("mixed", TOL_V_MIXED)])
-def test_multi_grid_launch_equals_separate_sweeps(precision, tol_v):
+def test_multi_grid_launch_equals_separate_sweeps(precision, tol_v, strategy):
+    """base_chord runs the multi-grid chord sweep (a CTA's slots bound to one
+    grid at a time) and the multi-grid hand-off sweep."""
     spec = [("case118_synth", 48), ("case2000_synth", 40), ("case6500_synth", 16)]
     grids = [grid_by_name(name, 0) for name, _ in spec]
-    multi = [_sweep(g, n, precision, 20 + i)[0] for i, (g, (_, n)) in enumerate(zip(grids, spec))]
-    alone = [_sweep(g, n, precision, 20 + i) for i, (g, (_, n)) in enumerate(zip(grids, spec))]
+    multi = [_sweep(g, n, precision, 20 + i, strategy)[0] for i, (g, (_, n)) in enumerate(zip(grids, spec))]
+    alone = [_sweep(g, n, precision, 20 + i, strategy) for i, (g, (_, n)) in enumerate(zip(grids, spec))]
     ms = compute_many(multi)
     assert ms > 0
     for sw_m, (sw_a, p, q), g in zip(multi, alone, grids):
         sw_a.compute()
         np.testing.assert_array_equal(sw_m.get_row_status(), sw_a.get_row_status())
         np.testing.assert_array_equal(sw_m.get_row_iterations(), sw_a.get_row_iterations())
+        np.testing.assert_array_equal(sw_m.get_row_factorizations(), sw_a.get_row_factorizations())
         ok = sw_a.get_row_status() == RowStatus.CONVERGED
         assert ok.mean() > 0.9
         np.testing.assert_array_equal(sw_m.V_results[ok], sw_a.V_results[ok])
