@@ -565,6 +565,7 @@ def run_ours_multi(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     sweeps = []
+    chord_log = []  # Newton steps on the shared base factors, per step
 
     def step():
         pre_ms = 0.0
@@ -577,7 +578,9 @@ def run_ours_multi(args):
             ev1.synchronize()
             pre_ms = ev0.elapsed_time(ev1)
         lib.run_multi(sessions, MAX_ITER, TOL, False, prec, start_mode, 0.0, 0, False, strat, ratio, reuse, learned)
-        ms = sweep_ms = sessions[0].timings()["kernel_ms"]
+        tm0 = sessions[0].timings()
+        ms = sweep_ms = tm0["kernel_ms"]
+        chord_log.append(int(tm0["chord_steps"]))
         for f in facades:
             f._ran = True
             ms += f.fp64_fallback()
@@ -609,12 +612,21 @@ def run_ours_multi(args):
     value = world * n_conv * args.steps / (total_ms / 1e3)
     # roofline of the multi-grid sweep launch: each grid's algorithmic bytes
     # per LU and per Newton step times its rows' counts in the last step
+    # a step on a grid's shared base factor reads no factor of its own; the
+    # chord steps are counted over all grids, so they are split by each
+    # grid's share of the Newton steps (an approximation)
     w = 4 if args.precision == "mixed" else 8
     launch_bytes = 0
+    chord_steps = chord_log[-1] if chord_log else 0
+    steps_all = max(1, int(sum(int(r_[3].sum()) for r_ in res)))
     for s_, (g_, _, _, _), r_ in zip(sessions, parts, res):
-        b_fact, b_iter = algorithmic_bytes(s_.info(), w)
+        info_ = s_.info()
+        b_fact, b_iter = algorithmic_bytes(info_, w)
         b_iter += 16 * g_.n_bus  # each step reads the row's Sbus
-        launch_bytes += b_fact * int(s_.factor_counts().sum()) + b_iter * int(r_[3].sum())
+        steps_g = int(r_[3].sum())
+        shared_g = int(round(chord_steps * steps_g / steps_all))
+        launch_bytes += (b_fact * int(s_.factor_counts().sum()) + (b_iter - w * info_["nnz_lu"]) * shared_g
+                         + b_iter * (steps_g - shared_g))
     sweep_ms = float(np.mean(sweeps[-args.steps:]))
     achieved_gbs = launch_bytes / (sweep_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
@@ -657,7 +669,10 @@ def run_ours_multi(args):
     h2d = sum(2 * p.nbytes + 4 * (len(t) + 1) + 4 * sum(len(x) for x in t) for _, t, p, _ in parts)
     d2h = sum(o[0].nbytes + o[1].nbytes + o[2].nbytes for o in outs)
 
-    per_step_launches = 1 + (sum(ls.launches_per_call(n) for ls, n in zip(learners, n_rows)) if learned else 0)
+    # base_chord: the multi-grid chord sweep, then the hand-off sweep
+    sweep_launches = 2 if strat == lib.REFACTOR_BASE_CHORD else 1
+    per_step_launches = sweep_launches + (sum(ls.launches_per_call(n) for ls, n in zip(learners, n_rows))
+                                          if learned else 0) + (1 if fallback_rows else 0)
     line = {
         "metric": METRIC,
         "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -680,9 +695,10 @@ def run_ours_multi(args):
         "plan_tails": [s.info()["tail_dim"] for s in sessions],
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 4), "traffic": None,
-                     "note": f"multi-grid sweep kernel ({round(sweep_ms, 3)} ms per launch); peak {peak_kind}; "
-                             f"algorithmic bytes per launch = sum over grids of bytes per LU x LUs + bytes per "
-                             f"Newton step x steps = {launch_bytes}"},
+                     "note": f"multi-grid chord sweep + hand-off sweep ({round(sweep_ms, 3)} ms per step); peak "
+                             f"{peak_kind}; algorithmic bytes = sum over grids of bytes per LU x LUs + bytes per "
+                             f"Newton step x steps, a step on the shared base factor without its factor read "
+                             f"({chord_steps} of {steps_all} steps) = {launch_bytes}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": args.steps * per_step_launches,
