@@ -37,6 +37,14 @@
 // Included by nr_kernel.cu inside its anonymous namespace (it uses that
 // file's helpers).
 
+// CTAs per SM the chord kernels are compiled for (registers per thread
+// follow: 3 -> 80).  The chord loop waits on dependent L2 loads, so more
+// resident warps pay: 3 per SM was 15 % faster than 2 on the 2000- and
+// 6500-bus sweeps.
+#ifndef GS2G_CHORD_CTAS_PER_SM
+#define GS2G_CHORD_CTAS_PER_SM 3
+#endif
+
 constexpr int CK = 4;      // rows per CTA
 constexpr int CB_MAX = 10;  // Broyden steps kept per row (the memory restarts beyond)
 
@@ -579,7 +587,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const SweepArgs a) {
+__global__ void __launch_bounds__(BS, GS2G_CHORD_CTAS_PER_SM) chord_kernel(const DevPlan P, const SweepArgs a) {
   PhaseProf prof;
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
   chord_body<T>(P, a, prof);
@@ -592,7 +600,7 @@ __global__ void __launch_bounds__(BS, 2) chord_kernel(const DevPlan P, const Swe
 // grids and move on as queues run dry.  The grid's plan and arguments are
 // copied into shared memory while the CTA works on it.
 template <typename T>
-__global__ void __launch_bounds__(BS, 2)
+__global__ void __launch_bounds__(BS, GS2G_CHORD_CTAS_PER_SM)
     chord_kernel_multi(const GridEntry* __restrict__ grids, int n_grids, unsigned long long* phase_cycles) {
   __shared__ __align__(16) GridEntry s_grid;
   PhaseProf prof;
