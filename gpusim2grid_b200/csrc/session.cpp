@@ -14,13 +14,19 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <pthread.h>
 
 #include "nr_kernel.cuh"
 #include "plan.hpp"
@@ -816,6 +822,93 @@ int gs2g_set_contingencies(gs2g_session* s, int n_rows, const int* ptr, const in
 
 extern "C++" {
 namespace {
+// Host copies of large results: the destination is usually fresh pageable
+// memory (a new numpy array), whose first touch costs a page fault per 4 KB,
+// so one thread copies at a few GB/s while the DMA delivers tens.  The copy
+// out of the pinned staging chunk is split over a small pool of persistent
+// threads (created on first use, shared by all sessions).
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool;
+    return pool;
+  }
+  // f(begin, end) over [0, n) in up to size() + 1 parts of at least `grain`
+  // items each; the caller runs the first part
+  void parallel_for(size_t n, size_t grain, const std::function<void(size_t, size_t)>& f) {
+    if (forked_) {  // a forked child has the pool object but not its threads
+      f(0, n);
+      return;
+    }
+    const int parts = (int)std::min<size_t>(workers_.size() + 1, std::max<size_t>(1, n / std::max<size_t>(grain, 1)));
+    if (parts <= 1) {
+      f(0, n);
+      return;
+    }
+    const size_t step = (n + parts - 1) / parts;
+    {
+      std::unique_lock<std::mutex> lk(m_);
+      for (int k = 1; k < parts; ++k) {
+        const size_t b = (size_t)k * step, e = std::min(n, b + step);
+        if (b < e) {
+          tasks_.push_back([&f, b, e] { f(b, e); });
+          ++pending_;
+        }
+      }
+    }
+    cv_.notify_all();
+    f(0, std::min(n, step));
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+  }
+  // memcpy(dst, src, n), split by 1 MB parts
+  void copy(void* dst, const void* src, size_t n) {
+    parallel_for(n, size_t(1) << 20, [=](size_t b, size_t e) {
+      std::memcpy(static_cast<char*>(dst) + b, static_cast<const char*>(src) + b, e - b);
+    });
+  }
+
+ private:
+  CopyPool() {
+    pthread_atfork(nullptr, nullptr, [] { forked_ = true; });
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int n = (int)std::min<unsigned>(7, hw > 1 ? hw - 1 : 0);
+    for (int i = 0; i < n; ++i) workers_.emplace_back([this] { run(); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  void run() {
+    for (;;) {
+      std::function<void()> f;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+        if (stop_ && tasks_.empty()) return;
+        f = std::move(tasks_.back());
+        tasks_.pop_back();
+      }
+      f();
+      {
+        std::lock_guard<std::mutex> lk(m_);
+        if (--pending_ == 0) done_.notify_all();
+      }
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::vector<std::function<void()>> tasks_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  int pending_ = 0;
+  bool stop_ = false;
+  static inline bool forked_ = false;
+};
+
 constexpr size_t kStageChunk = size_t(8) << 20;
 // the session's pinned double buffer for large copies, made on first use
 void ensure_stage(const gs2g_session* s) {
@@ -860,10 +953,12 @@ int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const d
     const double inv = 1.0 / sn_mva;
     h2d_staged(s, s->d_sbus_rows.p, m * 2 * sizeof(double), [&](double* dst, size_t off, size_t len) {
       const size_t q0 = off / (2 * sizeof(double)), nq = len / (2 * sizeof(double));
-      for (size_t q = 0; q < nq; ++q) {
-        dst[2 * q] = p_mw[q0 + q] * inv;
-        dst[2 * q + 1] = q_mvar[q0 + q] * inv;
-      }
+      CopyPool::get().parallel_for(nq, size_t(1) << 16, [&](size_t b, size_t e) {
+        for (size_t q = b; q < e; ++q) {
+          dst[2 * q] = p_mw[q0 + q] * inv;
+          dst[2 * q + 1] = q_mvar[q0 + q] * inv;
+        }
+      });
     });
   }
   s->n_inj = n_rows;
@@ -1301,7 +1396,7 @@ int gs2g_n_rows(const gs2g_session* s) { return s ? s->last_rows_run : 0; }
 namespace {
 // Large device-to-host copies into the caller's (pageable) memory go through
 // a pinned double buffer of the session: chunk i+1 is in flight while chunk
-// i is copied out on the host.
+// i is copied out on the host (by the copy pool).
 void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes) {
   constexpr size_t kChunk = kStageChunk;
   if (bytes < 2 * kChunk) {
@@ -1322,7 +1417,7 @@ void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes)
     if (i + 1 < nch) issue(i + 1);  // into the buffer chunk i-1 left, already copied out
     ck(cudaEventSynchronize(s->ev_stage[i & 1]), "read results");
     const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
-    std::memcpy(static_cast<char*>(dst) + off, buf[i & 1], len);
+    CopyPool::get().copy(static_cast<char*>(dst) + off, buf[i & 1], len);
   }
 }
 }  // namespace
