@@ -63,7 +63,7 @@ METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e
 # "source", with that step's counts of LUs, Newton steps and steps on the
 # shared base factor (same workload and command line as the default run)
 NCU_TRAFFIC = {"n1_sweep_case2000_synth": {
-    "dram_bytes": 2.0939e9 + 1.8876e9, "lus": 129, "steps": 13780, "chord_steps": 13633,
+    "dram_bytes": 3.2149e9 + 0.0063e9, "lus": 14, "steps": 12291, "chord_steps": 12277,
     "source": "profiles/chord_kernel_full_n1_case2000_learned.md (20k training rows; same sweep workload)"}}
 
 
