@@ -445,6 +445,15 @@ class InjectionSweepGPU(_BatchSweep):
         p, q, sn = self._inj
         return (p + 1j * q) / sn, None, self._n_scen
 
+    def set_injections_from_elements(self, load_p, load_q, gen_p):
+        """Per-element injections (lightsim2grid's batch API,
+        ``injection_sweep/gpu_facade.py:394``).  Mapping loads and generators
+        to buses needs a lightsim2grid grid; a facade built from an array
+        tuple has none, so this raises RuntimeError, as the reference does in
+        that mode."""
+        raise RuntimeError("set_injections_from_elements() needs a lightsim2grid grid; explicit-array (tuple) "
+                           "mode has no loads/generators to read. Use set_injections(p_mw, q_mvar, sn_mva) instead.")
+
     @property
     def n_scenarios(self):
         return self._n_scen

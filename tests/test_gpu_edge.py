@@ -129,3 +129,11 @@ def test_islanding_flags_every_single_and_some_double_outages(g118):
     for r, ids in enumerate(rows):
         islanded = bool(O.islands(g118.n_bus, g118.branch_from, g118.branch_to, ids))
         assert (st[r] == RowStatus.NOT_SIMULATED) == islanded, (r, ids)
+
+
+def test_set_injections_from_elements_needs_a_grid_object(g118):
+    """Array-tuple mode has no loads or generators to map: RuntimeError, as in
+    the reference (``injection_sweep/gpu_facade.py:394``)."""
+    sw = InjectionSweepGPU(g118.as_tuple(), init_from_n_powerflow=False)
+    with pytest.raises(RuntimeError, match="lightsim2grid grid"):
+        sw.set_injections_from_elements(np.zeros((1, 3)), np.zeros((1, 3)), np.zeros((1, 2)))
