@@ -86,6 +86,7 @@ struct ChordSlot {
   int comp;   // outage compensation set up
   int act;    // this round: 1 solve, 2 converged, 3 diverged, 4 budget spent, 5 hand off
   int nb;     // Broyden steps stored
+  int from_base;  // began from the rescue voltage (start selection): no rescue
   double nrm, last;
 };
 
@@ -370,7 +371,7 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   if (sl.act == 5) {
     if (tid == 0) {
       a.iters_out[row] = sl.it;
-      a.handoff[atomicAdd(a.n_handoff, 1)] = a.handoff_base + row;
+      a.handoff[atomicAdd(a.n_handoff, 1)] = (a.handoff_base + row) | (sl.from_base ? NO_RESCUE_BIT : 0);
     }
     __syncthreads();
     return;
@@ -468,6 +469,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
           sl[s].comp = 0;
           sl[s].act = 0;
           sl[s].nb = 0;
+          sl[s].from_base = 0;
           sl[s].last = INFINITY;
         }
         const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
@@ -497,7 +499,10 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
                             : mismatch_norm(P, ed, Y, va, sb, s_red);
       const bool sw = !(s_nrm[s] < na) && isfinite(na);
       __syncthreads();
-      if (tid == 0) sl[s].fresh = 0;
+      if (tid == 0) {
+        sl[s].fresh = 0;
+        if (sw) sl[s].from_base = a.alt_v0 == a.rescue_v0;
+      }
       if (sw) {
         for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = va[i];
         if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
@@ -509,10 +514,10 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
 
     // ---- per-slot decisions (the single-row kernel's, in its order) ---------
     if (tid == 0) {
-      const bool rescue = a.rescue_v0 != nullptr;
       for (int s = 0; s < CK; ++s) {
         if (!(active >> s & 1)) continue;
         ChordSlot& q = sl[s];
+        const bool rescue = a.rescue_v0 != nullptr && !q.from_base;
         q.nrm = s_nrm[s];
         if (!isfinite(q.nrm)) q.act = rescue ? 5 : 3;
         else if (q.nrm < a.tol) q.act = 2;

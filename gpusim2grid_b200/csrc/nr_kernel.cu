@@ -824,10 +824,18 @@ __device__ __noinline__ void skip_row_outputs(const SweepArgs a, const int row, 
 // voltage, edits, mismatch / Jacobian / factorization / solves / update
 // until the row converges, diverges or uses its budget (with the optional
 // rescue attempt), then the row's outputs.  ws: the CTA's workspace.
+// A row id with this bit set (rows handed off by the chord sweep) is not
+// rescued: it already began from the rescue voltage.
+constexpr int NO_RESCUE_BIT = 1 << 30;
+
 template <typename T>
-__device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, const int row, char* ws,
+__device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, const int row_arg, char* ws,
                                           const RowShared<T>& sh, PhaseProf& prof) {
   const int tid = threadIdx.x;
+  const int row = row_arg & ~NO_RESCUE_BIT;
+  // a row that began from the rescue voltage (the base V, chosen by start
+  // selection) is not restarted from it
+  bool from_rescue_v = (row_arg & NO_RESCUE_BIT) != 0;
   const WsLayout L = ws_layout<T>(P);
   double2* V = reinterpret_cast<double2*>(ws + L.V);
   double2* I = reinterpret_cast<double2*>(ws + L.I);
@@ -942,6 +950,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
         if (!(nrm < na) && isfinite(na)) {
           for (int i = tid; i < n; i += BS) V[i] = va[i];
           if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
+          from_rescue_v = a.alt_v0 == a.rescue_v0;
           __syncthreads();
           continue;  // mismatch again at the new start
         }
@@ -1090,7 +1099,7 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     }
     it_total += it;
     // status and attempt are block-uniform: the whole CTA restarts or leaves
-    if (status == ROW_CONVERGED || a.fixed_iters || a.rescue_v0 == nullptr || attempt > 0) break;
+    if (status == ROW_CONVERGED || a.fixed_iters || a.rescue_v0 == nullptr || attempt > 0 || from_rescue_v) break;
     const double2* rv = reinterpret_cast<const double2*>(a.rescue_v0);
     for (int i = tid; i < n; i += BS) V[i] = rv[i];
     if (tid == 0 && a.n_rescued != nullptr) atomicAdd(a.n_rescued, 1);
@@ -1185,7 +1194,9 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
       prof.flush(phase_cycles);
       return;
     }
-    const int row = row_list != nullptr ? row_list[q] : q;
+    const int entry = row_list != nullptr ? row_list[q] : q;
+    const int flag = entry & NO_RESCUE_BIT;
+    const int row = entry & ~NO_RESCUE_BIT;
     int g = 0;
     while (g + 1 < n_grids && row >= row_begin[g + 1]) ++g;
     if (g != cur) {
@@ -1196,7 +1207,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
       cur = g;
     }
     const int lr = row - row_begin[g];
-    solve_row<T>(s_grid.P, s_grid.a, s_grid.a.row_map != nullptr ? s_grid.a.row_map[lr] : lr, ws, sh, prof);
+    solve_row<T>(s_grid.P, s_grid.a, (s_grid.a.row_map != nullptr ? s_grid.a.row_map[lr] : lr) | flag, ws, sh, prof);
   }
 }
 
