@@ -70,7 +70,7 @@ NCU_TRAFFIC = {"n1_sweep_case2000_synth": {
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
@@ -164,15 +164,45 @@ def cpu_baseline(g, trips, p, q, n_rows_sample, cores=None):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock, max clock and clock-event reasons of the bench's GPU during
+    the timed region (read-only queries).  NVML every 10 ms when the bindings
+    load -- the device found by its PCI bus id, so CUDA_VISIBLE_DEVICES does
+    not shift it -- else nvidia-smi every 0.2 s."""
+
     def __init__(self, index=0):
         self.index = index
         self.samples = []
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            self._nvml = (pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus))
+        except Exception:
+            self._nvml = None
 
     def start(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t = threading.Thread(target=self._run_nvml if self._nvml else self._run, daemon=True)
         self._t.start()
+
+    def _run_nvml(self):
+        nv, h = self._nvml
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append([str(self.index), str(sm), str(mx), "",
+                                     *["Active" if r & b else "Not Active" for b in bits]])
+            except Exception:
+                pass
+            self._stop.wait(0.01)
 
     def _run(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
