@@ -45,18 +45,26 @@
 #define GS2G_CHORD_CTAS_PER_SM 3
 #endif
 
-constexpr int CK = 4;      // rows per CTA
+// Rows per CTA (build-time).  8 was measured against 4 on the 2000- and
+// 6500-bus sweeps: 10-16 % slower at 2 CTAs per SM (128 registers) and
+// 9-16 % slower at 3 (80 registers, more spills); 4 rows at 3 CTAs per SM
+// is the default.
+#ifndef GS2G_CHORD_ROWS
+#define GS2G_CHORD_ROWS 4
+#endif
+constexpr int CK = GS2G_CHORD_ROWS;  // rows per CTA
 constexpr int CB_MAX = 10;  // Broyden steps kept per row (the memory restarts beyond)
 
+// the CK right-hand sides of one unknown, loaded as one vector (or two)
 template <typename T>
-struct alignas(4 * sizeof(T)) Vec4 {
-  T v[4];
+struct alignas(16) Vec4 {
+  T v[CK];
 };
 
 template <typename T>
 __device__ __forceinline__ void fms4(Vec4<T>& acc, T a, const Vec4<T>& b) {
 #pragma unroll
-  for (int s = 0; s < 4; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
+  for (int s = 0; s < CK; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
 }
 
 // Workspace of one chord CTA: V [n] and F [dim] per slot, the interleaved
@@ -91,10 +99,10 @@ struct ChordSlot {
 };
 
 // NaN-sticky block max of four values at once (one pair of barriers).
-__device__ __forceinline__ void block_nanmax4(double v[4], double* s_red4) {
+__device__ __forceinline__ void block_nanmax4(double v[CK], double* s_red4) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < CK; ++s) {
     for (int o = 16; o > 0; o >>= 1) {
       const double w = __shfl_xor_sync(0xffffffffu, v[s], o);
       v[s] = (isnan(w) || isnan(v[s])) ? NAN : fmax(v[s], w);
@@ -102,13 +110,13 @@ __device__ __forceinline__ void block_nanmax4(double v[4], double* s_red4) {
   }
   if (lane == 0)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) s_red4[warp * 4 + s] = v[s];
+    for (int s = 0; s < CK; ++s) s_red4[warp * CK + s] = v[s];
   __syncthreads();
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < CK; ++s) {
     double r = s_red4[s];
     for (int w = 1; w < NWARP; ++w) {
-      const double x = s_red4[w * 4 + s];
+      const double x = s_red4[w * CK + s];
       r = (isnan(x) || isnan(r)) ? NAN : fmax(r, x);
     }
     v[s] = r;
@@ -117,19 +125,19 @@ __device__ __forceinline__ void block_nanmax4(double v[4], double* s_red4) {
 }
 
 // Block sum of four values at once (one pair of barriers).
-__device__ __forceinline__ void block_sum4(double v[4], double* s_red4) {
+__device__ __forceinline__ void block_sum4(double v[CK], double* s_red4) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int s = 0; s < 4; ++s)
+  for (int s = 0; s < CK; ++s)
     for (int o = 16; o > 0; o >>= 1) v[s] += __shfl_xor_sync(0xffffffffu, v[s], o);
   if (lane == 0)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) s_red4[warp * 4 + s] = v[s];
+    for (int s = 0; s < CK; ++s) s_red4[warp * CK + s] = v[s];
   __syncthreads();
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < CK; ++s) {
     double r = 0.0;
-    for (int w = 0; w < NWARP; ++w) r += s_red4[w * 4 + s];
+    for (int w = 0; w < NWARP; ++w) r += s_red4[w * CK + s];
     v[s] = r;
   }
   __syncthreads();
@@ -153,7 +161,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
   }
   auto step = [&](int s, int j) { return St + ((int64_t)s * CB_MAX + j) * dim; };
   for (int j = 0; j + 1 < maxnb; ++j) {
-    double d[CK] = {0.0, 0.0, 0.0, 0.0};
+    double d[CK] = {};
     for (int i = tid; i < dim; i += BS) {
       const Vec4<T> z = y[i];
 #pragma unroll
@@ -178,7 +186,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
   }
   // s_{nb} = z / (1 - (s_{nb-1} . z) / |s_{nb-1}|^2); a vanishing denominator
   // (the update breaks down) restarts the memory with the plain step z
-  double d[CK] = {0.0, 0.0, 0.0, 0.0};
+  double d[CK] = {};
   if (maxnb > 0) {
     for (int i = tid; i < dim; i += BS) {
       const Vec4<T> z = y[i];
@@ -199,7 +207,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
       else nb[s] = 0;
     }
   }
-  double q[CK] = {0.0, 0.0, 0.0, 0.0};
+  double q[CK] = {};
   for (int i = tid; i < dim; i += BS) {
     Vec4<T> z = y[i];
 #pragma unroll
@@ -236,7 +244,7 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
 #pragma unroll
   for (int s = 0; s < CK; ++s)
     sb[s] = reinterpret_cast<const double2*>(a.sbus) + (int64_t)(sl[s].row < 0 ? 0 : sl[s].row) * a.sbus_stride;
-  double lmax[CK] = {0.0, 0.0, 0.0, 0.0};
+  double lmax[CK] = {};
   for (int i = threadIdx.x; i < n; i += BS) {
     double2 acc[CK];
 #pragma unroll
@@ -324,7 +332,7 @@ __device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ 
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-      for (int s = 0; s < 4; ++s) acc[u].v[s] = T(0);
+      for (int s = 0; s < CK; ++s) acc[u].v[s] = T(0);
     const int nr = min(4, (nt - r0 - tid + BS - 1) / BS);  // rows of this thread in the pass (may be <= 0)
     const T* base = Sinv + r0 + tid;
 #pragma unroll 2
@@ -352,7 +360,7 @@ __device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict_
       for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms4(acc, fHV[P.bw_pos[q]], y[P.bw_row[q]]);
       const T d = fHV[k];
 #pragma unroll
-      for (int s = 0; s < 4; ++s) acc.v[s] = acc.v[s] / d;
+      for (int s = 0; s < CK; ++s) acc.v[s] = acc.v[s] / d;
       y[k] = acc;
     }
     __syncthreads();
@@ -399,7 +407,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   __shared__ int s_ek[CK][MAX_EDITS];
   __shared__ double2 s_ev[CK][MAX_EDITS];
   __shared__ double s_red[NWARP];
-  __shared__ double s_red4[NWARP * 4];
+  __shared__ double s_red4[NWARP * CK];
   __shared__ double s_nrm[CK];
   __shared__ int s_cr[CK][1 + MAX_COMP];
   __shared__ double s_cB[CK][MAX_COMP * MAX_COMP];
