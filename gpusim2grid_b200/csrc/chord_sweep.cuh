@@ -57,12 +57,12 @@ constexpr int CB_MAX = 10;  // Broyden steps kept per row (the memory restarts b
 
 // the CK right-hand sides of one unknown, loaded as one vector (or two)
 template <typename T>
-struct alignas(16) Vec4 {
+struct alignas(16) SlotVec {
   T v[CK];
 };
 
 template <typename T>
-__device__ __forceinline__ void fms4(Vec4<T>& acc, T a, const Vec4<T>& b) {
+__device__ __forceinline__ void fms_slots(SlotVec<T>& acc, T a, const SlotVec<T>& b) {
 #pragma unroll
   for (int s = 0; s < CK; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
 }
@@ -79,7 +79,7 @@ __host__ __device__ ChordWs chord_ws(const DevPlan& P) {
   int64_t o = 0;
   w.V = o; o = align256(o + (int64_t)CK * P.n_bus * 16);
   w.F = o; o = align256(o + (int64_t)CK * P.dim * 8);
-  w.y = o; o = align256(o + (int64_t)P.dim * sizeof(Vec4<T>));
+  w.y = o; o = align256(o + (int64_t)P.dim * sizeof(SlotVec<T>));
   w.S = o; o = align256(o + (int64_t)CK * CB_MAX * P.dim * sizeof(T));
   w.total = o;
   return w;
@@ -98,8 +98,8 @@ struct ChordSlot {
   double nrm, last;
 };
 
-// NaN-sticky block max of four values at once (one pair of barriers).
-__device__ __forceinline__ void block_nanmax4(double v[CK], double* s_red4) {
+// NaN-sticky block max of one value per slot at once (one pair of barriers).
+__device__ __forceinline__ void block_nanmax_slots(double v[CK], double* s_red_slots) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int s = 0; s < CK; ++s) {
@@ -110,13 +110,13 @@ __device__ __forceinline__ void block_nanmax4(double v[CK], double* s_red4) {
   }
   if (lane == 0)
 #pragma unroll
-    for (int s = 0; s < CK; ++s) s_red4[warp * CK + s] = v[s];
+    for (int s = 0; s < CK; ++s) s_red_slots[warp * CK + s] = v[s];
   __syncthreads();
 #pragma unroll
   for (int s = 0; s < CK; ++s) {
-    double r = s_red4[s];
+    double r = s_red_slots[s];
     for (int w = 1; w < NWARP; ++w) {
-      const double x = s_red4[w * CK + s];
+      const double x = s_red_slots[w * CK + s];
       r = (isnan(x) || isnan(r)) ? NAN : fmax(r, x);
     }
     v[s] = r;
@@ -124,20 +124,20 @@ __device__ __forceinline__ void block_nanmax4(double v[CK], double* s_red4) {
   __syncthreads();
 }
 
-// Block sum of four values at once (one pair of barriers).
-__device__ __forceinline__ void block_sum4(double v[CK], double* s_red4) {
+// Block sum of one value per slot at once (one pair of barriers).
+__device__ __forceinline__ void block_sum_slots(double v[CK], double* s_red_slots) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int s = 0; s < CK; ++s)
     for (int o = 16; o > 0; o >>= 1) v[s] += __shfl_xor_sync(0xffffffffu, v[s], o);
   if (lane == 0)
 #pragma unroll
-    for (int s = 0; s < CK; ++s) s_red4[warp * CK + s] = v[s];
+    for (int s = 0; s < CK; ++s) s_red_slots[warp * CK + s] = v[s];
   __syncthreads();
 #pragma unroll
   for (int s = 0; s < CK; ++s) {
     double r = 0.0;
-    for (int w = 0; w < NWARP; ++w) r += s_red4[w * CK + s];
+    for (int w = 0; w < NWARP; ++w) r += s_red_slots[w * CK + s];
     v[s] = r;
   }
   __syncthreads();
@@ -148,8 +148,8 @@ __device__ __forceinline__ void block_sum4(double v[CK], double* s_red4) {
 // next Broyden step (with its squared norm).  St: the CTA's steps
 // [CK][CB_MAX][dim]; s_ss: their squared norms.
 template <typename T>
-__device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, ChordSlot* sl, Vec4<T>* y, T* St,
-                                           double (*s_ss)[CB_MAX], double* s_red4) {
+__device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, ChordSlot* sl, SlotVec<T>* y, T* St,
+                                           double (*s_ss)[CB_MAX], double* s_red_slots) {
   const int tid = threadIdx.x;
   int nb[CK];
   int maxnb = 0;
@@ -163,12 +163,12 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
   for (int j = 0; j + 1 < maxnb; ++j) {
     double d[CK] = {};
     for (int i = tid; i < dim; i += BS) {
-      const Vec4<T> z = y[i];
+      const SlotVec<T> z = y[i];
 #pragma unroll
       for (int s = 0; s < CK; ++s)
         if (j + 1 < nb[s]) d[s] += (double)step(s, j)[i] * (double)z.v[s];
     }
-    block_sum4(d, s_red4);
+    block_sum_slots(d, s_red_slots);
     T cf[CK];
 #pragma unroll
     for (int s = 0; s < CK; ++s) {
@@ -176,7 +176,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
       cf[s] = (j + 1 < nb[s] && ss > 0.0) ? (T)(d[s] / ss) : T(0);
     }
     for (int i = tid; i < dim; i += BS) {
-      Vec4<T> z = y[i];
+      SlotVec<T> z = y[i];
 #pragma unroll
       for (int s = 0; s < CK; ++s)
         if (j + 1 < nb[s]) z.v[s] = fma(cf[s], step(s, j + 1)[i], z.v[s]);
@@ -189,12 +189,12 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
   double d[CK] = {};
   if (maxnb > 0) {
     for (int i = tid; i < dim; i += BS) {
-      const Vec4<T> z = y[i];
+      const SlotVec<T> z = y[i];
 #pragma unroll
       for (int s = 0; s < CK; ++s)
         if (nb[s] > 0) d[s] += (double)step(s, nb[s] - 1)[i] * (double)z.v[s];
     }
-    block_sum4(d, s_red4);
+    block_sum_slots(d, s_red_slots);
   }
   T sc[CK];
 #pragma unroll
@@ -209,7 +209,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
   }
   double q[CK] = {};
   for (int i = tid; i < dim; i += BS) {
-    Vec4<T> z = y[i];
+    SlotVec<T> z = y[i];
 #pragma unroll
     for (int s = 0; s < CK; ++s) {
       if (!(mask >> s & 1)) continue;
@@ -219,7 +219,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
     }
     y[i] = z;
   }
-  block_sum4(q, s_red4);
+  block_sum_slots(q, s_red_slots);
   if (tid == 0)
 #pragma unroll
     for (int s = 0; s < CK; ++s)
@@ -237,7 +237,7 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
 __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, const unsigned mask,
                                             const ChordSlot* sl, const int* s_ne, const int (*s_ek)[MAX_EDITS],
                                             const double2 (*s_ev)[MAX_EDITS], const double2* Vs, double* Fs,
-                                            double* nrm_out, double* s_red4) {
+                                            double* nrm_out, double* s_red_slots) {
   const int n = P.n_bus;
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const double2* sb[CK];
@@ -283,7 +283,7 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
       }
     }
   }
-  block_nanmax4(lmax, s_red4);
+  block_nanmax_slots(lmax, s_red_slots);
   if (threadIdx.x == 0)
 #pragma unroll
     for (int s = 0; s < CK; ++s)
@@ -293,12 +293,12 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
 
 // Forward over the head levels, all slots at once.
 template <typename T>
-__device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+__device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
   for (int lv = 0; lv < P.n_levels; ++lv) {
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int i = P.lev_piv[q0];
-      Vec4<T> acc = y[i];
-      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms4(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+      SlotVec<T> acc = y[i];
+      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
       y[i] = acc;
     }
     __syncthreads();
@@ -307,11 +307,11 @@ __device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict_
 
 // The tail rows against the head.
 template <typename T>
-__device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+__device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
   for (int ti = threadIdx.x; ti < P.nt; ti += BS) {
     const int i = P.p + ti;
-    Vec4<T> acc = y[i];
-    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms4(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+    SlotVec<T> acc = y[i];
+    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
     y[i] = acc;
   }
   __syncthreads();
@@ -322,13 +322,13 @@ __device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict_
 // Each thread owns up to four tail rows per pass; for each column a warp
 // reads 32 consecutive entries.
 template <typename T>
-__device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ Minv, Vec4<T>* y, Vec4<T>* ys) {
+__device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ Minv, SlotVec<T>* y, SlotVec<T>* ys) {
   const int tid = threadIdx.x, nt = P.nt;
   for (int i = tid; i < nt; i += BS) ys[i] = y[P.p + i];
   __syncthreads();
   const T* Sinv = Minv + (int64_t)P.p * P.dim + P.p;
   for (int r0 = 0; r0 < nt; r0 += 4 * BS) {
-    Vec4<T> acc[4];
+    SlotVec<T> acc[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -337,11 +337,11 @@ __device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ 
     const T* base = Sinv + r0 + tid;
 #pragma unroll 2
     for (int j = 0; j < nt; ++j) {
-      const Vec4<T> yj = ys[j];
+      const SlotVec<T> yj = ys[j];
       const T* col = base + (int64_t)j * P.dim;
 #pragma unroll
       for (int u = 0; u < 4; ++u)
-        if (u < nr) fms4(acc[u], -col[u * BS], yj);
+        if (u < nr) fms_slots(acc[u], -col[u * BS], yj);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
@@ -352,12 +352,12 @@ __device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ 
 
 // Backward over the head levels.
 template <typename T>
-__device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict__ fHV, Vec4<T>* y) {
+__device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
   for (int lv = P.n_levels - 1; lv >= 0; --lv) {
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int k = P.lev_piv[q0];
-      Vec4<T> acc = y[k];
-      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms4(acc, fHV[P.bw_pos[q]], y[P.bw_row[q]]);
+      SlotVec<T> acc = y[k];
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms_slots(acc, fHV[P.bw_pos[q]], y[P.bw_row[q]]);
       const T d = fHV[k];
 #pragma unroll
       for (int s = 0; s < CK; ++s) acc.v[s] = acc.v[s] / d;
@@ -407,7 +407,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   __shared__ int s_ek[CK][MAX_EDITS];
   __shared__ double2 s_ev[CK][MAX_EDITS];
   __shared__ double s_red[NWARP];
-  __shared__ double s_red4[NWARP * CK];
+  __shared__ double s_red_slots[NWARP * CK];
   __shared__ double s_nrm[CK];
   __shared__ int s_cr[CK][1 + MAX_COMP];
   __shared__ double s_cB[CK][MAX_COMP * MAX_COMP];
@@ -421,9 +421,9 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   double2* Vs = reinterpret_cast<double2*>(ws + L.V);
   double* Fs = reinterpret_cast<double*>(ws + L.F);
-  Vec4<T>* y = reinterpret_cast<Vec4<T>*>(ws + L.y);
+  SlotVec<T>* y = reinterpret_cast<SlotVec<T>*>(ws + L.y);
   T* St = reinterpret_cast<T*>(ws + L.S);
-  Vec4<T>* ys = reinterpret_cast<Vec4<T>*>(smem_raw);
+  SlotVec<T>* ys = reinterpret_cast<SlotVec<T>*>(smem_raw);
   const WsLayout BL = ws_layout<T>(P);  // layout of the base factor's workspace
   const T* fHV = reinterpret_cast<const T*>(a.base_ws + BL.HV);
   const T* Minv = reinterpret_cast<const T*>(a.base_inv);
@@ -496,7 +496,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     if (active == 0) break;
 
     // ---- mismatch of every slot, start selection for new rows --------------
-    chord_mismatch(P, a, active, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red4);
+    chord_mismatch(P, a, active, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red_slots);
     for (int s = 0; s < CK; ++s) {
       if (!(active >> s & 1) || !sl[s].fresh) continue;
       const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
@@ -515,7 +515,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = va[i];
         if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
         __syncthreads();
-        chord_mismatch(P, a, 1u << s, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red4);
+        chord_mismatch(P, a, 1u << s, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red_slots);
       }
     }
     prof.mark(PH_MISMATCH);
@@ -551,7 +551,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
 
     // ---- one solve on the base factor for every remaining slot -------------
     for (int i = tid; i < P.dim; i += BS) {
-      Vec4<T> r;
+      SlotVec<T> r;
 #pragma unroll
       for (int s = 0; s < CK; ++s) r.v[s] = (solve >> s & 1) ? (T)Fs[(int64_t)s * P.dim + i] : T(0);
       y[i] = r;
@@ -566,15 +566,15 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     chord_head_bw<T>(P, fHV, y);
     for (int s = 0; s < CK; ++s)
       if ((solve >> s & 1) && sl[s].comp) apply_compensation<T>(P.dim, &y[0].v[s], Minv, shs(s), CK);
-    if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red4);
+    if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots);
     prof.mark(PH_SOLVE_BACK);
 
     // ---- V update (FP64, polar) ---------------------------------------------
     for (int i = tid; i < n; i += BS) {
       const int fp = P.fP[i], fq = P.fQ[i];
       if (fp < 0 && fq < 0) continue;
-      const Vec4<T> ya = fp >= 0 ? y[fp] : Vec4<T>{};
-      const Vec4<T> ym = fq >= 0 ? y[fq] : Vec4<T>{};
+      const SlotVec<T> ya = fp >= 0 ? y[fp] : SlotVec<T>{};
+      const SlotVec<T> ym = fq >= 0 ? y[fq] : SlotVec<T>{};
 #pragma unroll
       for (int s = 0; s < CK; ++s) {
         if (!(solve >> s & 1)) continue;
@@ -632,5 +632,5 @@ __global__ void __launch_bounds__(BS, GS2G_CHORD_CTAS_PER_SM)
 
 template <typename T>
 int chord_smem_bytes(const DevPlan& P) {
-  return (int)(sizeof(Vec4<T>) * (size_t)(P.nt > 0 ? P.nt : 1));
+  return (int)(sizeof(SlotVec<T>) * (size_t)(P.nt > 0 ? P.nt : 1));
 }
