@@ -291,14 +291,15 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
   __syncthreads();
 }
 
-// Forward over the head levels, all slots at once.
+// Forward over the head levels, all slots at once.  fwv: the factor's
+// values in solve order (one sequential stream beside fw_col).
 template <typename T>
-__device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
+__device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict__ fwv, SlotVec<T>* y) {
   for (int lv = 0; lv < P.n_levels; ++lv) {
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int i = P.lev_piv[q0];
       SlotVec<T> acc = y[i];
-      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+      for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fwv[q], y[P.fw_col[q]]);
       y[i] = acc;
     }
     __syncthreads();
@@ -307,11 +308,11 @@ __device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict_
 
 // The tail rows against the head.
 template <typename T>
-__device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
+__device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict__ fwv, SlotVec<T>* y) {
   for (int ti = threadIdx.x; ti < P.nt; ti += BS) {
     const int i = P.p + ti;
     SlotVec<T> acc = y[i];
-    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fHV[P.fw_pos[q]], y[P.fw_col[q]]);
+    for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fwv[q], y[P.fw_col[q]]);
     y[i] = acc;
   }
   __syncthreads();
@@ -350,14 +351,16 @@ __device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ 
   __syncthreads();
 }
 
-// Backward over the head levels.
+// Backward over the head levels (bwv: values in solve order, fHV for the
+// pivots).
 template <typename T>
-__device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict__ fHV, SlotVec<T>* y) {
+__device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict__ fHV, const T* __restrict__ bwv,
+                                           SlotVec<T>* y) {
   for (int lv = P.n_levels - 1; lv >= 0; --lv) {
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int k = P.lev_piv[q0];
       SlotVec<T> acc = y[k];
-      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms_slots(acc, fHV[P.bw_pos[q]], y[P.bw_row[q]]);
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms_slots(acc, bwv[q], y[P.bw_row[q]]);
       const T d = fHV[k];
 #pragma unroll
       for (int s = 0; s < CK; ++s) acc.v[s] = acc.v[s] / d;
@@ -426,6 +429,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   SlotVec<T>* ys = reinterpret_cast<SlotVec<T>*>(smem_raw);
   const WsLayout BL = ws_layout<T>(P);  // layout of the base factor's workspace
   const T* fHV = reinterpret_cast<const T*>(a.base_ws + BL.HV);
+  const T* fwv = reinterpret_cast<const T*>(a.base_fwv);
+  const T* bwv = reinterpret_cast<const T*>(a.base_bwv);
   const T* Minv = reinterpret_cast<const T*>(a.base_inv);
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
   const double2* Vbase = reinterpret_cast<const double2*>(a.base_v);
@@ -557,13 +562,13 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
       y[i] = r;
     }
     __syncthreads();
-    chord_head_fw<T>(P, fHV, y);
+    chord_head_fw<T>(P, fwv, y);
     prof.mark(PH_SOLVE);
-    chord_tail_fw<T>(P, fHV, y);
+    chord_tail_fw<T>(P, fwv, y);
     prof.mark(PH_SOLVE_TAIL);
     if (P.nt > 0) chord_dense<T>(P, Minv, y, ys);
     prof.mark(PH_SOLVE_DENSE);
-    chord_head_bw<T>(P, fHV, y);
+    chord_head_bw<T>(P, fHV, bwv, y);
     for (int s = 0; s < CK; ++s)
       if ((solve >> s & 1) && sl[s].comp) apply_compensation<T>(P.dim, &y[0].v[s], Minv, shs(s), CK);
     if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots);

@@ -1224,6 +1224,10 @@ int64_t workspace_bytes(const DevPlan& P, int prec) {
   return prec == 1 ? ws_layout<float>(P).total : ws_layout<double>(P).total;
 }
 
+int64_t workspace_hv_offset(const DevPlan& P, int prec) {
+  return prec == 1 ? ws_layout<float>(P).HV : ws_layout<double>(P).HV;
+}
+
 namespace {
 // Dynamic shared memory above 48 KB needs an opt-in per kernel (per device
 // context); cheap and idempotent, so it is set before every query / launch.
@@ -1300,8 +1304,8 @@ int chord_ctas(const DevPlan& P, int prec, int device) {
 
 int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (n_ctas <= 0 || a.base_ws == nullptr || a.base_inv == nullptr || a.handoff == nullptr ||
-      a.n_handoff == nullptr || a.fixed_iters)
+  if (n_ctas <= 0 || a.base_ws == nullptr || a.base_inv == nullptr || a.base_fwv == nullptr ||
+      a.base_bwv == nullptr || a.handoff == nullptr || a.n_handoff == nullptr || a.fixed_iters)
     return (int)cudaErrorInvalidValue;
   cudaError_t e = prec == 1 ? chord_opt_in<float>(P) : chord_opt_in<double>(P);
   if (e != cudaSuccess) return (int)e;

@@ -102,6 +102,10 @@ struct SweepArgs {
   const char* base_ws;
   const double* base_v;  // complex [n_bus]: the voltage the base factor was taken at
   const char* base_inv;  // [dim x dim] of the sweep's type: column c = M0^-1 e_c (outage compensation)
+  // the base factor's head values in solve order (of the sweep's type):
+  // base_fwv[q] = HV[fw_pos[q]], base_bwv[q] = HV[bw_pos[q]] (nullptr: gather)
+  const char* base_fwv;
+  const char* base_bwv;
   char* inverse_out;     // inverse mode: row r of the launch writes column r of M0^-1 here
   int factor_only;
   // branch flows and limit check when the row leaves (loading_out nullptr: off)
@@ -147,6 +151,8 @@ enum Phase : int {
 
 // Per-CTA workspace bytes for precision `prec` (0: fp64 LU, 1: fp32 LU).
 int64_t workspace_bytes(const DevPlan& P, int prec);
+// byte offset of the head factor values (n_hv of the precision's type) in a workspace
+int64_t workspace_hv_offset(const DevPlan& P, int prec);
 
 // Launch the sweep on `stream` with `n_ctas` CTAs (<= 0: one wave at full
 // occupancy).  Returns the cudaError_t as int.

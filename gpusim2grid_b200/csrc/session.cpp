@@ -119,6 +119,7 @@ struct gs2g_session {
   DevBuf d_row_map;  // rows of gs2g_run_subset
   DevBuf d_base_ws;        // base case's factor for GS2G_REFACTOR_BASE_CHORD
   DevBuf d_base_inv;       // its inverse, column c = M0^-1 e_c (outage compensation)
+  DevBuf d_base_fwv, d_base_bwv;  // its head values in forward / backward solve order
   DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
   DevBuf d_chord_steps;    // Newton steps the last chord sweep took on the base factor
   int chord = 2;           // policy 2: 0 single-row sweep, 1 chord sweep, 2 chord sweep with Broyden steps
@@ -402,6 +403,8 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
     a.base_ws = s->d_base_ws.as<char>();
     a.base_v = s->d_basev.as<double>();
     a.base_inv = s->d_base_inv.as<char>();
+    a.base_fwv = s->d_base_fwv.as<char>();
+    a.base_bwv = s->d_base_bwv.as<char>();
   }
   a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
   a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
@@ -490,6 +493,8 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.base_ws = nullptr;
     a.base_v = nullptr;
     a.base_inv = nullptr;
+    a.base_fwv = nullptr;
+    a.base_bwv = nullptr;
     a.alt_v0 = nullptr;
     a.alt_s = nullptr;
   }
@@ -1154,6 +1159,24 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck((cudaError_t)gs2g::launch_sweep(s->dplan, ai, prec, n_ctas, s->stream), "base inverse launch");
   ck(cudaStreamSynchronize(s->stream), "base factor");
+  // its head values in solve order, so that the chord sweep streams them
+  // beside the column indices instead of gathering them through fw_pos / bw_pos
+  {
+    const int64_t hv_off = gs2g::workspace_hv_offset(s->dplan, prec);
+    const size_t n_hv = (size_t)s->dplan.n_hv;
+    std::vector<char> hv(std::max<size_t>(n_hv, 1) * elem);
+    if (n_hv)
+      ck(cudaMemcpy(hv.data(), s->d_base_ws.as<char>() + hv_off, n_hv * elem, cudaMemcpyDeviceToHost),
+         "read base factor");
+    auto packed = [&](const std::vector<int>& pos, DevBuf& dst) {
+      std::vector<char> v(std::max<size_t>(pos.size(), 1) * elem);
+      for (size_t q = 0; q < pos.size(); ++q) std::memcpy(v.data() + q * elem, hv.data() + (size_t)pos[q] * elem, elem);
+      dst.ensure(v.size());
+      ck(cudaMemcpy(dst.p, v.data(), v.size(), cudaMemcpyHostToDevice), "upload base factor values");
+    };
+    packed(s->plan.fw_pos, s->d_base_fwv);
+    packed(s->plan.bw_pos, s->d_base_bwv);
+  }
   s->base_factor_prec = prec;
 }
 
