@@ -65,8 +65,10 @@ class AcPfGPU:
     def _run(self, V0, max_iter, fixed, tol=None):
         t0 = time.perf_counter()
         self._s.set_start_rows(np.asarray(V0, dtype=np.complex128).reshape(1, -1))
+        # a free-running solve takes the reference's single-solve order: each
+        # step is taken, then the mismatch before it decides convergence
         self._s.run(int(max_iter), float(self.tol if tol is None else tol), bool(fixed), self._prec,
-                    lib.START_ROWS)
+                    lib.START_ROWS, step_then_check=not fixed)
         tm = self._s.timings()
         _, res, st, it = self._s.results()
         return AcPfTimings(converged=int(st[0]) == RowStatus.CONVERGED, nb_iter=int(it[0]),

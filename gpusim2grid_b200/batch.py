@@ -76,9 +76,7 @@ class _BatchSweep:
         self._prec = resolve_precision(precision)
         self.nb_iter = int(nb_iter)
         self.scheduling = resolve_scheduling("chunked" if scheduling is None else scheduling)
-        self.nb_iter_per_round = int(nb_iter_per_round)
-        if self.nb_iter_per_round < 1:
-            raise ValueError("nb_iter_per_round must be >= 1")
+        self.nb_iter_per_round = nb_iter_per_round
         self.tol = default_tol() if tol is None else float(tol)
         self._s = make_session(d, device)
         if init_from_n_powerflow:
@@ -108,6 +106,24 @@ class _BatchSweep:
         self._timings = BatchTimings()
 
     # -------------------------------------------------------------- options
+    @property
+    def nb_iter_per_round(self):
+        """Continuous scheduling: Newton steps every row runs between two
+        convergence tests (k >= 1).  A row runs a multiple of k steps, at
+        least k, also when it starts converged; after each round it leaves
+        DIVERGED (residual not finite), CONVERGED (below tol) or MAX_ITER
+        (steps >= nb_iter), as the reference's rounds
+        (``src/_cpp/contingency/batch_pf_driver.cu:2691-2724``).  Takes
+        effect on the next compute()."""
+        return self._nb_iter_per_round
+
+    @nb_iter_per_round.setter
+    def nb_iter_per_round(self, value):
+        value = int(value)
+        if value < 1:
+            raise ValueError("nb_iter_per_round must be >= 1")
+        self._nb_iter_per_round = value
+
     @property
     def start(self):
         """'base' (the converged base case, default), 'flat' (``Vinit``),
@@ -285,7 +301,7 @@ class _BatchSweep:
             self._warm = dict(predict_ms=(time.perf_counter() - t0) * 1e3)
             ratio, reuse = self._learned_opts
         self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False,
-                    _STRATEGY[self._strategy], ratio, reuse, rescue)
+                    _STRATEGY[self._strategy], ratio, reuse, rescue, self.nb_iter_per_round)
         tm = self._s.timings()
         if self._start == "learned":
             self._warm["n_rescued"] = int(tm["n_rescued"])
@@ -313,7 +329,7 @@ class _BatchSweep:
             return 0.0
         rows = bad.to(torch.int32).cpu().numpy()
         self._s.run_subset(rows, self.nb_iter, self.tol, False, lib.PREC_FP64, lib.START_VINIT, 0.0, n_ctas,
-                           lib.REFACTOR_EVERY)
+                           lib.REFACTOR_EVERY, 0.0, 0, False, self.nb_iter_per_round)
         self._fallback_rows = int(rows.size)
         self._host = None
         return float(self._s.timings()["kernel_ms"])
@@ -503,9 +519,10 @@ def compute_many(sweeps, batch_size=0):
         raise ValueError("compute_many needs at least one sweep")
     f0 = sweeps[0]
     for f in sweeps[1:]:
-        if (f._prec, f.nb_iter, f.tol, f.scheduling, f._strategy) != (f0._prec, f0.nb_iter, f0.tol, f0.scheduling,
-                                                                      f0._strategy):
-            raise ValueError("compute_many: precision, nb_iter, tol, scheduling and strategy must agree")
+        if (f._prec, f.nb_iter, f.tol, f.scheduling, f._strategy, f.nb_iter_per_round) != (
+                f0._prec, f0.nb_iter, f0.tol, f0.scheduling, f0._strategy, f0.nb_iter_per_round):
+            raise ValueError("compute_many: precision, nb_iter, tol, scheduling, strategy and nb_iter_per_round "
+                             "must agree")
     starts = {f._start for f in sweeps}
     if len(starts) != 1:
         raise ValueError("compute_many: every sweep must use the same start")
@@ -523,7 +540,7 @@ def compute_many(sweeps, batch_size=0):
         ratio, reuse = f0._learned_opts
     lib.run_multi([f._s for f in sweeps], f0.nb_iter, f0.tol, f0.scheduling == "chunked", f0._prec, _START[start],
                   0.0, max(int(batch_size), 0), False, _STRATEGY[f0._strategy], ratio, reuse,
-                  start in ("rows", "learned"))
+                  start in ("rows", "learned"), f0.nb_iter_per_round)
     kernel_ms = sweeps[0]._s.timings()["kernel_ms"]
     for f in sweeps:
         f._ran = True

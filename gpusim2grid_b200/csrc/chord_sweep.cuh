@@ -532,9 +532,14 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         ChordSlot& q = sl[s];
         const bool rescue = a.rescue_v0 != nullptr && !q.from_base;
         q.nrm = s_nrm[s];
-        if (!isfinite(q.nrm)) q.act = rescue ? 5 : 3;
-        else if (q.nrm < a.tol) q.act = 2;
-        else if (q.it >= a.max_iter) q.act = rescue ? 5 : 4;
+        // the row is tested only at the end of a round of round_k steps (and
+        // runs its first round whatever its mismatch); between tests a row
+        // whose mismatch is not finite is handed off as well, and the
+        // single-row sweep steps it to the end of its round
+        const bool test = q.it > 0 && q.it % (a.round_k > 1 ? a.round_k : 1) == 0;
+        if (!isfinite(q.nrm)) q.act = (rescue || !test) ? 5 : 3;
+        else if (test && q.nrm < a.tol) q.act = 2;
+        else if (test && q.it >= a.max_iter) q.act = rescue ? 5 : 4;
         else if (!keep_factor(q.nrm, q.last, a.refactor_ratio, q.since, a.max_reuse, q.it, a.max_iter, a.tol))
           q.act = 5;  // needs its own LU
         else q.act = 1;

@@ -780,9 +780,13 @@ __device__ __noinline__ void row_flows(const SweepArgs a, const int row, const d
       ld = 0.f;
       if (!tripped && a.br_rate[l] > 0.0) {
         const double2* yb = reinterpret_cast<const double2*>(a.br_y) + 4 * (int64_t)l;
-        const double2 Vf = V[a.br_from[l]], Vt = V[a.br_to[l]];
-        const double2 Sf = cmul(Vf, conj2(cadd(cmul(yb[0], Vf), cmul(yb[1], Vt))));
-        const double2 St = cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt))));
+        // an open end (negative endpoint) has V = 0 and carries no power
+        // (acpf_nr_kernels.cu:87-183)
+        const int bf = a.br_from[l], bt = a.br_to[l];
+        const double2 zero = make_double2(0.0, 0.0);
+        const double2 Vf = bf >= 0 ? V[bf] : zero, Vt = bt >= 0 ? V[bt] : zero;
+        const double2 Sf = bf >= 0 ? cmul(Vf, conj2(cadd(cmul(yb[0], Vf), cmul(yb[1], Vt)))) : zero;
+        const double2 St = bt >= 0 ? cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt)))) : zero;
         const double r = fmax(hypot(Sf.x, Sf.y), hypot(St.x, St.y)) / a.br_rate[l];
         ld = (float)r;
         lmax = fmax(lmax, r);
@@ -957,14 +961,27 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       }
       prof.mark(PH_MISMATCH);
       const bool finite = isfinite(nrm);
+      // single-solve order: this step is taken whatever the mismatch, and the
+      // mismatch before it decides convergence afterwards
+      bool converged_after_step = false;
       if (a.factor_only) {
         // factor the Jacobian at the start voltage, nothing else
       } else if (a.fixed_iters) {
-        if (it >= a.max_iter || !finite) {
+        // chunked schedule: exactly max_iter steps (a non-finite row keeps
+        // stepping), then the residual of the final voltage decides
+        if (it >= a.max_iter) {
           status = !finite ? ROW_DIVERGED : (nrm < a.tol ? ROW_CONVERGED : ROW_MAX_ITER);
           break;
         }
-      } else {
+      } else if (a.step_first) {
+        if (it >= a.max_iter) {
+          status = !finite ? ROW_DIVERGED : ROW_MAX_ITER;
+          break;
+        }
+        converged_after_step = nrm < a.tol;
+      } else if (it > 0 && it % (a.round_k > 1 ? a.round_k : 1) == 0) {
+        // continuous schedule: tested at the end of each round of round_k
+        // steps only; a loaded row always runs its first round
         if (!finite) { status = ROW_DIVERGED; break; }
         if (nrm < a.tol) { status = ROW_CONVERGED; break; }
         if (it >= a.max_iter) { status = ROW_MAX_ITER; break; }
@@ -1096,6 +1113,10 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       __syncthreads();
       prof.mark(PH_UPDATE);
       ++it;
+      if (converged_after_step) {
+        status = ROW_CONVERGED;
+        break;
+      }
     }
     it_total += it;
     // status and attempt are block-uniform: the whole CTA restarts or leaves

@@ -65,6 +65,13 @@ struct SweepArgs {
   int max_iter;
   double tol;
   int fixed_iters;        // 1: exactly max_iter steps then the residual; 0: stop at tol
+  // continuous schedule: a row's mismatch is tested only after every
+  // round_k-th step (so a row runs a multiple of round_k steps, at least
+  // round_k), the reference's nb_iter_per_round
+  int round_k;
+  // 1: the reference's single-solve order: each step is taken, then the
+  // mismatch evaluated before it decides convergence (no round rule)
+  int step_first;
   int refactor_policy;    // 0: refactor every step; 1: reuse the LU while ||F|| contracts;
                           // 2: as 1, starting on the base case's factor (base_ws)
   double refactor_ratio;  // policy 1: refactor when ||F_k|| > ratio * ||F_{k-1}||

@@ -91,7 +91,8 @@ void check(int rc) {
 
 gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
                         int n_ctas, bool profile = false, int refactor = 0, double refactor_ratio = 0.0,
-                        int max_reuse = 0, bool rescue = false) {
+                        int max_reuse = 0, bool rescue = false, int iters_per_round = 1,
+                        bool step_then_check = false) {
   gs2g_run_opts o{};
   o.max_iter = max_iter;
   o.tol = tol;
@@ -105,6 +106,8 @@ gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precisio
   o.refactor_ratio = refactor_ratio;
   o.max_reuse = max_reuse;
   o.rescue = rescue ? 1 : 0;
+  o.iters_per_round = iters_per_round;
+  o.step_then_check = step_then_check ? 1 : 0;
   return o;
 }
 
@@ -205,9 +208,10 @@ class Session {
   }
 
   void run_subset(IArr rows, int max_iter, double tol, bool fixed_iters, int precision, int start,
-                  double pivot_floor, int n_ctas, int refactor, double refactor_ratio, int max_reuse, bool rescue) {
+                  double pivot_floor, int n_ctas, int refactor, double refactor_ratio, int max_reuse, bool rescue,
+                  int iters_per_round) {
     gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, false, refactor,
-                                refactor_ratio, max_reuse, rescue);
+                                refactor_ratio, max_reuse, rescue, iters_per_round);
     const int n = (int)rows.size();
     const int* rp = rows.data();
     int rc;
@@ -240,8 +244,10 @@ class Session {
     check(gs2g_set_vinit(h(), reinterpret_cast<const double*>(v.data())));
   }
 
-  py::tuple solve_base(int max_iter, double tol, int precision, double pivot_floor) {
-    gs2g_run_opts o = make_opts(max_iter, tol, false, precision, GS2G_START_VINIT, pivot_floor, 1);
+  // the base case is a single solve: the reference's step-then-test order by default
+  py::tuple solve_base(int max_iter, double tol, int precision, double pivot_floor, bool step_then_check) {
+    gs2g_run_opts o = make_opts(max_iter, tol, false, precision, GS2G_START_VINIT, pivot_floor, 1, false, 0, 0.0, 0,
+                                false, 1, step_then_check);
     py::array_t<cplx> V(n_bus_);
     int st = 0, it = 0;
     double res = 0;
@@ -263,9 +269,10 @@ class Session {
   }
 
   void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas,
-           bool profile, int refactor, double refactor_ratio, int max_reuse, bool rescue) {
+           bool profile, int refactor, double refactor_ratio, int max_reuse, bool rescue, int iters_per_round,
+           bool step_then_check) {
     gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                                refactor_ratio, max_reuse, rescue);
+                                refactor_ratio, max_reuse, rescue, iters_per_round, step_then_check);
     int rc;
     {
       py::gil_scoped_release nogil;
@@ -383,6 +390,8 @@ class Session {
     d["n_rescued"] = t.n_rescued;
     d["n_base_start"] = t.n_base_start;
     d["chord_steps"] = t.chord_steps;
+    d["base_setup_ms"] = t.base_setup_ms;
+    d["base_setup_bytes"] = t.base_setup_bytes;
     return d;
   }
 
@@ -445,14 +454,14 @@ py::dict plan_info(int n_bus, IArr indptr, IArr indices, IArr pv, IArr pq, int t
 // Several sessions' current rows in one persistent launch (gs2g_run_multi).
 void run_multi(const std::vector<Session*>& sessions, int max_iter, double tol, bool fixed_iters, int precision,
                int start, double pivot_floor, int n_ctas, bool profile, int refactor, double refactor_ratio,
-               int max_reuse, bool rescue) {
+               int max_reuse, bool rescue, int iters_per_round) {
   std::vector<gs2g_session*> hs;
   for (Session* s : sessions) {
     if (!s) throw py::value_error("run_multi: None in the session list");
     hs.push_back(reinterpret_cast<gs2g_session*>(s->handle()));
   }
   gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                              refactor_ratio, max_reuse, rescue);
+                              refactor_ratio, max_reuse, rescue, iters_per_round);
   int rc;
   {
     py::gil_scoped_release nogil;
@@ -531,7 +540,7 @@ PYBIND11_MODULE(_gs2g, m) {
   m.def("run_multi", &run_multi, py::arg("sessions"), py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"),
         py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0,
         py::arg("profile") = false, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0,
-        py::arg("max_reuse") = 0, py::arg("rescue") = false);
+        py::arg("max_reuse") = 0, py::arg("rescue") = false, py::arg("iters_per_round") = 1);
   py::class_<Session>(m, "Session")
       .def(py::init<int, int, IArr, IArr, CArr, CArr, CArr, IArr, IArr, int>(), py::arg("device"), py::arg("n_bus"),
            py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),
@@ -551,19 +560,20 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("run_subset", &Session::run_subset, py::arg("rows"), py::arg("max_iter"), py::arg("tol"),
            py::arg("fixed_iters"), py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0,
            py::arg("n_ctas") = 0, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
-           py::arg("rescue") = false)
+           py::arg("rescue") = false, py::arg("iters_per_round") = 1)
       .def("branch_loading", &Session::branch_loading)
       .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)
       .def("set_vinit", &Session::set_vinit)
-      .def("solve_base", &Session::solve_base)
+      .def("solve_base", &Session::solve_base, py::arg("max_iter"), py::arg("tol"), py::arg("precision"),
+           py::arg("pivot_floor") = 0.0, py::arg("step_then_check") = true)
       .def("set_base_v", &Session::set_base_v)
       .def("run", &Session::run, py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"), py::arg("precision"),
            py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false,
            py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
-           py::arg("rescue") = false)
+           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("step_then_check") = false)
       .def("factor_counts", &Session::factor_counts)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)

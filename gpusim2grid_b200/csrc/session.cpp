@@ -36,6 +36,9 @@ namespace {
 thread_local std::string g_err;
 
 constexpr int kMaxEdits = 64;  // must match MAX_EDITS in nr_kernel.cu
+// a row runs at most max(max_iter, k) + k steps; k is bounded so that no
+// option value can keep a row stepping for long
+constexpr int kMaxItersPerRound = 1000;
 
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
@@ -223,14 +226,18 @@ struct DSU {
 // that trip two or more non-bridge branches.
 void compute_bridges(gs2g_session* s) {
   const int n = s->n_bus, m = s->n_branch;
+  // a branch open at one end (negative endpoint) joins no two buses
+  auto edge = [&](int l) { return s->br_from[l] >= 0 && s->br_to[l] >= 0; };
   std::vector<int> deg(n + 1, 0);
   for (int l = 0; l < m; ++l) {
+    if (!edge(l)) continue;
     ++deg[s->br_from[l] + 1];
     ++deg[s->br_to[l] + 1];
   }
   for (int v = 0; v < n; ++v) deg[v + 1] += deg[v];
   std::vector<int> adj_v(2 * m), adj_e(2 * m), fill(deg.begin(), deg.end() - 1);
   for (int l = 0; l < m; ++l) {
+    if (!edge(l)) continue;
     const int f = s->br_from[l], t = s->br_to[l];
     adj_v[fill[f]] = t;
     adj_e[fill[f]++] = l;
@@ -316,6 +323,7 @@ void assemble_rows(gs2g_session* s) {
           for (int l = 0; l < s->n_branch; ++l) {
             while (ui < uniq.size() && uniq[ui] < l) ++ui;
             if (ui < uniq.size() && uniq[ui] == l) continue;
+            if (s->br_from[l] < 0 || s->br_to[l] < 0) continue;  // open at one end: no edge
             if (d.u(s->br_from[l], s->br_to[l])) --comps;
           }
           island = comps > 1;
@@ -331,7 +339,10 @@ void assemble_rows(gs2g_session* s) {
       for (int l : uniq) {
         const double* v[4] = {&s->yff[2 * l], &s->ytt[2 * l], &s->yft[2 * l], &s->ytf[2 * l]};
         const int kk[4] = {s->k_ff[l], s->k_tt[l], s->k_ft[l], s->k_tf[l]};
-        for (int q = 0; q < 4; ++q) acc[kk[q]] += std::complex<double>(v[q][0], v[q][1]);
+        // an open endpoint has no Ybus row or column: its terms are skipped
+        // (contingency_analysis_helper.cpp:53-75)
+        for (int q = 0; q < 4; ++q)
+          if (kk[q] >= 0) acc[kk[q]] += std::complex<double>(v[q][0], v[q][1]);
       }
       if ((int)acc.size() > kMaxEdits)
         throw std::invalid_argument("row " + std::to_string(r) + " trips too many branches (" +
@@ -390,6 +401,10 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.max_iter = o.max_iter;
   a.tol = o.tol;
   a.fixed_iters = o.fixed_iters;
+  if (o.iters_per_round > kMaxItersPerRound)
+    throw std::invalid_argument("iters_per_round must be <= " + std::to_string(kMaxItersPerRound));
+  a.round_k = o.iters_per_round > 0 ? o.iters_per_round : 1;
+  a.step_first = o.step_then_check != 0 && !o.fixed_iters;
   a.v_out = out.v;
   a.res_out = out.res;
   a.status_out = out.status;
@@ -755,14 +770,17 @@ int gs2g_set_branch_data(gs2g_session* s, int n_branch, const int* from, const i
     throw std::invalid_argument("set_branch_data: bad arguments");
   std::vector<int> kff(n_branch), ktt(n_branch), kft(n_branch), ktf(n_branch);
   for (int l = 0; l < n_branch; ++l) {
+    // a negative endpoint is a side with no bus in the solved system (the
+    // open end of a half-open line): the branch has only its other end's
+    // self term (contingency_analysis_helper.cpp:53-75)
     const int f = from[l], t = to[l];
-    if (f < 0 || f >= s->n_bus || t < 0 || t >= s->n_bus || f == t)
+    if (f >= s->n_bus || t >= s->n_bus || (f >= 0 && f == t))
       throw std::invalid_argument("set_branch_data: branch " + std::to_string(l) + " has a bad endpoint");
-    kff[l] = ybus_find(s->plan, f, f);
-    ktt[l] = ybus_find(s->plan, t, t);
-    kft[l] = ybus_find(s->plan, f, t);
-    ktf[l] = ybus_find(s->plan, t, f);
-    if (kff[l] < 0 || ktt[l] < 0 || kft[l] < 0 || ktf[l] < 0)
+    kff[l] = f >= 0 ? ybus_find(s->plan, f, f) : -1;
+    ktt[l] = t >= 0 ? ybus_find(s->plan, t, t) : -1;
+    kft[l] = f >= 0 && t >= 0 ? ybus_find(s->plan, f, t) : -1;
+    ktf[l] = f >= 0 && t >= 0 ? ybus_find(s->plan, t, f) : -1;
+    if ((f >= 0 && kff[l] < 0) || (t >= 0 && ktt[l] < 0) || (f >= 0 && t >= 0 && (kft[l] < 0 || ktf[l] < 0)))
       throw std::invalid_argument("set_branch_data: branch " + std::to_string(l) + " is not in the Ybus pattern");
   }
   s->n_branch = n_branch;
@@ -812,8 +830,10 @@ int gs2g_set_contingencies(gs2g_session* s, int n_rows, const int* ptr, const in
     if (nnz > 0 && !ids) throw std::invalid_argument("set_contingencies: ids must not be NULL");
     for (int q = 0; q < nnz; ++q)
       if (ids[q] < 0 || ids[q] >= s->n_branch)
-        throw std::invalid_argument("set_contingencies: branch index " + std::to_string(ids[q]) +
-                                    " out of range (n_branches=" + std::to_string(s->n_branch) + ")");
+        // std::runtime_error, as build_contingency_from_branch_ids
+        // (contingency_analysis_helper.cpp:46-48): RuntimeError in Python
+        throw std::runtime_error("set_contingencies: branch index " + std::to_string(ids[q]) +
+                                 " out of range (n_branches=" + std::to_string(s->n_branch) + ")");
     s->ctg_ptr.assign(ptr, ptr + n_rows + 1);
     s->ctg_ids.assign(ids, ids + nnz);
   } else {
@@ -1124,6 +1144,7 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   if (s->base_factor_prec == prec) return;
   if (!s->has_base)
     throw std::runtime_error("refactor policy BASE_CHORD needs a base case (solve_base or set_base_v first)");
+  const auto t_setup = std::chrono::steady_clock::now();
   const int n = s->n_bus;
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, prec);
   s->d_base_ws.ensure((size_t)wsb);
@@ -1178,6 +1199,8 @@ void ensure_base_factor(gs2g_session* s, int prec) {
     packed(s->plan.bw_pos, s->d_base_bwv);
   }
   s->base_factor_prec = prec;
+  s->tm.base_setup_ms = ms_since(t_setup);
+  s->tm.base_setup_bytes = (int64_t)(s->d_base_ws.n + s->d_base_inv.n + s->d_base_fwv.n + s->d_base_bwv.n);
 }
 
 RunPrep prepare_rows(gs2g_session* s, const gs2g_run_opts& o) {
@@ -1559,6 +1582,10 @@ int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, i
     throw std::invalid_argument("run_rows_noalloc: NULL input or output");
   if (o->precision != GS2G_PREC_FP64 && o->precision != GS2G_PREC_MIXED)
     throw std::invalid_argument("precision must be GS2G_PREC_FP64 or GS2G_PREC_MIXED");
+  if (o->refactor_policy == GS2G_REFACTOR_BASE_CHORD)
+    throw std::invalid_argument("run_rows_noalloc: GS2G_REFACTOR_BASE_CHORD is not supported on the allocation-free "
+                                "path (it needs the session's base-factor buffers); use GS2G_REFACTOR_EVERY or "
+                                "GS2G_REFACTOR_ADAPTIVE");
   if (o->refactor_policy != GS2G_REFACTOR_EVERY && o->refactor_policy != GS2G_REFACTOR_ADAPTIVE)
     throw std::invalid_argument("refactor_policy must be GS2G_REFACTOR_EVERY or GS2G_REFACTOR_ADAPTIVE");
   if (o->max_iter < 0) throw std::invalid_argument("max_iter must be >= 0");
@@ -1578,6 +1605,10 @@ int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, i
   a.max_iter = o->max_iter;
   a.tol = o->tol;
   a.fixed_iters = o->fixed_iters;
+  if (o->iters_per_round > kMaxItersPerRound)
+    throw std::invalid_argument("iters_per_round must be <= " + std::to_string(kMaxItersPerRound));
+  a.round_k = o->iters_per_round > 0 ? o->iters_per_round : 1;
+  a.step_first = o->step_then_check != 0 && !o->fixed_iters;
   a.refactor_policy = o->refactor_policy;
   a.refactor_ratio = o->refactor_ratio > 0 ? o->refactor_ratio : 0.3;
   a.max_reuse = o->max_reuse > 0 ? o->max_reuse : 3;
@@ -1606,6 +1637,7 @@ int gs2g_acpf_nr(int device, int n_bus, const int* ybus_indptr, const int* ybus_
   o.fixed_iters = 0;
   o.precision = precision;
   o.start = GS2G_START_VINIT;
+  o.step_then_check = 1;  // the reference's single-solve order (acpf_nr.cu:505-561)
   int st = 0, it = 0;
   double res = 0;
   rc = gs2g_solve_base(s, &o, v_inout, &st, &it, &res);

@@ -36,6 +36,7 @@ __all__ = [
     "n1_branches",
     "injection_scenarios",
     "scenario_outages",
+    "half_open_variant",
 ]
 
 
@@ -76,6 +77,8 @@ class Grid:
     ytf: np.ndarray = None
     ytt: np.ndarray = None
     Ybus: sp.csr_matrix = None
+    # branches open at their to-end (branch_to = -1), see half_open_variant
+    open_branches: Optional[np.ndarray] = None
 
     @property
     def n_branch(self) -> int:
@@ -239,15 +242,21 @@ def grid_by_name(name: str, seed: int = 0) -> Grid:
 
 def _bridges(n_bus, f, t):
     """Bridge edges (branch ids whose removal disconnects the graph), by an
-    iterative Tarjan low-link DFS."""
+    iterative Tarjan low-link DFS.  A branch open at one end (a negative
+    endpoint) is no edge and never a bridge."""
+    f = np.asarray(f)
+    t = np.asarray(t)
+    edge = (f >= 0) & (t >= 0)
     adj_ptr = np.zeros(n_bus + 1, dtype=np.int64)
-    np.add.at(adj_ptr, f + 1, 1)
-    np.add.at(adj_ptr, t + 1, 1)
+    np.add.at(adj_ptr, f[edge] + 1, 1)
+    np.add.at(adj_ptr, t[edge] + 1, 1)
     adj_ptr = np.cumsum(adj_ptr)
     adj_to = np.empty(adj_ptr[-1], dtype=np.int64)
     adj_e = np.empty(adj_ptr[-1], dtype=np.int64)
     head = adj_ptr[:-1].copy()
     for e, (a, c) in enumerate(zip(f, t)):
+        if a < 0 or c < 0:
+            continue
         adj_to[head[a]] = c; adj_e[head[a]] = e; head[a] += 1
         adj_to[head[c]] = a; adj_e[head[c]] = e; head[c] += 1
     disc = -np.ones(n_bus, dtype=np.int64)
@@ -325,10 +334,43 @@ def scenario_outages(grid: Grid, n_rows: int, max_trips: int = 2, seed: int = 2,
 
 
 def _connected_without(grid: Grid, ids) -> bool:
-    keep = np.ones(grid.n_branch, dtype=bool)
+    keep = (grid.branch_from >= 0) & (grid.branch_to >= 0)
     keep[list(ids)] = False
     f, t = grid.branch_from[keep], grid.branch_to[keep]
     A = sp.coo_matrix((np.ones(f.size), (f, t)), shape=(grid.n_bus, grid.n_bus))
     from scipy.sparse.csgraph import connected_components
     ncomp, _ = connected_components(A, directed=False)
     return ncomp == 1
+
+
+def half_open_variant(grid: Grid, n_open: int = 2, seed: int = 0) -> Grid:
+    """The grid with ``n_open`` branches open at their to-end: their
+    ``branch_to`` is -1 (a side with no bus in the solved system, as the
+    reference's bus relabelling gives the open end of a half-open line,
+    ``contingency_analysis_helper.cpp:53-64``) and Ybus keeps only their
+    from-end self term yff (the line's charging seen from the live end).  The
+    branches are chosen among those whose loss keeps the grid connected, so
+    the variant stays connected."""
+    rng = np.random.default_rng(seed)
+    cand = [int(l) for l in rng.permutation(n1_branches(grid))]
+    chosen = []
+    for l in cand:
+        if len(chosen) == n_open:
+            break
+        if _connected_without(grid, chosen + [l]):
+            chosen.append(l)
+    ids = np.array(sorted(chosen), dtype=np.int32)
+    f = grid.branch_from.astype(np.int64)
+    t = grid.branch_to.astype(np.int64)
+    live = np.ones(grid.n_branch, dtype=bool)
+    live[ids] = False
+    rows = np.concatenate([f, t[live], f[live], t[live]])
+    cols = np.concatenate([f, t[live], t[live], f[live]])
+    vals = np.concatenate([grid.yff, grid.ytt[live], grid.yft[live], grid.ytf[live]])
+    Y = sp.coo_matrix((vals, (rows, cols)), shape=(grid.n_bus, grid.n_bus)).tocsr()
+    Y.sum_duplicates()
+    Y.sort_indices()
+    to = grid.branch_to.copy()
+    to[ids] = -1
+    return dataclasses.replace(grid, name=grid.name + "_half_open", branch_to=to, Ybus=Y.astype(np.complex128),
+                               open_branches=ids)

@@ -401,11 +401,15 @@ class LearnedStart:
         s.close()
         self.V_base = Vb
         f, t = grid.branch_from.astype(np.int64), grid.branch_to.astype(np.int64)
-        Sft = Vb[f] * np.conj(grid.yff * Vb[f] + grid.yft * Vb[t])
-        Stf = Vb[t] * np.conj(grid.ytf * Vb[f] + grid.ytt * Vb[t])
+        # an open end (negative endpoint) has V = 0 and carries no power
+        hf, ht = f >= 0, t >= 0
+        fz, tz = np.where(hf, f, 0), np.where(ht, t, 0)
+        Vf, Vt = np.where(hf, Vb[fz], 0), np.where(ht, Vb[tz], 0)
+        Sft = np.where(hf, Vf * np.conj(grid.yff * Vf + grid.yft * Vt), 0)
+        Stf = np.where(ht, Vt * np.conj(grid.ytf * Vf + grid.ytt * Vt), 0)
         off = self.dim  # outage channel
-        scratch = 2 * self.dim  # column for entries at the slack / pv Q (dropped)
-        col = lambda m, b, base: np.where(m[b] >= 0, base + m[b], scratch)
+        scratch = 2 * self.dim  # column for entries at the slack / pv Q / an open end (dropped)
+        col = lambda m, b, base: np.where((b >= 0) & (m[np.maximum(b, 0)] >= 0), base + m[np.maximum(b, 0)], scratch)
         cols = np.stack([col(ia, f, off), col(im, f, off), col(ia, t, off), col(im, t, off)], axis=1)
         vals = np.stack([Sft.real, Sft.imag, Stf.real, Stf.imag], axis=1)
         self._br_cols = torch.as_tensor(cols.astype(np.int64), device=dev)

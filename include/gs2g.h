@@ -95,6 +95,22 @@ typedef struct gs2g_run_opts {
    * a fresh max_iter budget and a new LU every step; its iteration and
    * factorization counts include both attempts. */
   int rescue;
+  /* Continuous schedule: Newton steps between two convergence tests of a
+   * row (the reference's nb_iter_per_round,
+   * src/gpusim2grid/contingency_analysis/_scheduling.py:145-156, rounds of
+   * src/_cpp/contingency/batch_pf_driver.cu:2691-2724).  After each round
+   * of k steps a row leaves DIVERGED (residual not finite), CONVERGED
+   * (residual < tol) or MAX_ITER (steps >= max_iter); a row therefore runs a
+   * multiple of k steps and at least k, also when it starts converged.
+   * <= 0 selects 1; above 1000 is rejected (GS2G_ERR_INVALID). */
+  int iters_per_round;
+  /* 1: the reference's single-solve order (src/_cpp/acpf_nr.cu:505-561):
+   * every iteration takes a full Newton step and then tests the mismatch
+   * evaluated before that step, so a converged solve reports one step more
+   * than the steps needed and returns the voltage after it; a solve that
+   * never passes the test within max_iter steps ends MAX_ITER (DIVERGED
+   * when its last mismatch is not finite).  Continuous schedule only. */
+  int step_then_check;
 } gs2g_run_opts;
 
 #define GS2G_REFACTOR_EVERY 0
@@ -123,6 +139,12 @@ typedef struct gs2g_timings {
   int n_rescued;    /* rows of the last run restarted (gs2g_run_opts.rescue) */
   int n_base_start; /* rows of the last run that began from the base V instead of their given start */
   int64_t chord_steps; /* Newton steps of the last run taken in the chord sweep on the shared base factor */
+  /* GS2G_REFACTOR_BASE_CHORD: the last set-up of the shared base factor (its
+   * factorization, explicit inverse and packed solve values; done once per
+   * session, base case and precision, outside every gs2g_run that reuses it):
+   * wall ms and the device bytes it holds */
+  double base_setup_ms;
+  int64_t base_setup_bytes;
 } gs2g_timings;
 
 const char* gs2g_last_error(void);
@@ -262,7 +284,17 @@ int gs2g_sync(gs2g_session* s);
  *   overlap on the GPU race.  Returns once the work is enqueued on `stream`
  *   (NULL = default stream); synchronise it before reading the outputs.
  *   The rescue option restarts from the session's Vinit; its count is not
- *   recorded (gs2g_timings is not touched). */
+ *   recorded (gs2g_timings is not touched).
+ *   Of gs2g_run_opts it reads max_iter, tol, fixed_iters, precision,
+ *   pivot_floor, refactor_policy (GS2G_REFACTOR_EVERY or _ADAPTIVE only;
+ *   GS2G_REFACTOR_BASE_CHORD needs session buffers and is rejected),
+ *   refactor_ratio, max_reuse, rescue, iters_per_round and step_then_check;
+ *   start, n_ctas and profile_phases are ignored (the rows start from v0, the
+ *   CTA count is what fits the scratch, no phase counters).
+ *   The device address of the scratch array is looked up once per device
+ *   and kept for the life of the process: after cudaDeviceReset (or any
+ *   re-creation of the device's primary context) this entry point must not
+ *   be called again in that process. */
 int gs2g_run_rows_noalloc(const gs2g_session* s, int n_rows, const double* v0, int64_t v0_stride,
                           const double* sbus, int64_t sbus_stride, const gs2g_run_opts* o, double* v_out,
                           double* residuals, int* status, int* iters, void* stream);

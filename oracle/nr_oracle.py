@@ -97,41 +97,76 @@ def nan_inf_norm(F):
     return float(np.max(np.abs(F)))
 
 
-def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="converge"):
-    """One NR solve.
+def newton_step(Y, V, F, pvpq, pq):
+    """One full Newton step from V with mismatch F: J at V, dx = J^-1 F, then
+    the polar update (acpf_nr.cu nr_iter_step: SpMV, fill F, fill J,
+    factorize, solve, update V).  A step that cannot be taken (a non-finite
+    mismatch or a singular J) leaves every unknown NaN, as NaN propagates
+    through the reference's solve."""
+    if np.all(np.isfinite(F)):
+        J = jacobian(Y, V, pvpq, pq)
+        try:
+            dx = spla.splu(J, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.1,
+                           options=dict(SymmetricMode=True)).solve(F)
+        except RuntimeError:
+            dx = np.full(F.size, np.nan)
+    else:
+        dx = np.full(F.size, np.nan)
+    return update_v(V, dx, pvpq, pq)
 
-    mode="converge": evaluate F(V_k); stop with CONVERGED once ‖F‖∞ < tol (no
-    further step); otherwise step.  ``iters`` counts Newton steps taken.
-    mode="fixed": take exactly ``max_iter`` steps without checking, then report
-    the residual of the final V (the reference's chunked schedule,
-    ``src/_cpp/contingency/driver.cuh:136-259`` + the residual pass).
+
+def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1):
+    """One NR solve under one of the reference's three schedules.
+
+    mode="continuous" (``src/_cpp/contingency/batch_pf_driver.cu:2691-2724``):
+    rounds of ``k`` steps (``nb_iter_per_round``); after each round the
+    residual of the current V decides: not finite -> DIVERGED, < tol ->
+    CONVERGED, steps >= max_iter -> MAX_ITER, else another round.  A row
+    always runs its first round, also when it starts converged, so ``iters``
+    is a positive multiple of k.
+    mode="fixed" (the chunked schedule, ``src/_cpp/contingency/driver.cuh:136-259``
+    + the residual pass ``batch_pf_driver.cu:2019-2061``): exactly ``max_iter``
+    steps, then the residual of the final V decides.
+    mode="single" (``src/_cpp/acpf_nr.cu:505-561``): each iteration takes a
+    full step, then tests the mismatch evaluated BEFORE it; a converged
+    solve reports the step that followed the passing test and returns the V
+    after it; no pass within ``max_iter`` steps is MAX_ITER (DIVERGED when the
+    last mismatch is not finite).  ``residual`` is the last mismatch
+    evaluated (for a converged single solve: the one that passed).
+    "converge" is an alias of "continuous".
 
     Returns (V, status, iters, residual).
     """
     Y = sp.csr_matrix(Y)
     pvpq, pq_, _ = j_layout(Y.shape[0], pv, pq)
     V = np.asarray(V0, dtype=np.complex128).copy()
+    k = max(int(k), 1)
+    if mode == "converge":
+        mode = "continuous"
+    if mode not in ("continuous", "fixed", "single"):
+        raise ValueError(f"unknown mode {mode!r}")
     it = 0
     while True:
         F = mismatch(Y, V, Sbus, pvpq, pq_)
         nrm = nan_inf_norm(F)
-        if mode == "converge":
-            if not np.isfinite(nrm):
+        finite = np.isfinite(nrm)
+        if mode == "fixed":
+            if it >= max_iter:
+                return V, (DIVERGED if not finite else CONVERGED if nrm < tol else MAX_ITER), it, nrm
+        elif mode == "single":
+            if it >= max_iter:
+                return V, (DIVERGED if not finite else MAX_ITER), it, nrm
+        elif it > 0 and it % k == 0:
+            if not finite:
                 return V, DIVERGED, it, nrm
             if nrm < tol:
                 return V, CONVERGED, it, nrm
-        if it >= max_iter:
-            if not np.isfinite(nrm):
-                return V, DIVERGED, it, nrm
-            return V, (CONVERGED if nrm < tol else MAX_ITER), it, nrm
-        J = jacobian(Y, V, pvpq, pq_)
-        try:
-            dx = spla.splu(J, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.1,
-                            options=dict(SymmetricMode=True)).solve(F)
-        except RuntimeError:
-            return V, DIVERGED, it, float("nan")
-        V = update_v(V, dx, pvpq, pq_)
+            if it >= max_iter:
+                return V, MAX_ITER, it, nrm
+        V = newton_step(Y, V, F, pvpq, pq_)
         it += 1
+        if mode == "single" and nrm < tol:
+            return V, CONVERGED, it, nrm
 
 
 def trip_branches(Y, branch_ids, f, t, yff, yft, ytf, ytt):
@@ -148,6 +183,8 @@ def trip_branches(Y, branch_ids, f, t, yff, yft, ytf, ytt):
         seen.append(l)
         i, j = int(f[l]), int(t[l])
         for (r, c, v) in ((i, i, yff[l]), (j, j, ytt[l]), (i, j, yft[l]), (j, i, ytf[l])):
+            if r < 0 or c < 0:
+                continue  # an open endpoint has no Ybus row or column (:53-75)
             lo, hi = Y.indptr[r], Y.indptr[r + 1]
             k = lo + int(np.searchsorted(Y.indices[lo:hi], c))
             assert k < hi and Y.indices[k] == c
@@ -158,16 +195,16 @@ def trip_branches(Y, branch_ids, f, t, yff, yft, ytf, ytt):
 def islands(n_bus, f, t, branch_ids):
     """True when removing ``branch_ids`` disconnects the branch graph."""
     from scipy.sparse.csgraph import connected_components
-    keep = np.ones(len(f), dtype=bool)
+    f, t = np.asarray(f), np.asarray(t)
+    keep = (f >= 0) & (t >= 0)  # a branch open at one end joins no two buses
     keep[list(branch_ids)] = False
-    A = sp.coo_matrix((np.ones(keep.sum()), (np.asarray(f)[keep], np.asarray(t)[keep])),
-                      shape=(n_bus, n_bus))
+    A = sp.coo_matrix((np.ones(keep.sum()), (f[keep], t[keep])), shape=(n_bus, n_bus))
     ncomp, _ = connected_components(A, directed=False)
     return ncomp > 1
 
 
 def contingency_sweep(Y, V0, Sbus, pv, pq, branch_rows, f, t, yff, yft, ytf, ytt,
-                      max_iter=10, tol=1e-8, mode="converge"):
+                      max_iter=10, tol=1e-8, mode="continuous", k=1):
     """Solve every row (a list of tripped-branch lists).  Islanding rows are
     NOT_SIMULATED with NaN voltages (contingency_analysis_helper.cpp:634-651)."""
     n = Y.shape[0]
@@ -179,12 +216,12 @@ def contingency_sweep(Y, V0, Sbus, pv, pq, branch_rows, f, t, yff, yft, ytf, ytt
         if islands(n, f, t, ids):
             continue
         Yr = trip_branches(Y, ids, f, t, yff, yft, ytf, ytt)
-        V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode)
+        V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode, k)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
 
 
-def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="converge"):
+def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1):
     """Solve one row per Sbus row."""
     B, n = Sbus_rows.shape
     out_V = np.empty((B, n), dtype=np.complex128)
@@ -192,7 +229,7 @@ def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="conve
     iters = np.empty(B, dtype=np.int32)
     res = np.empty(B)
     for r in range(B):
-        V, st, it, nrm = nr_solve(Y, V0, Sbus_rows[r], pv, pq, max_iter, tol, mode)
+        V, st, it, nrm = nr_solve(Y, V0, Sbus_rows[r], pv, pq, max_iter, tol, mode, k)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
 
@@ -204,7 +241,12 @@ def branch_flows(V, f, t, yff, yft, ytf, ytt):
     V = np.asarray(V)
     f = np.asarray(f)
     t = np.asarray(t)
-    return V[f] * np.conj(yff * V[f] + yft * V[t]), V[t] * np.conj(ytf * V[f] + ytt * V[t])
+    # an open end (negative endpoint) has V = 0 and carries no power
+    hf, ht = f >= 0, t >= 0
+    Vf = np.where(hf, V[np.where(hf, f, 0)], 0)
+    Vt = np.where(ht, V[np.where(ht, t, 0)], 0)
+    return (np.where(hf, Vf * np.conj(yff * Vf + yft * Vt), 0),
+            np.where(ht, Vt * np.conj(ytf * Vf + ytt * Vt), 0))
 
 
 def branch_loading(V, f, t, yff, yft, ytf, ytt, rate_pu, tripped=()):
@@ -218,3 +260,26 @@ def branch_loading(V, f, t, yff, yft, ytf, ytt, rate_pu, tripped=()):
     if len(tripped):
         out[list(tripped)] = 0.0
     return out
+
+
+def branch_currents_amps(V, f, t, yff, yft, ytf, ytt, bus_vn_kv, sn_mva):
+    """Branch terminal current magnitudes in amperes (the reference's host
+    check, ``src/gpusim2grid/acpf_nr/_branch_flows.py``, same formulas as its
+    ``compute_branch_flows_kernel``): I_or = yff V_f + yft V_t at the from end,
+    I_ex = ytf V_f + ytt V_t at the to end, each scaled by its own bus's base
+    current sn_mva / (sqrt(3) vn_kv) kA.  An open end (negative endpoint) has
+    V = 0, carries 0 A, and its base falls back to the other end's."""
+    V = np.asarray(V)
+    f = np.asarray(f)
+    t = np.asarray(t)
+    vn = np.asarray(bus_vn_kv, dtype=np.float64)
+    hf, ht = f >= 0, t >= 0
+    fz, tz = np.where(hf, f, 0), np.where(ht, t, 0)
+    Vf = np.where(hf, V[fz], 0)
+    Vt = np.where(ht, V[tz], 0)
+    i_or = np.where(hf, np.abs(yff * Vf + yft * Vt), 0.0)
+    i_ex = np.where(ht, np.abs(ytf * Vf + ytt * Vt), 0.0)
+    vf = np.where(hf, vn[fz], np.where(ht, vn[tz], 1.0))
+    vt = np.where(ht, vn[tz], vf)
+    base = lambda kv: sn_mva * 1e6 / (np.sqrt(3.0) * kv * 1e3)
+    return i_or * base(vf), i_ex * base(vt)

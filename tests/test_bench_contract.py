@@ -32,3 +32,5 @@ def test_reference_arm_json_line(workload):
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and "4 of" in cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    # the reference arm never maps this repository's engine (no package import)
+    assert d["native_so_loaded"] == []

@@ -56,3 +56,26 @@ def test_plan_info_through_ctypes(g118):
     assert b"plan_info" in lib.gs2g_last_error()
     assert lib.gs2g_version() >= 100
     assert lib.gs2g_max_edits_per_row() == 64
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of gs2g_run_opts and gs2g_timings used by the tests
+    and shown in INTEGRATION.md have the header's size and field offsets (a
+    shorter mirror would let the library read past the caller's struct)."""
+    import subprocess
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_zz_no_alloc import RunOpts
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "gs2g.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu\\n", sizeof(gs2g_run_opts), '
+                   'offsetof(gs2g_run_opts, iters_per_round), offsetof(gs2g_run_opts, step_then_check), '
+                   'sizeof(gs2g_timings)); return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    size, off_k, off_s, _ = map(int, subprocess.run([str(exe)], capture_output=True, text=True,
+                                                    check=True).stdout.split())
+    assert ctypes.sizeof(RunOpts) == size
+    assert RunOpts.iters_per_round.offset == off_k and RunOpts.step_then_check.offset == off_s
+    doc = open(os.path.join(os.path.dirname(HEADER), "..", "INTEGRATION.md")).read()
+    assert '("iters_per_round", I), ("step_then_check", I)' in doc

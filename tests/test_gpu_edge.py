@@ -84,10 +84,14 @@ def test_unit_scale_injection_reproduces_base(g118):
     assert np.abs(sw.V_results - Vb[None]).max() < 1e-9
 
 
-def test_out_of_range_branch_is_value_error(g118):
+def test_out_of_range_branch_is_runtime_error(g118):
+    """build_contingency_from_branch_ids throws std::runtime_error
+    (reference contingency_analysis_helper.cpp:46-48): RuntimeError."""
     ca = _ca(g118)
-    with pytest.raises(ValueError):
+    with pytest.raises(RuntimeError, match="out of range"):
         ca.add_contingencies_by_branch_id([[g118.n_branch + 3]])
+    with pytest.raises(RuntimeError, match="out of range"):
+        ca.add_contingencies_by_branch_id([[0], [-1]])
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -72,7 +72,7 @@ def test_islanding_detected(g118):
 def test_golden_vectors_reproduce(g118):
     gd = np.load(GOLD)
     Y, V0, S, _, _, pv, pq = g118.as_tuple()
-    Vb, st, it, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    Vb, st, it, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8, mode="single")
     np.testing.assert_allclose(Vb, gd["V_base"], atol=1e-12)
     assert it == int(gd["base_iters"])
     ptr, ids = gd["ctg_ptr"], gd["ctg_ids"]
@@ -112,3 +112,60 @@ def test_branch_flows_balance_every_bus(g118):
                           tripped=[5])
     assert np.all(ld[:3] == 0) and ld[5] == 0
     np.testing.assert_allclose(ld[6:], np.maximum(np.abs(Sf), np.abs(St))[6:] / rate[6:])
+
+
+def test_schedules_count_steps_as_the_reference(g118):
+    """The three schedules on one solve: the single-solve order takes one
+    step past the first passing test (acpf_nr.cu:505-561); rounds of k steps
+    end on a multiple of k (batch_pf_driver.cu:2691-2724); a row that starts
+    converged still runs its first round."""
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vc, st_c, it_c, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8)
+    Vs, st_s, it_s, res_s = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8, mode="single")
+    assert st_c == st_s == O.CONVERGED and it_s == it_c + 1 and res_s < 1e-8
+    pvpq, pq_, _ = O.j_layout(g118.n_bus, pv, pq)
+    # the single solve's V is the continuous one's plus one more Newton step
+    V1 = O.newton_step(Y, Vc, O.mismatch(Y, Vc, S, pvpq, pq_), pvpq, pq_)
+    np.testing.assert_allclose(Vs, V1, atol=1e-13)
+    for k in (2, 3, 4):
+        _, st, it, res = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-8, k=k)
+        assert st == O.CONVERGED and it % k == 0 and it - k < it_c <= it and res < 1e-8
+    # budget: MAX_ITER at the first round end at or past max_iter
+    _, st, it, _ = O.nr_solve(Y, V0, S, pv, pq, 2, 1e-8, k=3)
+    assert st == O.MAX_ITER and it == 3
+    # a converged start still runs one round
+    _, st, it, _ = O.nr_solve(Y, Vc, S, pv, pq, 10, 1e-8, k=2)
+    assert st == O.CONVERGED and it == 2
+    # NaN injections: DIVERGED at the end of the first round
+    Sn = S.copy()
+    Sn[pq[0]] = np.nan
+    _, st, it, _ = O.nr_solve(Y, V0, Sn, pv, pq, 10, 1e-8, k=3)
+    assert st == O.DIVERGED and it == 3
+    _, st, it, _ = O.nr_solve(Y, V0, Sn, pv, pq, 4, 1e-8, mode="fixed")
+    assert st == O.DIVERGED and it == 4
+    _, st, it, _ = O.nr_solve(Y, V0, Sn, pv, pq, 4, 1e-8, mode="single")
+    assert st == O.DIVERGED and it == 4
+
+
+def test_half_open_branch_trips_only_its_live_end(g118):
+    """A branch whose to-end is open (endpoint -1) contributes only its
+    from-end self term; tripping it removes that term alone and joins no two
+    buses in the islanding test (contingency_analysis_helper.cpp:53-75)."""
+    from gpusim2grid_b200.synthetic import half_open_variant
+    h = half_open_variant(g118, n_open=2, seed=0)
+    l = int(h.open_branches[0])
+    assert h.branch_to[l] == -1 and h.branch_from[l] >= 0
+    Y, V0, S, _, _, pv, pq = h.as_tuple()
+    Yt = O.trip_branches(Y, [l], h.branch_from, h.branch_to, h.yff, h.yft, h.ytf, h.ytt)
+    d = (Y - Yt).tocoo()
+    nz = np.abs(d.data) > 0
+    assert list(zip(d.row[nz], d.col[nz])) == [(h.branch_from[l], h.branch_from[l])]
+    np.testing.assert_allclose(d.data[nz], [h.yff[l]])
+    assert not O.islands(h.n_bus, h.branch_from, h.branch_to, [l])
+    # flows: the open end carries nothing, the live end its charging
+    V, st, _, _ = O.nr_solve(Y, V0, S, pv, pq, 10, 1e-10)
+    assert st == O.CONVERGED
+    Sf, St = O.branch_flows(V, h.branch_from, h.branch_to, h.yff, h.yft, h.ytf, h.ytt)
+    assert St[l] == 0
+    f = h.branch_from[l]
+    np.testing.assert_allclose(Sf[l], V[f] * np.conj(h.yff[l] * V[f]))
