@@ -20,9 +20,12 @@ solved by plain FP64 Newton from a flat start (``fp64_flat_value``).
            flushed (256 MiB write) before every timed step.
 `e2e`    : the same metric through the public facade with host buffers
            (contingency lists in, voltages + statuses + residuals out).
---impl reference: the CPU restatement of the reference's Newton–Raphson
-           (scipy SuperLU, FP64) on all host cores, over a bounded sample of
-           the same rows.
+`cfg2`   : (default workload only) the 6500-bus injection sweep measured the
+           same way: value, FP64 comparison, agreement, roofline.
+`cpu_baseline` / --impl reference: the compiled CPU restatement of the
+           reference's Newton-Raphson (oracle/cpu_nr.cpp: FP64, own sparse LU,
+           OpenMP over rows on every host thread) over all rows of the same
+           workload, or a sample sized to --cpu-budget-s when they take longer.
 With N > 1 (torchrun), every rank solves its own copy of the workload
 (replicas: rows are independent, there is no collective on the data path);
 time is the max over ranks.
@@ -72,7 +75,8 @@ def _args():
     ap.add_argument("--refactor-ratio", type=float, default=None,
                     help="contraction ratio above which a row factors its own Jacobian (default: the facade's)")
     ap.add_argument("--max-reuse", type=int, default=None, help="chord steps on one factor at most (default: the facade's)")
-    ap.add_argument("--cpu-sample-rows", type=int, default=48)
+    ap.add_argument("--cpu-budget-s", type=float, default=8.0,
+                    help="seconds one CPU-baseline pass may take: all rows if they fit, else a sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="solve only the first ROWS rows (profiling cases)")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="n1_sweep_case2000_synth")
@@ -152,43 +156,67 @@ def _workload(name):
 
 
 # ---------------------------------------------------------------- CPU side
-def _cpu_rows(args_tuple):
-    """Oracle NR over rows given as (tripped branches, Sbus row or None)."""
-    from oracle import nr_oracle as O
-    (Y, V0, S, pv, pq, rows, f, t, yff, yft, ytf, ytt) = args_tuple
-    conv = iters = 0
-    for trips, sb in rows:
-        Yr = O.trip_branches(Y, trips, f, t, yff, yft, ytf, ytt) if trips else Y
-        _, st, it, _ = O.nr_solve(Yr, V0, S if sb is None else sb, pv, pq, MAX_ITER, TOL)
-        conv += int(st == O.CONVERGED)
-        iters += int(it)
-    return conv, iters
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
 
 
-def cpu_baseline(g, trips, p, q, n_rows_sample, cores=None):
-    """Time the oracle port (FP64 NR from flat, scipy SuperLU) over an evenly
-    spaced sample of the workload's rows on `cores` spawned worker
-    processes.  Returns (solves/s, cores, sample description)."""
-    import multiprocessing as mp
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    cores = cores or os.cpu_count() or 1
-    Y, V0, S, _, _, pv, pq = g.as_tuple()
-    n = len(trips) if trips is not None else p.shape[0]
-    idx = list(range(0, n, max(1, n // n_rows_sample)))[:n_rows_sample]
-    rows = [((trips[r] if trips is not None else []),
-             (None if p is None else (p[r] + 1j * q[r]) / g.sn_mva)) for r in idx]
-    chunks = [rows[i::cores] for i in range(cores)]
-    payload = [(Y, V0, S, pv, pq, c, g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt) for c in chunks if c]
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(len(payload)) as pool:
-        pool.map(_cpu_rows, [(Y, V0, S, pv, pq, rows[:1], g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt)]
-                 * len(payload))  # warm every worker's imports
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.lower().startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+class CpuBaseline:
+    """The compiled CPU Newton-Raphson (oracle/cpu_nr.cpp: FP64, flat start,
+    own minimum-degree ordering, static-pivot sparse + dense LU refactored
+    every step, OpenMP over rows on every host thread) over a workload's
+    rows: all of them when a calibration pass says they fit ``budget_s``,
+    else an evenly spaced sample sized to it."""
+
+    def __init__(self, g, trips, p, q, budget_s=8.0):
+        from oracle import cpu_nr
+        self.cpu_nr = cpu_nr
+        self.g, self.trips, self.p, self.q = g, trips, p, q
+        self.n = len(trips) if trips is not None else p.shape[0]
+        self.threads = _host_threads()
+        cal = np.unique(np.linspace(0, self.n - 1, min(self.n, 2 * self.threads)).astype(int))
+        _, dt = self._run(cal)
+        rate = len(cal) / dt
+        k = self.n if self.n / rate <= budget_s else max(len(cal), int(rate * budget_s))
+        self.idx = np.arange(self.n) if k >= self.n else np.unique(np.linspace(0, self.n - 1, k).astype(int))
+        self.sample = (f"{len(self.idx)} of {self.n} rows" + (" (all)" if len(self.idx) == self.n else
+                                                               " (evenly spaced)")
+                       + ", flat start, compiled FP64 NR (oracle/cpu_nr.cpp), OpenMP over rows")
+
+    def _run(self, idx):
+        g = self.g
+        Y, V0, S, _, _, pv, pq = g.as_tuple()
+        t = [self.trips[r] for r in idx] if self.trips is not None else None
+        sb = None if self.p is None else (self.p[idx] + 1j * self.q[idx]) / g.sn_mva
+        br = (g.branch_from, g.branch_to, g.yff, g.yft, g.ytf, g.ytt) if t is not None else None
         t0 = time.perf_counter()
-        out = pool.map(_cpu_rows, payload)
-        dt = time.perf_counter() - t0
-    conv = sum(o[0] for o in out)
-    return conv / dt, len(payload), f"{len(rows)} of {n} rows (evenly spaced), flat start, scipy SuperLU FP64 NR"
+        _, st, _, _, _ = self.cpu_nr.sweep(Y, V0, S, pv, pq, branches=br, trips=t, sbus_rows=sb, max_iter=MAX_ITER,
+                                           tol=TOL, threads=self.threads)
+        return int((st == 0).sum()), time.perf_counter() - t0
+
+    def measure(self):
+        """Converged solves/s of one pass over the chosen rows."""
+        conv, dt = self._run(self.idx)
+        return conv / dt
+
+
+def cpu_baseline(g, trips, p, q, budget_s=8.0):
+    """(solves/s, threads, sample description) of one timed pass."""
+    cb = CpuBaseline(g, trips, p, q, budget_s)
+    return cb.measure(), cb.threads, cb.sample
 
 
 # ---------------------------------------------------------------- clocks
@@ -591,9 +619,9 @@ def run_ours(args):
                             **{k: sub[k] for k in CFG2_KEYS})
         line["gpu_launches"] += sub["gpu_launches"]
     if rank == 0 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_sample_rows)
+        v, cores, sample = cpu_baseline(g, trips, p, q, args.cpu_budget_s)
         line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
-                                "sample": sample}
+                                "sample": sample, "cpu_model": _cpu_model()}
     replicas.finish()
     if rank == 0:
         print(json.dumps(line))
@@ -605,14 +633,13 @@ def _ids(rows):
     return ptr, np.fromiter((b for r in rows for b in r), dtype=np.int32, count=int(ptr[-1]))
 
 
-def cpu_baseline_multi(parts, n_rows_sample):
-    """The oracle port over an equal share of the sample from every grid; the
-    workload holds equal row counts per grid, so its rate is the harmonic
-    mean of the per-grid rates."""
-    share = max(1, n_rows_sample // len(parts))
+def cpu_baseline_multi(parts, budget_s=8.0):
+    """The compiled CPU NR over every grid's rows (an equal share of the time
+    budget each); the workload holds equal row counts per grid, so its rate
+    is the harmonic mean of the per-grid rates."""
     secs, cores, samples = 0.0, None, []
     for g, trips, p, q in parts:
-        v, cores, sample = cpu_baseline(g, trips, p, q, share)
+        v, cores, sample = cpu_baseline(g, trips, p, q, budget_s / len(parts))
         secs += 1.0 / max(v, 1e-12)
         samples.append(f"{g.name}: {sample}")
     return len(parts) / secs, cores, "; ".join(samples)
@@ -801,9 +828,9 @@ def run_ours_multi(args):
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_baseline_multi(parts, args.cpu_sample_rows)
+        v, cores, sample = cpu_baseline_multi(parts, args.cpu_budget_s)
         line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": cores, "kind": "port",
-                                "sample": sample}
+                                "sample": sample, "cpu_model": _cpu_model()}
     replicas.finish()
     if rank == 0:
         print(json.dumps(line))
@@ -811,25 +838,28 @@ def run_ours_multi(args):
 
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
+    """The reference's CPU path restated (the reference itself cannot be
+    built here): the compiled FP64 Newton-Raphson of oracle/cpu_nr.cpp on
+    every host thread, over the same workload's rows.  Each step is one pass
+    over all rows, or over an evenly spaced sample sized to about
+    --cpu-budget-s seconds when all rows would take longer."""
     rank, world, _ = _dist()
     if rank != 0:
         return
     w = _workload(args.workload)
     multi = isinstance(w, list)
-    base = (lambda k: cpu_baseline_multi(w, k)) if multi else (lambda k: cpu_baseline(*w, k))
-    vals = []
+    parts = w if multi else [w]
+    bases = [CpuBaseline(g, trips, p, q, args.cpu_budget_s / len(parts)) for g, trips, p, q in parts]
+
+    def one():
+        return len(bases) / sum(1.0 / max(b.measure(), 1e-12) for b in bases)
+
     for _ in range(args.warmup):
-        base(8)
-    cores = sample = None
-    for _ in range(args.steps):
-        v, cores, sample = base(args.cpu_sample_rows)
-        vals.append(v)
+        one()
+    vals = [one() for _ in range(args.steps)]
     value = float(np.mean(vals))
-    if multi:
-        n = sum(p.shape[0] for _, _, p, _ in w)
-    else:
-        g, trips, p, q = w
-        n = len(trips) if trips is not None else p.shape[0]
+    n = sum(b.n for b in bases)
+    sample = "; ".join(f"{g.name}: {b.sample}" for (g, _, _, _), b in zip(parts, bases))
     print(json.dumps({
         "impl": "reference",
         "metric": METRIC,
@@ -838,11 +868,12 @@ def run_reference(args):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": args.workload, "grid": WORKLOADS[args.workload][0], "rows": n, "start": "flat",
                    "tol_pu": TOL, "max_iter": MAX_ITER},
-        "cpu_baseline": {"value": round(value, 2), "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+        "cpu_baseline": {"value": round(value, 2), "unit": "solves/s", "cores": bases[0].threads, "kind": "port",
+                         "sample": sample, "cpu_model": _cpu_model()},
         "e2e": {"value": round(value, 2), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (gpusim2grid) needs cuDSS, Eigen and lightsim2grid, none installable here; "
-                "this arm times the CPU restatement of its Newton-Raphson (oracle/nr_oracle.py)",
+                "this arm times the compiled CPU restatement of its Newton-Raphson (oracle/cpu_nr.cpp, pinned to "
+                "oracle/nr_oracle.py, itself pinned to the reference's own Python)",
         "native_so_loaded": _native_maps(),
     }))
 

@@ -979,6 +979,11 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
           break;
         }
         converged_after_step = nrm < a.tol;
+      } else if (!finite && it == 0 && attempt == 0 && a.rescue_v0 != nullptr && !from_rescue_v) {
+        // a given start whose mismatch is not finite is no start at all: the
+        // row goes to its rescue attempt without a step
+        status = ROW_DIVERGED;
+        break;
       } else if (it > 0 && it % (a.round_k > 1 ? a.round_k : 1) == 0) {
         // continuous schedule: tested at the end of each round of round_k
         // steps only; a loaded row always runs its first round

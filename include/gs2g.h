@@ -93,7 +93,8 @@ typedef struct gs2g_run_opts {
    * A row that ends unconverged (MAX_ITER or DIVERGED) restarts once, inside
    * the same launch, from the base V (from Vinit without a base case), with
    * a fresh max_iter budget and a new LU every step; its iteration and
-   * factorization counts include both attempts. */
+   * factorization counts include both attempts.  A given start whose
+   * mismatch is not finite goes to that restart at once, without a step. */
   int rescue;
   /* Continuous schedule: Newton steps between two convergence tests of a
    * row (the reference's nb_iter_per_round,

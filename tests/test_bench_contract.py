@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 @pytest.mark.parametrize("workload", ["n1_sweep_case2000_synth", "injection_sweep_case6500_synth"])
 def test_reference_arm_json_line(workload):
     cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "0",
-           "--cpu-sample-rows", "4"]
+           "--cpu-budget-s", "0.5"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.strip().splitlines() if ln.startswith("{")]
@@ -29,7 +29,8 @@ def test_reference_arm_json_line(workload):
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 0 and d["n_gpus"] == 1
     assert d["config"]["workload"] == workload
     cb = d["cpu_baseline"]
-    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and "4 of" in cb["sample"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and " of " in cb["sample"]
+    assert "cpu_nr" in cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     # the reference arm never maps this repository's engine (no package import)

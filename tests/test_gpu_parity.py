@@ -194,8 +194,12 @@ def test_half_open_branches_vs_oracle(g118, strategy):
     np.testing.assert_array_equal(ca.get_row_status(), so)
     assert np.all(so == RowStatus.CONVERGED)
     if strategy == "refactor_every":
+        # plain Newton: the oracle's iterates, so its iteration counts and voltages to rounding
         np.testing.assert_array_equal(ca.get_row_iterations(), io)
-    assert np.abs(ca.V_results - Vo).max() < TOL_V_FP64
+        assert np.abs(ca.V_results - Vo).max() < TOL_V_FP64
+    else:
+        # chord / Broyden steps converge to the same solution along other iterates
+        assert np.abs(ca.V_results - Vo).max() < TOL_V_MIXED
     loading, _, _ = ca.branch_loading()
     for r in range(len(rows)):
         ref = O.branch_loading(Vo[r], h.branch_from, h.branch_to, h.yff, h.yft, h.ytf, h.ytt, rate / h.sn_mva,
