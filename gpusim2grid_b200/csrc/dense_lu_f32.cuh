@@ -100,16 +100,21 @@ __device__ __forceinline__ void stage_tile(float* sA, float* sB, const float* A2
   asm volatile("cp.async.commit_group;\n" ::);
 }
 
-// A22[M x N] -= A21[M x 64] A12[64 x N].
+// A22[M x N] -= A21[M x 64] A12[64 x N].  With parts > 1 the CTA takes the
+// output tiles part, part + parts, ... (the CTAs of a cluster split them).
 __device__ __noinline__ void trailing_update(float* A22, const float* A21, const float* A12, int ld, int M, int N, float* sA,
-                                float* sB) {
+                                float* sB, int part = 0, int parts = 1) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tr = (warp >> 1) * 4 + (lane >> 3);  // 0..15
   const int tc = (warp & 1) * 8 + (lane & 7);    // 0..15
   const int n_ti = (M + TM - 1) / TM, n_tj = (N + TN - 1) / TN;
   const int n_tiles = n_ti * n_tj;
-  stage_tile(sA, sB, A21, A12, ld, M, N, 0, 0);
-  for (int t = 0; t < n_tiles; ++t) {
+  if (part >= n_tiles) {
+    __syncthreads();
+    return;
+  }
+  stage_tile(sA, sB, A21, A12, ld, M, N, (part / n_tj) * TM, (part % n_tj) * TN);
+  for (int t = part; t < n_tiles; t += parts) {
     const int i0 = (t / n_tj) * TM, j0 = (t % n_tj) * TN;
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
@@ -141,8 +146,8 @@ __device__ __noinline__ void trailing_update(float* A22, const float* A21, const
         for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
     __syncthreads();  // every thread is done reading this tile's operands
-    if (t + 1 < n_tiles) {
-      const int t1 = t + 1;
+    if (t + parts < n_tiles) {
+      const int t1 = t + parts;
       stage_tile(sA, sB, A21, A12, ld, M, N, (t1 / n_tj) * TM, (t1 % n_tj) * TN);
     }
     // epilogue in batches of EB rows: all loads of a batch are issued before
@@ -258,9 +263,11 @@ __device__ __forceinline__ void subst64(float (&x)[KP], const float* M, const fl
   }
 }
 
-// L21 = A21 U11^-1 (x U11 = a per row), one thread per row.
-__device__ __noinline__ void trsm_rows(float* A21, int ld, int M, const float* D, const float* rp) {
-  for (int r = threadIdx.x; r < M; r += BS) {
+// L21 = A21 U11^-1 (x U11 = a per row), one thread per row (with parts > 1:
+// rows part * BS + tid, then every parts * BS).
+__device__ __noinline__ void trsm_rows(float* A21, int ld, int M, const float* D, const float* rp, int part = 0,
+                                       int parts = 1) {
+  for (int r = part * BS + threadIdx.x; r < M; r += BS * parts) {
     float4* row = reinterpret_cast<float4*>(A21 + (int64_t)r * ld);
     float x[KP];
 #pragma unroll
@@ -279,8 +286,8 @@ __device__ __noinline__ void trsm_rows(float* A21, int ld, int M, const float* D
 
 // U12 = L11^-1 A12 (per column: y^T L11^T = a^T, L11^T upper with unit
 // diagonal, given by its rows LT = rows of L11^T), one thread per column.
-__device__ __noinline__ void trsm_cols(float* A12, int ld, int N, const float* LT) {
-  for (int c = threadIdx.x; c < N; c += BS) {
+__device__ __noinline__ void trsm_cols(float* A12, int ld, int N, const float* LT, int part = 0, int parts = 1) {
+  for (int c = part * BS + threadIdx.x; c < N; c += BS * parts) {
     float y[KP];
     const float* src = A12 + c;
 #pragma unroll
@@ -337,6 +344,64 @@ __device__ void lu(float* A, int n, int ld, float* smem, double pfloor) {
       trailing_update(A22, A21, A12, ld, m, m, sA, sB);
     }
     __syncthreads();
+  }
+}
+
+// Barrier over every thread of every CTA of the cluster, ordering the
+// memory accesses before it (global and distributed shared) before those
+// after it.  Block-uniform calls only.
+__device__ __forceinline__ void cluster_sync_all() {
+  __threadfence();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// The same LU as lu(), by the `parts` CTAs of a cluster together (this CTA
+// has rank `part`); A in global memory, every CTA with its own scratch.
+// Each CTA factors the diagonal block itself (the 64 x 64 block is cheap and
+// every CTA needs it in its own shared memory), the row and column
+// substitutions and the trailing-update tiles are split by rank, and three
+// cluster barriers per panel order the stages.  Every element goes through
+// the same operations in the same order as in lu(), so the factor is
+// bit-identical.  Every CTA of the cluster must call it with the same n.
+__device__ void lu_cluster(float* A, int n, int ld, float* smem, double pfloor, int part, int parts) {
+  float* D = smem;
+  float* rp = D + Smem::d_elems;
+  float* sA = rp + Smem::r_elems;
+  float* sB = sA + Smem::a_elems;
+  const int tid = threadIdx.x;
+  for (int k0 = 0; k0 < n; k0 += KP) {
+    const int kb = min(KP, n - k0);
+    float* Akk = A + (int64_t)k0 * ld + k0;
+    for (int idx = tid; idx < KP * KP; idx += BS) {
+      const int r = idx >> 6, c = idx & 63;
+      D[r * SD + c] = (r < kb && c < kb) ? Akk[(int64_t)r * ld + c] : (r == c ? 1.f : 0.f);
+    }
+    __syncthreads();
+    factor_diag(D, rp, pfloor);
+    cluster_sync_all();  // every CTA holds the block: rank 0 may write it back below
+    const int m = n - k0 - kb;  // > 0 only with kb == 64
+    float* A21 = A + (int64_t)(k0 + kb) * ld + k0;
+    float* A12 = A + (int64_t)k0 * ld + k0 + kb;
+    float* A22 = A + (int64_t)(k0 + kb) * ld + k0 + kb;
+    if (m > 0) {
+      float* LT = sA;
+      for (int idx = tid; idx < KP * KP; idx += BS) {
+        const int r = idx >> 6, c = idx & 63;
+        LT[c * SD + r] = r > c ? D[r * SD + c] : 0.f;
+      }
+      __syncthreads();
+      trsm_rows(A21, ld, m, D, rp, part, parts);
+      trsm_cols(A12, ld, m, LT, part, parts);
+    }
+    if (part == 0)
+      for (int idx = tid; idx < kb * kb; idx += BS) {
+        const int r = idx / kb, c = idx % kb;
+        Akk[(int64_t)r * ld + c] = D[r * SD + c];
+      }
+    cluster_sync_all();  // L21, U12 and the diagonal block complete
+    if (m > 0) trailing_update(A22, A21, A12, ld, m, m, sA, sB, part, parts);
+    cluster_sync_all();  // A22 complete
   }
 }
 

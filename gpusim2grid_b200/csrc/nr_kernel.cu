@@ -832,9 +832,18 @@ __device__ __noinline__ void skip_row_outputs(const SweepArgs a, const int row, 
 // rescued: it already began from the rescue voltage.
 constexpr int NO_RESCUE_BIT = 1 << 30;
 
+// A row solved by the leading CTA of a cluster whose other CTAs join its
+// dense tail LU (sweep_kernel_cluster): the command word the leader posts in
+// its shared memory, and the cluster size.
+constexpr int CLUSTER_CMD_LU = 1, CLUSTER_CMD_DONE = 2;
+struct ClusterLu {
+  int* cmd;
+  int parts;
+};
+
 template <typename T>
 __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, const int row_arg, char* ws,
-                                          const RowShared<T>& sh, PhaseProf& prof) {
+                                          const RowShared<T>& sh, PhaseProf& prof, const ClusterLu* cl = nullptr) {
   const int tid = threadIdx.x;
   const int row = row_arg & ~NO_RESCUE_BIT;
   // a row that began from the rescue voltage (the base V, chosen by start
@@ -1087,7 +1096,22 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
 
       prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
-      if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+      if (P.nt > 0) {
+        if constexpr (sizeof(T) == 4) {
+          if (cl != nullptr) {
+            // the cluster's other CTAs join: post the command, two barriers
+            // (posted; read by all), then the shared factorization
+            if (tid == 0) *cl->cmd = CLUSTER_CMD_LU;
+            gs2g::dense32::cluster_sync_all();
+            gs2g::dense32::cluster_sync_all();
+            gs2g::dense32::lu_cluster(S, P.nt, P.ld, s_dense, a.pivot_floor, 0, cl->parts);
+          } else {
+            dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+          }
+        } else {
+          dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
+        }
+      }
       fHV = HV;
       fS = S;
       comp_on = false;
@@ -1180,6 +1204,104 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM) sweep_kernel(const D
   }
 }
 
+// The rank of this CTA in its cluster, and an int of the leading CTA's
+// shared memory read through distributed shared memory.
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ int ld_shared_rank0(const int* p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  unsigned ra;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(ra) : "r"(a), "r"(0));
+  int v;
+  asm volatile("ld.shared::cluster.u32 %0, [%1];\n" : "=r"(v) : "r"(ra) : "memory");
+  return v;
+}
+
+// The single-row sweep with a cluster of HANDOFF_CLUSTER CTAs per row (FP32
+// factors): the leading CTA (rank 0) runs the row's whole Newton loop in its
+// workspace as sweep_kernel does, and the other CTAs join each of its dense
+// tail LUs (dense32::lu_cluster), the one step whose work grows as the cube
+// of the tail.  For the few rows the chord sweep hands off, whose LUs would
+// otherwise each run on one SM after every other row has finished.  When
+// the rows outnumber the clusters, every CTA takes rows of its own instead.
+// Protocol, all through cluster barriers (every CTA passes the same number):
+// per row, the leader takes a queue entry and publishes it (barrier), every
+// CTA reads it (barrier); then for each dense LU the leader posts
+// CLUSTER_CMD_LU (barrier, read, barrier) and all factor together; after the
+// row it posts CLUSTER_CMD_DONE (barrier, read, barrier).
+constexpr int HANDOFF_CLUSTER = 8;
+
+template <typename T>
+__global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
+    sweep_kernel_cluster(const DevPlan P, const SweepArgs a) {
+  static_assert(sizeof(T) == 4, "the cluster LU is the FP32 one");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_row;
+  __shared__ int s_cmd;
+  __shared__ int s_ne;
+  __shared__ int s_ek[MAX_EDITS];
+  __shared__ double2 s_ev[MAX_EDITS];
+  __shared__ double s_red[NWARP];
+  __shared__ T s_blk[64];
+  __shared__ int s_cr[1 + MAX_COMP];
+  __shared__ double s_cB[MAX_COMP * MAX_COMP];
+  __shared__ double s_cLU[MAX_COMP * MAX_COMP];
+  __shared__ int s_cpiv[MAX_COMP];
+  __shared__ double s_cw[MAX_COMP];
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw), s_cr, s_cB, s_cLU, s_cpiv,
+                        s_cw};
+  const int rank = (int)cluster_ctarank();
+  const int n_rows = a.n_rows_dev != nullptr ? *a.n_rows_dev : a.n_rows;
+  PhaseProf prof;
+  if ((int64_t)n_rows * HANDOFF_CLUSTER > gridDim.x) {
+    // more rows than clusters: sharing the LUs would leave rows waiting for a
+    // cluster, so every CTA runs rows of its own, as sweep_kernel does (the
+    // choice is the same for the whole grid: no cluster barrier is used)
+    prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
+    char* own = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
+    for (;;) {
+      if (threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
+      __syncthreads();
+      const int q = s_row;
+      __syncthreads();  // every thread has read s_row before it is overwritten
+      if (q >= n_rows) break;
+      solve_row<T>(P, a, a.row_map != nullptr ? a.row_map[q] : q, own, sh, prof);
+    }
+    prof.flush(a.phase_cycles);
+    return;
+  }
+  // the row lives in the leader's workspace
+  char* ws = a.workspace + (int64_t)(blockIdx.x - rank) * a.ws_stride;
+  T* S = reinterpret_cast<T*>(ws + ws_layout<T>(P).S);
+  prof.init(a.phase_cycles != nullptr && threadIdx.x == 0 && rank == 0);
+  const ClusterLu cl{&s_cmd, HANDOFF_CLUSTER};
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
+    dense32::cluster_sync_all();
+    const int q = ld_shared_rank0(&s_row);
+    dense32::cluster_sync_all();
+    if (q >= n_rows) break;
+    if (rank == 0) {
+      solve_row<T>(P, a, a.row_map != nullptr ? a.row_map[q] : q, ws, sh, prof, &cl);
+      if (threadIdx.x == 0) s_cmd = CLUSTER_CMD_DONE;
+      dense32::cluster_sync_all();
+      dense32::cluster_sync_all();
+    } else {
+      for (;;) {
+        dense32::cluster_sync_all();
+        const int cmd = ld_shared_rank0(&s_cmd);
+        dense32::cluster_sync_all();
+        if (cmd != CLUSTER_CMD_LU) break;
+        dense32::lu_cluster(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, HANDOFF_CLUSTER);
+      }
+    }
+  }
+  prof.flush(a.phase_cycles);
+}
+
 // One persistent launch over the rows of several grids: row r of the
 // launch is row r - row_begin[g] of grid g (row_begin ascending, n_grids
 // <= MAX_GRIDS).  A CTA loads a grid's plan and arguments into shared
@@ -1264,6 +1386,9 @@ cudaError_t opt_in_smem() {
   e = cudaFuncSetAttribute(sweep_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<double>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(sweep_kernel_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem_bytes<float>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_kernel_cluster<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem_bytes<float>());
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_kernel_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1359,6 +1484,18 @@ int launch_chord_multi(const GridEntry* d_grids, int n_grids, int smem, unsigned
 }
 
 int chord_smem(const DevPlan& P, int prec) { return prec == 1 ? chord_smem_bytes<float>(P) : chord_smem_bytes<double>(P); }
+
+int handoff_cluster_size() { return HANDOFF_CLUSTER; }
+
+int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int n_ctas, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0 || n_ctas % HANDOFF_CLUSTER != 0 || a.inverse_out != nullptr || a.factor_only)
+    return (int)cudaErrorInvalidValue;
+  const cudaError_t e = opt_in_smem();
+  if (e != cudaSuccess) return (int)e;
+  sweep_kernel_cluster<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
+  return (int)cudaGetLastError();
+}
 
 int launch_sweep(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);

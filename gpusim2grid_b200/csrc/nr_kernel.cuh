@@ -178,6 +178,13 @@ int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
 // CTAs that fit at once for `prec` (for sizing the workspace).
 int sweep_ctas(int prec, int device);
 
+// The single-row sweep in FP32 with a cluster of handoff_cluster_size() CTAs
+// per row: the cluster's leading CTA runs the row (its workspace: the
+// leader's block index times ws_stride), and all of them share each of its
+// dense tail LUs.  n_ctas a multiple of the cluster size.
+int handoff_cluster_size();
+int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int n_ctas, void* stream);
+
 // Several grids in one persistent launch (see sweep_kernel_multi): the plan
 // and the per-grid launch arguments of each grid (SweepArgs fields n_rows,
 // ybus, v0, sbus, edits, skip, options and outputs; its queue, workspace and

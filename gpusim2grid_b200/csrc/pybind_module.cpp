@@ -227,6 +227,7 @@ class Session {
   }
 
   void set_chord(int mode) { check(gs2g_session_set_chord(h(), mode)); }
+  void set_handoff(int cluster) { check(gs2g_session_set_handoff(h(), cluster)); }
 
   uintptr_t start_rows_buffer(int n_rows) {
     double* p = nullptr;
@@ -563,6 +564,7 @@ PYBIND11_MODULE(_gs2g, m) {
            py::arg("rescue") = false, py::arg("iters_per_round") = 1)
       .def("branch_loading", &Session::branch_loading)
       .def("set_chord", &Session::set_chord, py::arg("mode"))
+      .def("set_handoff", &Session::set_handoff, py::arg("cluster"))
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)

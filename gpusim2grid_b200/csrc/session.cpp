@@ -126,6 +126,7 @@ struct gs2g_session {
   DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
   DevBuf d_chord_steps;    // Newton steps the last chord sweep took on the base factor
   int chord = 2;           // policy 2: 0 single-row sweep, 1 chord sweep, 2 chord sweep with Broyden steps
+  int handoff_cluster = 1;  // mixed precision: the chord sweep's hand-offs run with a cluster of CTAs per row
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -513,7 +514,18 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.alt_v0 = nullptr;
     a.alt_s = nullptr;
   }
-  if (n_rows > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
+  // hand-offs in mixed precision with a dense tail worth sharing: a cluster
+  // of CTAs per row (the rows are few and each of their LUs would otherwise
+  // run on one SM after every other row has finished)
+  const int csize = gs2g::handoff_cluster_size();
+  const bool cluster = chord && s->handoff_cluster && o.precision == GS2G_PREC_MIXED && s->dplan.nt >= 64 &&
+                       n_ctas >= csize;
+  if (n_rows > 0 && cluster) {
+    const int n_cl = std::max(1, std::min(n_ctas / csize, n_rows));
+    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, n_cl * csize, s->stream), "hand-off cluster launch");
+  } else if (n_rows > 0) {
+    ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
+  }
   ck(cudaEventRecord(s->ev1, s->stream), "event");
   ck(cudaStreamSynchronize(s->stream), "sweep");
   float ms = 0;
@@ -662,6 +674,14 @@ int gs2g_session_set_chord(gs2g_session* s, int mode) {
   if (!s) throw std::invalid_argument("session_set_chord: NULL session");
   if (mode < 0 || mode > 2) throw std::invalid_argument("session_set_chord: mode must be 0, 1 or 2");
   s->chord = mode;
+  GS2G_CATCH
+}
+
+int gs2g_session_set_handoff(gs2g_session* s, int cluster) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_set_handoff: NULL session");
+  if (cluster != 0 && cluster != 1) throw std::invalid_argument("session_set_handoff: cluster must be 0 or 1");
+  s->handoff_cluster = cluster;
   GS2G_CATCH
 }
 

@@ -176,6 +176,13 @@ int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int
  * convergence); mode 1: plain chord steps, the same decisions as the
  * single-row sweep; mode 0: every row in the single-row sweep. */
 int gs2g_session_set_chord(gs2g_session* s, int mode);
+/* Hand-offs of the chord sweep in mixed precision (rows that factor their
+ * own Jacobian): cluster = 1 (default) runs each such row on a cluster of 8
+ * CTAs, the leading CTA running the row and all 8 sharing each of its dense
+ * tail LUs (bit-identical to the one-CTA factorization); 0 runs each on one
+ * CTA.  Grids whose dense tail is under 64 always use one CTA.  No
+ * counterpart in the reference (its batch LU has no per-row kernel). */
+int gs2g_session_set_handoff(gs2g_session* s, int cluster);
 int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
 int gs2g_get_device(const gs2g_session* s, int* device);
 

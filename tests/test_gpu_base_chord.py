@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import TOL_V_MIXED
-from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, RowStatus
+from gpusim2grid_b200 import ContingencyAnalysisGPU, InjectionSweepGPU, RowStatus, ScenarioSweepGPU
 from gpusim2grid_b200.synthetic import injection_scenarios, n1_branches
 
 pytestmark = pytest.mark.gpu
@@ -68,3 +68,42 @@ def test_device_rows_match_host_definitions(g118):
     np.testing.assert_array_equal(ptr.cpu().numpy(), np.cumsum([0] + [len(t) for t in trips]))
     np.testing.assert_array_equal(ids.cpu().numpy(), [b for t in trips for b in t])
     assert isinstance(sbus, torch.Tensor) and sbus.is_cuda
+
+
+@pytest.mark.parametrize("name,kind", [("case2000_synth", "n1"), ("case2000_synth", "heavy"),
+                                       ("case6500_synth", "heavy")])
+def test_cluster_handoffs_equal_one_cta_handoffs(name, kind):
+    """The chord sweep's hand-offs (rows that factor their own Jacobian) run
+    on a cluster of CTAs per row in mixed precision when every such row can
+    have a cluster (the N-1 sweep: about a dozen rows), all CTAs of the
+    cluster sharing each dense tail LU; with more hand-offs than clusters
+    (heavily loaded scenarios) every CTA takes rows of its own.  The shared
+    factorization is bit-identical to the one-CTA one, so every output must
+    be too."""
+    from gpusim2grid_b200.synthetic import grid_by_name, scenario_outages
+    g = grid_by_name(name, 0)
+    out = []
+    for cluster in (0, 1):
+        kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", tol=1e-8,
+                  start="base", strategy="base_chord")
+        if kind == "n1":
+            sw = ContingencyAnalysisGPU(g.as_tuple(), **kw)
+            sw.set_branch_data(*g.branch_data())
+            sw.add_contingencies_by_branch_id([[int(b)] for b in n1_branches(g)])
+        else:
+            n = 512
+            p, q = injection_scenarios(g, n, seed=31)
+            sw = ScenarioSweepGPU(g.as_tuple(), **kw)
+            sw.set_branch_data(*g.branch_data())
+            # heavier loading than the sweeps' scenarios, so that many rows leave the chord
+            sw.set_injections(1.25 * p, 1.25 * q, g.sn_mva)
+            sw.set_topology(scenario_outages(g, n, max_trips=2, seed=32))
+        sw.session.set_handoff(cluster)
+        sw.compute()
+        out.append((sw.V_results, sw.get_row_status(), sw.get_row_iterations(), sw.get_row_factorizations()))
+    (V0, s0, i0, f0), (V1, s1, i1, f1) = out
+    assert f0.sum() > 0  # some rows were handed off and factored their own Jacobian
+    np.testing.assert_array_equal(s0, s1)
+    np.testing.assert_array_equal(i0, i1)
+    np.testing.assert_array_equal(f0, f1)
+    np.testing.assert_array_equal(V0, V1)
