@@ -517,9 +517,9 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
             t1 = time.perf_counter()
             ca.compute()
             t2 = time.perf_counter()
-            V = ca.V_results
-            stt = ca.get_row_status()
-            r = ca.last_residuals()
+            # voltages, statuses and residuals into host memory (the
+            # session's page-locked result buffer, one DMA per array)
+            V, r, stt, itv = ca.results_view()
             t3 = time.perf_counter()
             e2e_s.append(t3 - t0)
             e2e_parts.append((t1 - t0, t2 - t1, t3 - t2, ca.timings.t_kernel_ms / 1e3))
@@ -528,7 +528,7 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
                              [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
         n_ids = sum(len(r_) for r_ in trips) if trips is not None else 0
         h2d = (4 * (n + 1) + 4 * n_ids if trips is not None else 0) + (2 * p.nbytes if p is not None else 0)
-        d2h = V.nbytes + stt.nbytes + r.nbytes
+        d2h = V.nbytes + stt.nbytes + r.nbytes + itv.nbytes
         e2e_obj = {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(d2h), "split": e2e_split}
 

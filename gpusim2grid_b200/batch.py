@@ -70,7 +70,7 @@ def _ids_csr(rows):
 class _BatchSweep:
     def __init__(self, grid, *, init_from_n_powerflow=True, precision="fp64", nb_iter=4, max_iter_base=10,
                  tol_base=1e-8, device=None, scheduling=None, nb_iter_per_round=1, tol=None, start="base",
-                 strategy="refactor_every", **_ignored):
+                 strategy="refactor_every", handle_disconnected_grid=False, **_ignored):
         d = grid_arrays(grid)
         self._d = d
         self._prec = resolve_precision(precision)
@@ -93,6 +93,7 @@ class _BatchSweep:
             self._base_iters = it
         self.start = start
         self.strategy = strategy
+        self.handle_disconnected_grid = handle_disconnected_grid
         self.refactor_ratio = 0.3
         self.max_reuse = 3
         # mixed precision, continuous schedule: rows that end MAX_ITER or
@@ -123,6 +124,21 @@ class _BatchSweep:
         if value < 1:
             raise ValueError("nb_iter_per_round must be >= 1")
         self._nb_iter_per_round = value
+
+    @property
+    def handle_disconnected_grid(self):
+        """A row whose trips split the grid: False (default) leaves it
+        NOT_SIMULATED with NaN voltages; True solves its largest component
+        (most buses; on a tie the one holding the lowest bus) with the other
+        buses masked -- frozen during the iteration, NaN in the results -- as
+        the reference's option of that name.  A split that strands a slack
+        bus stays NOT_SIMULATED.  Takes effect on the next compute()."""
+        return self._handle_disconnected
+
+    @handle_disconnected_grid.setter
+    def handle_disconnected_grid(self, value):
+        self._handle_disconnected = bool(value)
+        self._s.set_handle_disconnected(self._handle_disconnected)
 
     @property
     def start(self):
@@ -375,6 +391,16 @@ class _BatchSweep:
         """(n_rows, n_bus) complex voltages of the last ``compute()`` (host copy)."""
         return self._results()[0]
 
+    def results_view(self):
+        """(V, residuals, status, iterations) of the last ``compute()`` as
+        numpy views of page-locked host memory the session owns, filled by
+        one DMA per array: no further host copy.  Valid until the next
+        ``compute()`` or ``results_view()`` -- the lifetime of the reference's
+        ``V_results`` device buffer; copy what must outlive it."""
+        if not self._ran:
+            raise RuntimeError("Call compute() first.")
+        return self._s.results_view()
+
     def converged(self, tol=None):
         res = self.last_residuals()
         return res < (self.tol if tol is None else tol)
@@ -501,8 +527,10 @@ class ScenarioSweepGPU(InjectionSweepGPU):
         return self._topo is not None
 
     def get_disconnected(self):
-        """(n_rows,) bool: rows whose topology islands the grid (never solved)."""
-        return self.get_row_status() == RowStatus.NOT_SIMULATED
+        """(n_rows,) int: 1 for a row whose topology islands the grid and was
+        not solved (NaN), 0 otherwise -- a split solved on its largest
+        component under ``handle_disconnected_grid`` counts as solved."""
+        return (self.get_row_status() == RowStatus.NOT_SIMULATED).astype(np.int64)
 
 
 def compute_many(sweeps, batch_size=0):

@@ -95,6 +95,7 @@ struct ChordSlot {
   int act;    // this round: 1 solve, 2 converged, 3 diverged, 4 budget spent, 5 hand off
   int nb;     // Broyden steps stored
   int from_base;  // began from the rescue voltage (start selection): no rescue
+  int masked;     // the row masks buses (handle_disconnected_grid): handed off at once
   double nrm, last;
 };
 
@@ -478,7 +479,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
           sl[s].row = row;
           sl[s].it = 0;
           sl[s].since = 0;
-          sl[s].fresh = a.alt_v0 != nullptr;
+          sl[s].masked = a.mask_ptr != nullptr && a.mask_ptr[row + 1] > a.mask_ptr[row];
+          sl[s].fresh = a.alt_v0 != nullptr && !sl[s].masked;
           sl[s].comp = 0;
           sl[s].act = 0;
           sl[s].nb = 0;
@@ -490,7 +492,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         __syncthreads();
         const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
         bool c = false;
-        if (ed.n > 0 && Minv != nullptr && Vbase != nullptr) c = setup_compensation<T>(P, ed, Y, Vbase, Minv, shs(s));
+        if (ed.n > 0 && Minv != nullptr && Vbase != nullptr && !sl[s].masked)
+          c = setup_compensation<T>(P, ed, Y, Vbase, Minv, shs(s));
         if (tid == 0) sl[s].comp = c;
         __syncthreads();
         break;
@@ -537,7 +540,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         // whose mismatch is not finite is handed off as well, and the
         // single-row sweep steps it to the end of its round
         const bool test = q.it > 0 && q.it % (a.round_k > 1 ? a.round_k : 1) == 0;
-        if (!isfinite(q.nrm)) q.act = (rescue || !test) ? 5 : 3;
+        if (q.masked) q.act = 5;  // masked rows are solved on their own factor
+        else if (!isfinite(q.nrm)) q.act = (rescue || !test) ? 5 : 3;
         else if (test && q.nrm < a.tol) q.act = 2;
         else if (test && q.it >= a.max_iter) q.act = rescue ? 5 : 4;
         else if (!keep_factor(q.nrm, q.last, a.refactor_ratio, q.since, a.max_reuse, q.it, a.max_iter, a.tol))

@@ -437,7 +437,7 @@ __host__ __device__ __forceinline__ int64_t align256(int64_t x) { return (x + 25
 constexpr int MAX_COMP = 16;  // compensated Jacobian positions per row (base_chord)
 
 struct WsLayout {
-  int64_t V, I, F, HV, S, y, total;
+  int64_t V, I, F, HV, S, y, M, total;
 };
 
 template <typename T>
@@ -450,6 +450,7 @@ __host__ __device__ WsLayout ws_layout(const DevPlan& P) {
   w.HV = o; o = align256(o + (int64_t)P.n_hv * sizeof(T));
   w.S = o; o = align256(o + (int64_t)P.nt * P.ld * sizeof(T));
   w.y = o; o = align256(o + (int64_t)P.dim * sizeof(T));
+  w.M = o; o = align256(o + (int64_t)((P.n_bus + 31) / 32) * 4);  // masked-bus bitmap
   w.total = o;
   return w;
 }
@@ -789,8 +790,11 @@ __device__ __noinline__ void row_flows(const SweepArgs a, const int row, const d
         const double2 St = bt >= 0 ? cmul(Vt, conj2(cadd(cmul(yb[2], Vf), cmul(yb[3], Vt)))) : zero;
         const double r = fmax(hypot(Sf.x, Sf.y), hypot(St.x, St.y)) / a.br_rate[l];
         ld = (float)r;
-        lmax = fmax(lmax, r);
-        nv += r > 1.0;
+        // a branch at a masked (NaN) bus has no flow to report: NaN, not counted
+        if (!isnan(r)) {
+          lmax = fmax(lmax, r);
+          nv += r > 1.0;
+        }
       }
     }
     a.loading_out[(int64_t)row * a.n_branch + l] = ld;
@@ -896,13 +900,27 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
     const double2* sb = reinterpret_cast<const double2*>(a.sbus) + (int64_t)row * a.sbus_stride;
     for (int i = tid; i < n; i += BS) V[i] = v0[i];
+    // buses outside the row's largest component (handle_disconnected_grid)
+    unsigned* mbits = reinterpret_cast<unsigned*>(ws + L.M);
+    const bool has_mask = a.mask_ptr != nullptr && a.mask_ptr[row + 1] > a.mask_ptr[row];
+    if (has_mask) {
+      for (int w = tid; w < (n + 31) / 32; w += BS) mbits[w] = 0u;
+      __syncthreads();
+      for (int q = a.mask_ptr[row] + tid; q < a.mask_ptr[row + 1]; q += BS) {
+        const int b = a.mask_bus[q];
+        atomicOr(mbits + (b >> 5), 1u << (b & 31));
+      }
+    }
+    auto masked = [&](int b) { return has_mask && ((mbits[b >> 5] >> (b & 31)) & 1u); };
     __syncthreads();
     const RowEdits ed{s_ne, s_ek, s_ev};
     prof.start();
 
     int it_total = 0, status = ROW_MAX_ITER, n_factor = 0;
     double nrm = NAN;
-    bool check_alt = a.alt_v0 != nullptr && !a.fixed_iters && !a.factor_only;
+    // a masked row starts from its own start on its own factor (start
+    // selection and the base factor know nothing of its masked rows)
+    bool check_alt = a.alt_v0 != nullptr && !a.fixed_iters && !a.factor_only && !has_mask;
     // attempt 0 starts from the row's own start voltage; with a rescue
     // voltage, a row that ends unconverged there gets one more attempt from
     // it, with a fresh Newton budget (iterations and factorizations add up)
@@ -911,7 +929,8 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     int it = (attempt == 0 && a.iters_in != nullptr) ? a.iters_in[row] : 0;
     // policy 2 starts on the base case's factor (shared by every CTA, read
     // only) and moves to the row's own factor at its first refactor
-    const bool on_base = a.refactor_policy == 2 && a.base_ws != nullptr && attempt == 0 && !a.factor_only;
+    const bool on_base =
+        a.refactor_policy == 2 && a.base_ws != nullptr && attempt == 0 && !a.factor_only && !has_mask;
     const T* fHV = on_base ? reinterpret_cast<const T*>(a.base_ws + L.HV) : HV;
     const T* fS = on_base ? reinterpret_cast<const T*>(a.base_ws + L.S) : S;
     bool have_factor = on_base;
@@ -940,6 +959,12 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       for (int i = tid; i < n; i += BS) {
         const double2 s = csub(cmul(V[i], conj2(I[i])), sb[i]);
         const int fp = P.fP[i], fq = P.fQ[i];
+        if (masked(i)) {
+          // a masked bus: identity row, zero mismatch, out of the norm
+          if (fp >= 0) F[fp] = 0.0;
+          if (fq >= 0) F[fq] = 0.0;
+          continue;
+        }
         if (fp >= 0) {
           F[fp] = -s.x;
           const double ax = fabs(s.x);
@@ -1042,7 +1067,15 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
           const double2 vn = make_double2(Vj.x * inv, Vj.y * inv);
           dVm = cmul(Vi, conj2(cmul(yk, vn)));
         }
-        const double vals[4] = {dVa.x, dVm.x, dVa.y, dVm.y};
+        double vals[4] = {dVa.x, dVm.x, dVa.y, dVm.y};
+        if (masked(i) || masked(j)) {
+          // a masked bus's rows are identity rows; live rows see no coupling to it
+          const double one = (i == j) ? 1.0 : 0.0;
+          vals[0] = one;
+          vals[1] = 0.0;
+          vals[2] = 0.0;
+          vals[3] = one;
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int dst = P.jmap[4 * k + q];
@@ -1156,6 +1189,12 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     __syncthreads();
     }  // attempts
 
+    // masked buses are reported NaN (their voltage was frozen, not solved)
+    if (has_mask) {
+      for (int i = tid; i < n; i += BS)
+        if (masked(i)) V[i] = make_double2(NAN, NAN);
+      __syncthreads();
+    }
     // ---- branch flows and limit check as the row leaves --------------------
     if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
 

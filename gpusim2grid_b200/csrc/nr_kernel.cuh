@@ -62,6 +62,12 @@ struct SweepArgs {
   const int* edit_k;      // Ybus entry index
   const double* edit_val; // complex delta to SUBTRACT
   const int* row_skip;    // [n_rows] nonzero: NOT_SIMULATED (nullptr: none)
+  // handle_disconnected_grid: buses of row r outside its largest component,
+  // mask_bus[mask_ptr[r] .. mask_ptr[r + 1]) (nullptr: none).  Their P/Q
+  // equations become identity rows with zero mismatch (the voltage stays
+  // frozen), they leave the norm, and their voltages are reported NaN.
+  const int* mask_ptr;
+  const int* mask_bus;
   int max_iter;
   double tol;
   int fixed_iters;        // 1: exactly max_iter steps then the residual; 0: stop at tol

@@ -228,6 +228,7 @@ class Session {
 
   void set_chord(int mode) { check(gs2g_session_set_chord(h(), mode)); }
   void set_handoff(int cluster) { check(gs2g_session_set_handoff(h(), cluster)); }
+  void set_handle_disconnected(bool on) { check(gs2g_session_set_handle_disconnected(h(), on ? 1 : 0)); }
 
   uintptr_t start_rows_buffer(int n_rows) {
     double* p = nullptr;
@@ -321,6 +322,26 @@ class Session {
     }
     check(rc);
     return py::make_tuple(V, res, st, it);
+  }
+
+  // numpy views of the session's pinned host copy of the last results
+  // (gs2g_get_results_host), kept alive by this session object; valid until
+  // the next results_view(), run or close
+  py::tuple results_view(py::object self) {
+    double *v = nullptr, *r = nullptr;
+    int *st = nullptr, *it = nullptr;
+    int rc;
+    {
+      py::gil_scoped_release nogil;
+      rc = gs2g_get_results_host(h(), &v, &r, &st, &it);
+    }
+    check(rc);
+    const py::ssize_t nr = gs2g_n_rows(h());
+    py::array_t<cplx> V({nr, (py::ssize_t)n_bus_}, reinterpret_cast<cplx*>(v), self);
+    py::array_t<double> res({nr}, r, self);
+    py::array_t<int> sa({nr}, st, self);
+    py::array_t<int> ia({nr}, it, self);
+    return py::make_tuple(V, res, sa, ia);
   }
 
   py::array_t<int> factor_counts() const {
@@ -565,6 +586,7 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("branch_loading", &Session::branch_loading)
       .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("set_handoff", &Session::set_handoff, py::arg("cluster"))
+      .def("set_handle_disconnected", &Session::set_handle_disconnected, py::arg("on"))
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,
            py::arg("force_tau") = -1)
       .def("set_sbus", &Session::set_sbus)
@@ -579,6 +601,7 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("factor_counts", &Session::factor_counts)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)
+      .def("results_view", [](py::object self) { return self.cast<Session&>().results_view(self); })
       .def("device_results", &Session::device_results)
       .def("dlpack", &Session::dlpack)
       .def("device_rows", &Session::device_rows)

@@ -114,8 +114,13 @@ struct gs2g_session {
 
   // assembled rows on the device
   int n_rows = 0;
-  bool rows_have_sbus = false, rows_have_edits = false, rows_have_skip = false;
+  bool rows_have_sbus = false, rows_have_edits = false, rows_have_skip = false, rows_have_mask = false;
   DevBuf d_sbus_rows, d_edit_ptr, d_edit_k, d_edit_val, d_row_skip;
+  // handle_disconnected_grid: a row whose trips split the grid solves the
+  // largest component, the other buses masked (their voltages NaN)
+  int handle_disconnected = 0;
+  std::vector<uint8_t> is_slack;      // buses in neither pv nor pq (the angle reference)
+  DevBuf d_mask_ptr, d_mask_bus;      // masked buses per assembled row (CSR)
   DevBuf d_v_out, d_res, d_status, d_iters, d_factors;
   DevBuf d_ws, d_queue, d_phase;
   DevBuf d_multi;  // grid table of gs2g_run_multi (when this session leads)
@@ -135,6 +140,9 @@ struct gs2g_session {
   int last_rows_run = 0;
   // pinned double buffer for large result copies (see d2h_staged)
   mutable void* h_stage = nullptr;
+  // pinned host copy of the last run's results (gs2g_get_results_host)
+  void* h_res = nullptr;
+  size_t h_res_bytes = 0;
   mutable cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
 
@@ -294,6 +302,7 @@ void assemble_rows(gs2g_session* s) {
   s->rows_have_sbus = s->n_inj > 0;
   s->rows_have_edits = s->n_ctg > 0;
   s->rows_have_skip = false;
+  s->rows_have_mask = false;
   if (nr == 0) {
     s->rows_dirty = false;
     return;
@@ -310,6 +319,8 @@ void assemble_rows(gs2g_session* s) {
     std::vector<uint8_t> skip(nr, 0);
     std::vector<int> uniq;
     bool any_skip = false;
+    std::vector<int> mptr(nr + 1, 0), mbus;  // masked buses per row (handle_disconnected)
+    std::vector<int> comp_size, comp_min;
     for (int r = 0; r < nr; ++r) {
       uniq.assign(s->ctg_ids.begin() + s->ctg_ptr[r], s->ctg_ids.begin() + s->ctg_ptr[r + 1]);
       std::sort(uniq.begin(), uniq.end());
@@ -329,13 +340,53 @@ void assemble_rows(gs2g_session* s) {
           }
           island = comps > 1;
         }
-        if (island) {
+        bool masked_ok = false;
+        if (island && s->handle_disconnected && s->base_components == 1) {
+          // the largest component is solved, the other buses are masked
+          // (compute_component_masks, contingency_analysis_helper.cpp:657):
+          // largest by bus count, on a tie the one holding the lowest bus;
+          // a row that would mask an angle reference bus is not simulated
+          DSU d(n);
+          size_t ui = 0;
+          for (int l = 0; l < s->n_branch; ++l) {
+            while (ui < uniq.size() && uniq[ui] < l) ++ui;
+            if (ui < uniq.size() && uniq[ui] == l) continue;
+            if (s->br_from[l] < 0 || s->br_to[l] < 0) continue;
+            d.u(s->br_from[l], s->br_to[l]);
+          }
+          comp_size.assign(n, 0);
+          comp_min.assign(n, n);
+          for (int b = 0; b < n; ++b) {
+            const int c = d.f(b);
+            ++comp_size[c];
+            comp_min[c] = std::min(comp_min[c], b);
+          }
+          int main_c = -1;
+          for (int b = 0; b < n; ++b) {
+            const int c = d.f(b);
+            if (c != b) continue;  // one visit per component (its root)
+            if (main_c < 0 || comp_size[c] > comp_size[main_c] ||
+                (comp_size[c] == comp_size[main_c] && comp_min[c] < comp_min[main_c]))
+              main_c = c;
+          }
+          masked_ok = true;
+          const size_t m0 = mbus.size();
+          for (int b = 0; b < n && masked_ok; ++b) {
+            if (d.f(b) == main_c) continue;
+            if (s->is_slack[b]) masked_ok = false;
+            mbus.push_back(b);
+          }
+          if (!masked_ok) mbus.resize(m0);
+        }
+        if (island && !masked_ok) {
           skip[r] = 1;
           any_skip = true;
           eptr[r + 1] = (int)ek.size();
+          mptr[r + 1] = (int)mbus.size();
           continue;
         }
       }
+      mptr[r + 1] = (int)mbus.size();
       std::map<int, std::complex<double>> acc;
       for (int l : uniq) {
         const double* v[4] = {&s->yff[2 * l], &s->ytt[2 * l], &s->yft[2 * l], &s->ytf[2 * l]};
@@ -362,6 +413,13 @@ void assemble_rows(gs2g_session* s) {
     if (!ek.empty()) {
       ck(cudaMemcpy(s->d_edit_k.p, ek.data(), ek.size() * sizeof(int), cudaMemcpyHostToDevice), "upload edits");
       ck(cudaMemcpy(s->d_edit_val.p, ev.data(), ev.size() * sizeof(double), cudaMemcpyHostToDevice), "upload edits");
+    }
+    if (!mbus.empty()) {
+      s->d_mask_ptr.ensure(mptr.size() * sizeof(int));
+      s->d_mask_bus.ensure(mbus.size() * sizeof(int));
+      ck(cudaMemcpy(s->d_mask_ptr.p, mptr.data(), mptr.size() * sizeof(int), cudaMemcpyHostToDevice), "upload masks");
+      ck(cudaMemcpy(s->d_mask_bus.p, mbus.data(), mbus.size() * sizeof(int), cudaMemcpyHostToDevice), "upload masks");
+      s->rows_have_mask = true;
     }
     if (any_skip) {
       std::vector<int> sk(skip.begin(), skip.end());
@@ -399,6 +457,8 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.edit_k = use_rows && s->rows_have_edits ? s->d_edit_k.as<int>() : nullptr;
   a.edit_val = use_rows && s->rows_have_edits ? s->d_edit_val.as<double>() : nullptr;
   a.row_skip = use_rows && s->rows_have_skip ? s->d_row_skip.as<int>() : nullptr;
+  a.mask_ptr = use_rows && s->rows_have_mask ? s->d_mask_ptr.as<int>() : nullptr;
+  a.mask_bus = use_rows && s->rows_have_mask ? s->d_mask_bus.as<int>() : nullptr;
   a.max_iter = o.max_iter;
   a.tol = o.tol;
   a.fixed_iters = o.fixed_iters;
@@ -653,6 +713,9 @@ int gs2g_session_create(int device, int n_bus, const int* ybus_indptr, const int
   s->y_ix = ix;
   s->pv.assign(pv, pv + n_pv);
   s->pq.assign(pq, pq + n_pq);
+  s->is_slack.assign(n_bus, 1);
+  for (int i = 0; i < n_pv; ++i) s->is_slack[pv[i]] = 0;
+  for (int i = 0; i < n_pq; ++i) s->is_slack[pq[i]] = 0;
   s->vinit.assign(vinit, vinit + 2 * n_bus);
   s->sbus.assign(sbus, sbus + 2 * n_bus);
   ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
@@ -674,6 +737,15 @@ int gs2g_session_set_chord(gs2g_session* s, int mode) {
   if (!s) throw std::invalid_argument("session_set_chord: NULL session");
   if (mode < 0 || mode > 2) throw std::invalid_argument("session_set_chord: mode must be 0, 1 or 2");
   s->chord = mode;
+  GS2G_CATCH
+}
+
+int gs2g_session_set_handle_disconnected(gs2g_session* s, int on) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_set_handle_disconnected: NULL session");
+  if (on != 0 && on != 1) throw std::invalid_argument("session_set_handle_disconnected: on must be 0 or 1");
+  if (s->handle_disconnected != on) s->rows_dirty = true;
+  s->handle_disconnected = on;
   GS2G_CATCH
 }
 
@@ -717,6 +789,7 @@ int gs2g_session_destroy(gs2g_session* s) {
     for (cudaEvent_t e : s->ev_stage)
       if (e) cudaEventDestroy(e);
     if (s->h_stage) cudaFreeHost(s->h_stage);
+    if (s->h_res) cudaFreeHost(s->h_res);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
   }
@@ -1487,6 +1560,35 @@ void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes)
   }
 }
 }  // namespace
+
+int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int** status, int** iters) {
+  GS2G_TRY
+  if (!s || !v || !residuals || !status || !iters) throw std::invalid_argument("get_results_host: NULL argument");
+  DeviceGuard g(s->device);
+  const size_t nr = s->last_rows_run, n = s->n_bus;
+  const size_t bv = nr * n * 2 * sizeof(double), br = nr * sizeof(double), bi = nr * sizeof(int);
+  const size_t o_r = bv, o_s = o_r + br, o_i = o_s + bi, total = std::max<size_t>(o_i + bi, 16);
+  if (s->h_res_bytes < total) {
+    if (s->h_res) ck(cudaFreeHost(s->h_res), "free pinned results");
+    s->h_res = nullptr;
+    s->h_res_bytes = 0;
+    ck(cudaMallocHost(&s->h_res, total), "pinned results");
+    s->h_res_bytes = total;
+  }
+  char* h = static_cast<char*>(s->h_res);
+  if (nr) {
+    ck(cudaMemcpyAsync(h, s->d_v_out.p, bv, cudaMemcpyDeviceToHost, s->stream), "read results");
+    ck(cudaMemcpyAsync(h + o_r, s->d_res.p, br, cudaMemcpyDeviceToHost, s->stream), "read residuals");
+    ck(cudaMemcpyAsync(h + o_s, s->d_status.p, bi, cudaMemcpyDeviceToHost, s->stream), "read status");
+    ck(cudaMemcpyAsync(h + o_i, s->d_iters.p, bi, cudaMemcpyDeviceToHost, s->stream), "read iters");
+    ck(cudaStreamSynchronize(s->stream), "read results");
+  }
+  *v = reinterpret_cast<double*>(h);
+  *residuals = reinterpret_cast<double*>(h + o_r);
+  *status = reinterpret_cast<int*>(h + o_s);
+  *iters = reinterpret_cast<int*>(h + o_i);
+  GS2G_CATCH
+}
 
 int gs2g_get_results(const gs2g_session* s, double* v_out, double* residuals, int* status, int* iters) {
   GS2G_TRY

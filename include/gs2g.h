@@ -183,6 +183,17 @@ int gs2g_session_set_chord(gs2g_session* s, int mode);
  * CTA.  Grids whose dense tail is under 64 always use one CTA.  No
  * counterpart in the reference (its batch LU has no per-row kernel). */
 int gs2g_session_set_handoff(gs2g_session* s, int cluster);
+/* handle_disconnected_grid (the reference's facade option,
+ * src/gpusim2grid/contingency_analysis/gpu_facade.py:349, :544): on = 1
+ * solves a row whose trips split the grid on its largest component -- the
+ * most buses, on a tie the component holding the lowest bus
+ * (compute_component_masks, src/_cpp/contingency_analysis_helper.cpp:657)
+ * -- with every other bus masked: identity Jacobian rows and zero mismatch
+ * for its P/Q equations (apply_bus_mask_kernel, src/_cpp/acpf_nr_kernels.cu:219),
+ * so its voltage stays frozen, and NaN voltages for it in the results.  A
+ * row that would mask an angle-reference (slack) bus is NOT_SIMULATED, as
+ * are all splitting rows with on = 0 (default). */
+int gs2g_session_set_handle_disconnected(gs2g_session* s, int on);
 int gs2g_grid_get_info(const gs2g_session* s, gs2g_grid_info* out);
 int gs2g_get_device(const gs2g_session* s, int* device);
 
@@ -258,6 +269,14 @@ int gs2g_get_factor_counts(const gs2g_session* s, int* factors);
 int gs2g_set_branch_limits(gs2g_session* s, int n_branch, const double* rate_mva, double sn_mva);
 /* loading [n_rows x n_branch], n_violations [n_rows], max_loading [n_rows]; any may be NULL. */
 int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violations, float* max_loading);
+/* Host copies of the last run's results in page-locked memory the session
+ * owns (one DMA per array at full link speed, no copy through pageable
+ * memory): V [n_rows x n_bus] complex, residuals, status, iters.  The
+ * pointers stay valid, and their contents unchanged, until the next call of
+ * this function, the next run or destroy: the lifetime of the reference's
+ * V_results device buffer (src/gpusim2grid/contingency_analysis/gpu_facade.py:1203)
+ * and of its DLPack exports.  No counterpart for the pinned copy itself. */
+int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int** status, int** iters);
 /* Device pointers of the last run's results (valid until the next run or destroy). */
 int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
 /* Device copies of the current row definitions (uploaded first if they

@@ -203,20 +203,56 @@ def islands(n_bus, f, t, branch_ids):
     return ncomp > 1
 
 
+def main_component(n_bus, f, t, branch_ids):
+    """Boolean mask of the buses of the largest connected component once
+    ``branch_ids`` are out: the most buses, on a tie the component holding
+    the lowest bus (compute_component_masks,
+    contingency_analysis_helper.cpp:657-700: components labelled from bus 0
+    upwards, the first largest wins)."""
+    from scipy.sparse.csgraph import connected_components
+    f, t = np.asarray(f), np.asarray(t)
+    keep = (f >= 0) & (t >= 0)
+    keep[list(branch_ids)] = False
+    A = sp.coo_matrix((np.ones(keep.sum()), (f[keep], t[keep])), shape=(n_bus, n_bus))
+    _, lab = connected_components(A, directed=False)
+    # scipy labels components in order of their lowest bus, as the reference
+    counts = np.bincount(lab)
+    return lab == int(np.argmax(counts))
+
+
 def contingency_sweep(Y, V0, Sbus, pv, pq, branch_rows, f, t, yff, yft, ytf, ytt,
-                      max_iter=10, tol=1e-8, mode="continuous", k=1):
+                      max_iter=10, tol=1e-8, mode="continuous", k=1, handle_disconnected=False):
     """Solve every row (a list of tripped-branch lists).  Islanding rows are
-    NOT_SIMULATED with NaN voltages (contingency_analysis_helper.cpp:634-651)."""
+    NOT_SIMULATED with NaN voltages (contingency_analysis_helper.cpp:634-651),
+    or, with ``handle_disconnected``, solved on their largest component with
+    the other buses masked (identity rows, zero mismatch:
+    acpf_nr_kernels.cu:219; NaN voltages in the result) unless that masks a
+    slack bus (then NOT_SIMULATED).  Masking a decoupled part is the same as
+    leaving its buses out of the unknowns and the mismatch, which is how it
+    is restated here."""
     n = Y.shape[0]
+    pv, pq = np.asarray(pv), np.asarray(pq)
+    slack = np.ones(n, dtype=bool)
+    slack[pv] = False
+    slack[pq] = False
     out_V = np.full((len(branch_rows), n), np.nan + 0j)
     status = np.full(len(branch_rows), NOT_SIMULATED, dtype=np.int32)
     iters = np.zeros(len(branch_rows), dtype=np.int32)
     res = np.full(len(branch_rows), np.nan)
     for r, ids in enumerate(branch_rows):
+        live = None
         if islands(n, f, t, ids):
-            continue
+            if not handle_disconnected:
+                continue
+            live = main_component(n, f, t, ids)
+            if slack[~live].any():
+                continue
         Yr = trip_branches(Y, ids, f, t, yff, yft, ytf, ytt)
-        V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode, k)
+        if live is None:
+            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode, k)
+        else:
+            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv[live[pv]], pq[live[pq]], max_iter, tol, mode, k)
+            V = np.where(live, V, np.nan + 0j)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
 

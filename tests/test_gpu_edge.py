@@ -141,3 +141,63 @@ def test_set_injections_from_elements_needs_a_grid_object(g118):
     sw = InjectionSweepGPU(g118.as_tuple(), init_from_n_powerflow=False)
     with pytest.raises(RuntimeError, match="lightsim2grid grid"):
         sw.set_injections_from_elements(np.zeros((1, 3)), np.zeros((1, 3)), np.zeros((1, 2)))
+
+
+def test_results_view_equals_the_owned_copies(g118):
+    """results_view(): the same results as the owned host copies, from the
+    session's page-locked buffer (valid until the next compute())."""
+    ca = _ca(g118)
+    ca.add_contingencies_by_branch_id([[int(b)] for b in n1_branches(g118)[:20]])
+    ca.compute()
+    V, res, st, it = ca.results_view()
+    np.testing.assert_array_equal(V, ca.V_results)
+    np.testing.assert_array_equal(res, ca.last_residuals())
+    np.testing.assert_array_equal(st, ca.get_row_status())
+    np.testing.assert_array_equal(it, ca.get_row_iterations())
+    assert V.shape == (20, g118.n_bus) and not V.flags.owndata
+
+
+@pytest.mark.parametrize("precision,strategy,tol_v", [("fp64", "refactor_every", 1e-9),
+                                                      ("mixed", "base_chord", 1e-6)])
+def test_handle_disconnected_grid_vs_oracle(g118, precision, strategy, tol_v):
+    """handle_disconnected_grid: rows whose trips split the grid solve the
+    largest component, with NaN voltages at the other buses, or stay
+    NOT_SIMULATED when the split strands the slack; flows of branches at a
+    masked bus are NaN and left out of the row's count and maximum."""
+    m = g118.n_branch
+    rows = [[b] for b in range(m)]
+    rng = np.random.default_rng(11)
+    for _ in range(48):
+        rows.append(sorted(int(v) for v in rng.choice(m, 2, replace=False)))
+    ca = _ca(g118, precision=precision, strategy=strategy, handle_disconnected_grid=True)
+    rate = np.full(m, 150.0)
+    ca.set_branch_limits(rate)
+    ca.add_contingencies_by_branch_id(rows)
+    ca.compute()
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    Vo, so, io, ro = O.contingency_sweep(Y, V0, S, pv, pq, rows, g118.branch_from, g118.branch_to, g118.yff,
+                                         g118.yft, g118.ytf, g118.ytt, 10, 1e-8, handle_disconnected=True)
+    st = ca.get_row_status()
+    np.testing.assert_array_equal(st, so)
+    split = np.array([O.islands(g118.n_bus, g118.branch_from, g118.branch_to, r) for r in rows])
+    assert (split & (so == RowStatus.CONVERGED)).sum() > 0  # some splits were solved
+    V = ca.V_results
+    np.testing.assert_array_equal(np.isnan(V), np.isnan(Vo))
+    ok = so == RowStatus.CONVERGED
+    assert np.nanmax(np.abs(V[ok] - Vo[ok])) < tol_v
+    assert np.all(ca.last_residuals()[ok] < 1e-8)
+    if strategy == "refactor_every":
+        np.testing.assert_array_equal(ca.get_row_iterations(), io)
+    loading, nviol, mx = ca.branch_loading()
+    for r in np.flatnonzero(ok & split):
+        ref = O.branch_loading(np.nan_to_num(Vo[r]), g118.branch_from, g118.branch_to, g118.yff, g118.yft,
+                               g118.ytf, g118.ytt, rate / g118.sn_mva, tripped=rows[r])
+        dead = np.isnan(Vo[r][g118.branch_from]) | np.isnan(Vo[r][g118.branch_to])
+        assert np.all(np.isnan(loading[r][dead & ~np.isin(np.arange(m), rows[r])]))
+        live = ~dead
+        np.testing.assert_allclose(loading[r][live], ref[live], rtol=1e-5, atol=1e-6)
+        assert np.isfinite(mx[r]) and nviol[r] == int((ref[live] > 1).sum())
+    # off: every split is NOT_SIMULATED
+    ca.handle_disconnected_grid = False
+    ca.compute()
+    assert np.all((ca.get_row_status() == RowStatus.NOT_SIMULATED) == split)

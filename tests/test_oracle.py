@@ -169,3 +169,28 @@ def test_half_open_branch_trips_only_its_live_end(g118):
     assert St[l] == 0
     f = h.branch_from[l]
     np.testing.assert_allclose(Sf[l], V[f] * np.conj(h.yff[l] * V[f]))
+
+
+def test_disconnected_rows_solve_their_largest_component(g118):
+    """handle_disconnected: a bridge outage solves the main component (power
+    balance holds on its buses), masks the rest as NaN, and a split that
+    strands the slack stays NOT_SIMULATED."""
+    bridges = np.setdiff1d(np.arange(g118.n_branch), n1_branches(g118))
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    rows = [[int(b)] for b in bridges]
+    V, st, it, res = O.contingency_sweep(Y, V0, S, pv, pq, rows, g118.branch_from, g118.branch_to, g118.yff,
+                                         g118.yft, g118.ytf, g118.ytt, 10, 1e-8, handle_disconnected=True)
+    solved = st == O.CONVERGED
+    assert solved.sum() >= 1
+    for r in np.flatnonzero(solved):
+        live = O.main_component(g118.n_bus, g118.branch_from, g118.branch_to, rows[r])
+        assert g118.slack in np.flatnonzero(live) and live.sum() >= g118.n_bus / 2
+        assert np.all(np.isnan(V[r][~live])) and np.all(np.isfinite(V[r][live]))
+        Yr = O.trip_branches(Y, rows[r], g118.branch_from, g118.branch_to, g118.yff, g118.yft, g118.ytf, g118.ytt)
+        Vz = np.where(live, V[r], 0)
+        mis = Vz * np.conj(Yr @ Vz) - S
+        pvpq = np.concatenate([pv, pq])
+        assert np.abs(mis.real[pvpq[live[pvpq]]]).max() < 1e-8 and np.abs(mis.imag[pq[live[pq]]]).max() < 1e-8
+    for r in np.flatnonzero(~solved):
+        live = O.main_component(g118.n_bus, g118.branch_from, g118.branch_to, rows[r])
+        assert not live[g118.slack] and st[r] == O.NOT_SIMULATED
