@@ -391,6 +391,38 @@ class _BatchSweep:
         """(n_rows, n_bus) complex voltages of the last ``compute()`` (host copy)."""
         return self._results()[0]
 
+    @property
+    def dim_J(self):
+        """Unknowns of a row: len(pv + pq) angles, then len(pq) magnitudes."""
+        return int(self._s.info()["dim_j"])
+
+    def solve_JT(self, rhs):
+        """Batched adjoint of the last ``compute()``: for every row r,
+        ``lam[r] = J_r^-T rhs[r]``, J_r the row's Jacobian (FP64) at its
+        converged voltage, in the reference's J layout (theta rows on sorted
+        pv + pq, then Vm rows on pq).  ``rhs`` is (n_rows, dim_J), numpy or a
+        torch tensor (returned in the same kind); non-finite entries count as
+        0; rows that did not converge give 0 (the reference's
+        ``solve_JT_batch_dlpack``)."""
+        if not self._ran:
+            raise RuntimeError("Call compute() first.")
+        import torch
+        n = self._s.n_rows()
+        is_torch = isinstance(rhs, torch.Tensor)
+        dev = torch.device("cuda", self._device_index())
+        r = rhs if is_torch else torch.as_tensor(np.asarray(rhs))
+        r = r.to(device=dev, dtype=torch.float64).contiguous()
+        if r.shape != (n, self.dim_J):
+            raise ValueError(f"rhs must be ({n}, {self.dim_J}), got {tuple(r.shape)}")
+        lam = torch.empty_like(r)
+        torch.cuda.current_stream(dev).synchronize()
+        self._s.solve_jt(n, r.data_ptr(), lam.data_ptr())
+        return lam if is_torch else lam.cpu().numpy()
+
+    def _device_index(self):
+        import torch
+        return int(torch.from_dlpack(self._s.dlpack("status")).device.index)
+
     def results_view(self):
         """(V, residuals, status, iterations) of the last ``compute()`` as
         numpy views of page-locked host memory the session owns, filled by

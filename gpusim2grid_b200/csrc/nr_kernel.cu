@@ -1399,6 +1399,7 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
 }
 
 #include "chord_sweep.cuh"
+#include "adjoint.cuh"
 
 template <typename T>
 int smem_bytes() {
@@ -1523,6 +1524,16 @@ int launch_chord_multi(const GridEntry* d_grids, int n_grids, int smem, unsigned
 }
 
 int chord_smem(const DevPlan& P, int prec) { return prec == 1 ? chord_smem_bytes<float>(P) : chord_smem_bytes<double>(P); }
+
+int launch_adjoint(const DevPlan& P, const SweepArgs& a, const double* rhs, double* lam, int n_ctas, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_ctas <= 0 || a.v_out == nullptr || a.status_out == nullptr || a.queue == nullptr) return (int)cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(adjoint_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes<double>());
+  if (e != cudaSuccess) return (int)e;
+  adjoint_kernel<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(P, a, rhs, lam);
+  return (int)cudaGetLastError();
+}
 
 int handoff_cluster_size() { return HANDOFF_CLUSTER; }
 

@@ -47,6 +47,14 @@ struct DevPlan {
   const int* bw_ptr;  // [p + 1]
   const int* bw_row;
   const int* bw_pos;
+  // transposed solves (see plan.hpp) and the J-index -> factor position map
+  const int* ut_ptr;
+  const int* ut_row;
+  const int* ut_pos;
+  const int* lt_ptr;
+  const int* lt_row;
+  const int* lt_pos;
+  const int* iperm;
 };
 
 // One launch = one sweep over a list of rows.
@@ -189,6 +197,14 @@ int sweep_ctas(int prec, int device);
 // leader's block index times ws_stride), and all of them share each of its
 // dense tail LUs.  n_ctas a multiple of the cluster size.
 int handoff_cluster_size();
+
+// Batched adjoint (FP64): lam[r] = J_r^-T rhs[r] for the a.n_rows rows of a
+// sweep (a.v_out the converged voltages, a.status_out their statuses, the
+// rows' edits and masks as in the sweep), J_r at the row's converged V; rows
+// that did not converge get 0.  rhs / lam [n_rows x dim] in the reference's
+// J layout.  Workspace a.workspace / a.ws_stride (double layout), queue
+// zeroed by the caller.
+int launch_adjoint(const DevPlan& P, const SweepArgs& a, const double* rhs, double* lam, int n_ctas, void* stream);
 int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int n_ctas, void* stream);
 
 // Several grids in one persistent launch (see sweep_kernel_multi): the plan

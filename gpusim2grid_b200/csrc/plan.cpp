@@ -570,6 +570,35 @@ Plan build_plan(int n_bus, const int* ybus_indptr, const int* ybus_indices,
     }
   P.diag_pos.resize(p);
   std::iota(P.diag_pos.begin(), P.diag_pos.end(), 0);
+  // the same entries by column, for the transposed solves
+  {
+    P.ut_ptr.assign(d + 1, 0);
+    for (int k = 0; k < p; ++k)
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) ++P.ut_ptr[P.bw_row[q] + 1];
+    for (int j = 0; j < d; ++j) P.ut_ptr[j + 1] += P.ut_ptr[j];
+    P.ut_row.resize(P.ut_ptr[d]);
+    P.ut_pos.resize(P.ut_ptr[d]);
+    std::vector<int> fill(P.ut_ptr.begin(), P.ut_ptr.end() - 1);
+    for (int k = 0; k < p; ++k)
+      for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) {
+        const int j = P.bw_row[q];
+        P.ut_row[fill[j]] = k;
+        P.ut_pos[fill[j]++] = P.bw_pos[q];
+      }
+    P.lt_ptr.assign(p + 1, 0);
+    for (int r = 0; r < d; ++r)
+      for (int q = P.fw_ptr[r]; q < P.fw_ptr[r + 1]; ++q) ++P.lt_ptr[P.fw_col[q] + 1];
+    for (int i = 0; i < p; ++i) P.lt_ptr[i + 1] += P.lt_ptr[i];
+    P.lt_row.resize(P.lt_ptr[p]);
+    P.lt_pos.resize(P.lt_ptr[p]);
+    std::vector<int> fl(P.lt_ptr.begin(), P.lt_ptr.end() - 1);
+    for (int r = 0; r < d; ++r)
+      for (int q = P.fw_ptr[r]; q < P.fw_ptr[r + 1]; ++q) {
+        const int i = P.fw_col[q];
+        P.lt_row[fl[i]] = r;
+        P.lt_pos[fl[i]++] = P.fw_pos[q];
+      }
+  }
 
   // ---- Jacobian fill map -------------------------------------------------
   auto dest = [&](int r, int c) -> int {

@@ -97,6 +97,12 @@ struct Plan {
   // backward: per head pivot k, (i, HV pos of u_ki) over i in struct(k)
   std::vector<int> bw_ptr, bw_row, bw_pos;
   std::vector<int> diag_pos;  // HV position of u_kk, k < p (== k)
+  // transposed solves (the adjoint J^T x = b; the factor pattern is
+  // structurally symmetric, so they follow the same level schedule):
+  // per column j, (k, HV pos of u_kj) over head rows k < j;
+  std::vector<int> ut_ptr, ut_row, ut_pos;  // [dim + 1]
+  // per head column i, (r, HV pos of l_ri) over rows r > i (head or tail)
+  std::vector<int> lt_ptr, lt_row, lt_pos;  // [p + 1]
 
   // ---- Jacobian fill map --------------------------------------------------
   // per Ybus entry k: destinations of its J11 (P-θ), J12 (P-Vm), J21 (Q-θ),

@@ -202,6 +202,13 @@ void upload_plan(gs2g_session* s) {
   D.bw_ptr = upload_vec(s, P.bw_ptr);
   D.bw_row = upload_vec(s, P.bw_row);
   D.bw_pos = upload_vec(s, P.bw_pos);
+  D.ut_ptr = upload_vec(s, P.ut_ptr);
+  D.ut_row = upload_vec(s, P.ut_row);
+  D.ut_pos = upload_vec(s, P.ut_pos);
+  D.lt_ptr = upload_vec(s, P.lt_ptr);
+  D.lt_row = upload_vec(s, P.lt_row);
+  D.lt_pos = upload_vec(s, P.lt_pos);
+  D.iperm = upload_vec(s, P.iperm);
 }
 
 // Ybus entry index of (i, j), -1 if not in the pattern.
@@ -1560,6 +1567,32 @@ void d2h_staged(const gs2g_session* s, void* dst, const void* src, size_t bytes)
   }
 }
 }  // namespace
+
+int gs2g_solve_jt(gs2g_session* s, int n_rows, const double* rhs, double* lam) {
+  GS2G_TRY
+  if (!s || n_rows < 0 || (n_rows > 0 && (!rhs || !lam))) throw std::invalid_argument("solve_jt: bad arguments");
+  if (n_rows != s->last_rows_run)
+    throw std::invalid_argument("solve_jt: n_rows (" + std::to_string(n_rows) + ") must be the rows of the last run (" +
+                                std::to_string(s->last_rows_run) + ")");
+  if (n_rows == 0) return GS2G_OK;
+  DeviceGuard g(s->device);
+  assemble_rows(s);
+  gs2g_run_opts o{};
+  o.precision = GS2G_PREC_FP64;
+  OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>()};
+  gs2g::SweepArgs a = make_args(s, o, n_rows, s->d_vinit.as<double>(), 0, s->d_sbus.as<double>(), 0, true, ob);
+  const int64_t wsb = gs2g::workspace_bytes(s->dplan, GS2G_PREC_FP64);
+  const int n_ctas = std::max(1, std::min(gs2g::sweep_ctas(GS2G_PREC_FP64, s->device), n_rows));
+  s->d_ws.ensure((size_t)wsb * n_ctas);
+  s->d_queue.ensure(4 * sizeof(int));
+  a.queue = s->d_queue.as<int>();
+  a.workspace = s->d_ws.as<char>();
+  a.ws_stride = wsb;
+  ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
+  ck((cudaError_t)gs2g::launch_adjoint(s->dplan, a, rhs, lam, n_ctas, s->stream), "adjoint launch");
+  ck(cudaStreamSynchronize(s->stream), "adjoint");
+  GS2G_CATCH
+}
 
 int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int** status, int** iters) {
   GS2G_TRY

@@ -277,6 +277,18 @@ int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violat
  * V_results device buffer (src/gpusim2grid/contingency_analysis/gpu_facade.py:1203)
  * and of its DLPack exports.  No counterpart for the pinned copy itself. */
 int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int** status, int** iters);
+/* Batched adjoint of the last run: for every row r of it, lam[r] = J_r^-T
+ * rhs[r], J_r the row's Jacobian (FP64) at its converged voltage, with its
+ * branch trips and masked buses; the sensitivity of the converged state to
+ * the row's injections (dx/ds = J^-1, so dL/ds = J^-T dL/dx).  rhs and lam
+ * are device arrays [n_rows x dim_J] in the reference's J layout (P/theta
+ * rows on sorted pv+pq, then Q/Vm rows on pq); non-finite rhs entries count
+ * as 0; rows that did not converge, and a masked bus's entries, get 0.
+ * n_rows must equal the last run's rows.  Replaces the reference's
+ * solve_JT_batch (src/_cpp/contingency/batch_pf_driver.cuh:180-224,
+ * src/gpusim2grid/differentiable/_batch_pf.py backward); each row's J is
+ * refactored here instead of keeping the forward factors. */
+int gs2g_solve_jt(gs2g_session* s, int n_rows, const double* rhs, double* lam);
 /* Device pointers of the last run's results (valid until the next run or destroy). */
 int gs2g_get_device_results(const gs2g_session* s, double** v, double** residuals, int** status, int** iters);
 /* Device copies of the current row definitions (uploaded first if they
