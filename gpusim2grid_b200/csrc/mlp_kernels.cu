@@ -338,6 +338,74 @@ __global__ void start_voltages_kernel(const float* y, int ldy, const float* ymea
   }
 }
 
+// Standardised bf16 network inputs of the rows, in one pass (one CTA per
+// row of the padded input block X [rows_pad x ldx]):
+//   column c < n_pvpq:            Re(S_r - S_base) at bus pvpq[c]
+//   column n_pvpq + c', c' < n_pq: Im(S_r - S_base) at bus pq[c']
+//   (0 without injection rows)
+//   plus, for every branch the row trips, the four contributions
+//   br_val[4 b + k] at column br_col[4 b + k] (columns >= n_in dropped)
+// then (x - mean) / std for c < n_in, 0 in the padding.  At most
+// FEAT_MAX_TERMS trip contributions per row are held; more are read back
+// from global memory per column.
+constexpr int FEAT_MAX_TERMS = 256;
+__global__ void features_kernel(const double2* __restrict__ sbus_rows, const double2* __restrict__ sbus_base,
+                                const int* __restrict__ pvpq, int n_pvpq, const int* __restrict__ pq, int n_pq,
+                                const int* __restrict__ trip_ptr, const int* __restrict__ trip_ids,
+                                const int* __restrict__ br_col, const float* __restrict__ br_val,
+                                const float* __restrict__ x_mean, const float* __restrict__ x_std, int n_in,
+                                __nv_bfloat16* __restrict__ X, int ldx, int rows, int n_bus) {
+  __shared__ int s_c[FEAT_MAX_TERMS];
+  __shared__ float s_v[FEAT_MAX_TERMS];
+  __shared__ int s_n;
+  const int r = blockIdx.x;
+  __nv_bfloat16* xr = X + (int64_t)r * ldx;
+  if (r >= rows) {
+    for (int c = threadIdx.x; c < ldx; c += blockDim.x) xr[c] = __float2bfloat16(0.f);
+    return;
+  }
+  const int q0 = trip_ptr != nullptr ? trip_ptr[r] : 0, q1 = trip_ptr != nullptr ? trip_ptr[r + 1] : 0;
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int q = q0; q < q1 && n + 4 <= FEAT_MAX_TERMS; ++q) {
+      const int b = trip_ids[q];
+      for (int k = 0; k < 4; ++k) {
+        const int c = br_col[4 * b + k];
+        if (c >= 0 && c < n_in) {
+          s_c[n] = c;
+          s_v[n] = br_val[4 * b + k];
+          ++n;
+        }
+      }
+    }
+    s_n = n;
+  }
+  __syncthreads();
+  const int n_terms = s_n;
+  const bool overflow = (q1 - q0) * 4 > FEAT_MAX_TERMS;
+  const double2* sr = sbus_rows != nullptr ? sbus_rows + (int64_t)r * n_bus : nullptr;
+  const int dim = n_pvpq + n_pq;
+  for (int c = threadIdx.x; c < ldx; c += blockDim.x) {
+    float v = 0.f;
+    if (c < n_in) {
+      if (sr != nullptr && c < dim) {
+        const int b = c < n_pvpq ? pvpq[c] : pq[c - n_pvpq];
+        v = c < n_pvpq ? (float)(sr[b].x - sbus_base[b].x) : (float)(sr[b].y - sbus_base[b].y);
+      }
+      if (!overflow) {
+        for (int e = 0; e < n_terms; ++e)
+          if (s_c[e] == c) v += s_v[e];
+      } else {
+        for (int q = q0; q < q1; ++q)
+          for (int k = 0; k < 4; ++k)
+            if (br_col[4 * trip_ids[q] + k] == c) v += br_val[4 * trip_ids[q] + k];
+      }
+      v = (v - x_mean[c]) / x_std[c];
+    }
+    xr[c] = __float2bfloat16(v);
+  }
+}
+
 inline int grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   if (b > 148 * 32) b = 148 * 32;
@@ -446,6 +514,20 @@ int gs2g_mlp_adam(float* w, const float* g, float* m, float* v, void* w_bf16, in
   }
   adam_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, (__nv_bfloat16*)w_bf16, n, lr, beta1,
                                                                   beta2, eps, 1.f - c1, 1.f - c2, weight_decay);
+  return status_of(cudaGetLastError());
+}
+
+int gs2g_mlp_features(const double* sbus_rows, const double* sbus_base, const int* pvpq, int n_pvpq, const int* pq,
+                      int n_pq, const int* trip_ptr, const int* trip_ids, const int* br_col, const float* br_val,
+                      const float* x_mean, const float* x_std, int n_in, void* x_bf16, int ldx, int rows,
+                      int rows_pad, int n_bus, void* stream) {
+  if (rows < 0 || rows_pad < rows || n_in < 0 || ldx < n_in || n_bus <= 0 || n_pvpq < 0 || n_pq < 0 || !x_bf16 ||
+      !x_mean || !x_std || !sbus_base || (trip_ptr && (!trip_ids || !br_col || !br_val)))
+    return invalid("features: bad arguments");
+  if (rows_pad == 0) return 0;
+  gs2g::mlp::features_kernel<<<rows_pad, 256, 0, (cudaStream_t)stream>>>(
+      (const double2*)sbus_rows, (const double2*)sbus_base, pvpq, n_pvpq, pq, n_pq, trip_ptr, trip_ids, br_col,
+      br_val, x_mean, x_std, n_in, (__nv_bfloat16*)x_bf16, ldx, rows, n_bus);
   return status_of(cudaGetLastError());
 }
 

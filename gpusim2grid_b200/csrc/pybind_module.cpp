@@ -543,6 +543,15 @@ void bind_mlp(py::module_& m) {
     check(gs2g_mlp_adam(P<float>(w), P<float>(g), P<float>(mo), P<float>(v), P<void>(wb), n, lr, b1, b2, eps, step,
                         wd, S(stream)));
   });
+  mm.def("features", [](uintptr_t sbus_rows, uintptr_t sbus_base, uintptr_t pvpq, int n_pvpq, uintptr_t pq, int n_pq,
+                        uintptr_t trip_ptr, uintptr_t trip_ids, uintptr_t br_col, uintptr_t br_val, uintptr_t x_mean,
+                        uintptr_t x_std, int n_in, uintptr_t x, int ldx, int rows, int rows_pad, int n_bus,
+                        uintptr_t stream) {
+    check(gs2g_mlp_features(P<const double>(sbus_rows), P<const double>(sbus_base), P<const int>(pvpq), n_pvpq,
+                            P<const int>(pq), n_pq, P<const int>(trip_ptr), P<const int>(trip_ids), P<const int>(br_col),
+                            P<const float>(br_val), P<const float>(x_mean), P<const float>(x_std), n_in, P<void>(x),
+                            ldx, rows, rows_pad, n_bus, S(stream)));
+  });
   mm.def("start_voltages", [](uintptr_t y, int ldy, uintptr_t ymean, uintptr_t ystd, uintptr_t ia, uintptr_t im,
                               uintptr_t vinit, int n_bus, uintptr_t v0, int rows, uintptr_t stream) {
     check(gs2g_mlp_start_voltages(P<float>(y), ldy, P<float>(ymean), P<float>(ystd), P<int>(ia), P<int>(im),

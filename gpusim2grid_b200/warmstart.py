@@ -281,8 +281,12 @@ class WarmStartMLP:
 
     # ----------------------------------------------------------- inference
     def predict(self, X, chunk=16384):
-        """Standardised outputs (rows, o) fp32 for standardised bf16 inputs."""
+        """Standardised outputs (rows, o) fp32 for standardised bf16 inputs.
+        Up to ``chunk`` rows the result is the network's own output buffer,
+        reused by the next call of the same size."""
         R = X.shape[0]
+        if R <= chunk:
+            return self._forward(X, self._buffers(R, False))
         out = torch.empty(R, self.o, dtype=torch.float32, device=self.device)
         for r0 in range(0, R, chunk):
             Xc = X[r0:r0 + chunk]
@@ -414,6 +418,14 @@ class LearnedStart:
         vals = np.stack([Sft.real, Sft.imag, Stf.real, Stf.imag], axis=1)
         self._br_cols = torch.as_tensor(cols.astype(np.int64), device=dev)
         self._br_vals = torch.as_tensor(vals.astype(np.float32), device=dev)
+        # the same tables for the fused input kernel (int32; the scratch
+        # column n_in is dropped by the kernel)
+        self._pvpq32 = self._pvpq.to(torch.int32)
+        self._pq32 = self._pq.to(torch.int32)
+        self._br_cols32 = self._br_cols.to(torch.int32).contiguous()
+        self._br_vals32 = self._br_vals.contiguous()
+        self._trips_dev = (None, None)
+        self._xbuf = {}
         self.n_in = 2 * self.dim
         self.net = WarmStartMLP(self.n_in, self.dim, hidden=hidden, layers=layers, device=self.device.index,
                                 seed=seed)
@@ -493,14 +505,53 @@ class LearnedStart:
         return self.report
 
     # ----------------------------------------------------------- inference
+    def _device_trips(self, trips):
+        """(ptr, ids) int32 device tensors of a trip CSR given as device
+        tensors, arrays or a list of lists (the last conversion is kept)."""
+        if trips is None:
+            return None, None
+        key = trips if isinstance(trips, tuple) else None
+        if key is not None and self._trips_dev[0] is key:
+            return self._trips_dev[1]
+        ptr, ids = trips if isinstance(trips, tuple) else _csr(trips)
+        cv = lambda a: torch.as_tensor(a if isinstance(a, torch.Tensor) else np.asarray(a),
+                                       device=self.device).to(torch.int32).contiguous()
+        out = (cv(ptr), cv(ids) if len(ids) else torch.zeros(1, dtype=torch.int32, device=self.device))
+        self._trips_dev = (key, out)
+        return out
+
+    def inputs(self, sbus_rows=None, trips=None, n_rows=None):
+        """Standardised bf16 network inputs (rows padded to 128, k0) in one
+        fused kernel (gs2g_mlp_features): the same values as
+        ``net.device_inputs(features(...))``, without the intermediate
+        tensors.  The returned block is reused by the next call."""
+        if n_rows is None:
+            n_rows = sbus_rows.shape[0] if sbus_rows is not None else (
+                len(trips[0]) - 1 if isinstance(trips, tuple) else len(trips))
+        net = self.net
+        rp = _ceil(max(n_rows, 1), 128)
+        X = self._xbuf.get(rp)
+        if X is None:
+            X = self._xbuf[rp] = torch.empty(rp, net.k0, dtype=torch.bfloat16, device=self.device)
+        sb = None
+        if sbus_rows is not None:
+            sb = torch.as_tensor(sbus_rows, device=self.device)
+            if sb.dtype != torch.complex128 or not sb.is_contiguous():
+                sb = sb.to(torch.complex128).contiguous()
+        tp, ti = self._device_trips(trips)
+        _M.features(0 if sb is None else sb.data_ptr(), self._sbase.data_ptr(), self._pvpq32.data_ptr(), self.n_pvpq,
+                    self._pq32.data_ptr(), self.n_pq, 0 if tp is None else tp.data_ptr(),
+                    0 if ti is None else ti.data_ptr(), self._br_cols32.data_ptr(), self._br_vals32.data_ptr(),
+                    net.x_mean.data_ptr(), net.x_std.data_ptr(), net.n_in, X.data_ptr(), net.k0, n_rows, rp,
+                    self._d["n_bus"], _stream())
+        return X, n_rows
+
     def start_voltages(self, sbus_rows=None, trips=None, n_rows=None, out_ptr=None):
         """Predicted V0 (rows, n_bus) complex128 on the device, enqueued on
         torch's current stream.  With ``out_ptr`` (a device address of rows x
         n_bus complex128, e.g. a session's ``start_rows_buffer``) V0 is
         written there and None is returned."""
-        F = self.features(sbus_rows, trips, n_rows)
-        R = F.shape[0]
-        X = self.net.device_inputs(F)
+        X, R = self.inputs(sbus_rows, trips, n_rows)
         y = self.net.predict(X)
         V0 = None
         if out_ptr is None:
@@ -512,6 +563,8 @@ class LearnedStart:
         return V0
 
     def launches_per_call(self, n_rows):
-        """Kernels of this library one ``start_voltages`` call launches."""
+        """Kernels of this library one ``start_voltages`` call launches: the
+        fused inputs, a GEMM and a bias/activation per layer and chunk, the
+        start voltages."""
         chunks = max(1, -(-_ceil(max(n_rows, 1), 128) // 16384))
-        return 2 * (self.net.layers + 1) * chunks + 1
+        return 2 * (self.net.layers + 1) * chunks + 2

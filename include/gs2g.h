@@ -374,6 +374,18 @@ int gs2g_mlp_to_bf16(const float* in, void* out, int64_t n, void* stream);
  * copy when w_bf16 is not NULL. */
 int gs2g_mlp_adam(float* w, const float* g, float* m, float* v, void* w_bf16, int64_t n, float lr, float beta1,
                   float beta2, float eps, int step, float weight_decay, void* stream);
+/* The network's standardised bf16 input block X [rows_pad x ldx] of `rows`
+ * rows in one pass: columns [0, n_pvpq) the rows' active injections minus
+ * the base case at buses pvpq, [n_pvpq, n_pvpq + n_pq) the reactive ones at
+ * buses pq (0 when sbus_rows is NULL; complex rows of n_bus per unit),
+ * plus, for every tripped branch b of a row (CSR trip_ptr / trip_ids, NULL:
+ * none), the four values br_val[4b + k] at columns br_col[4b + k] (a column
+ * < 0 or >= n_in is dropped); then (x - x_mean) / x_std for the n_in input
+ * columns and 0 in the padding columns and rows. */
+int gs2g_mlp_features(const double* sbus_rows, const double* sbus_base, const int* pvpq, int n_pvpq, const int* pq,
+                      int n_pq, const int* trip_ptr, const int* trip_ids, const int* br_col, const float* br_val,
+                      const float* x_mean, const float* x_std, int n_in, void* x_bf16, int ldx, int rows,
+                      int rows_pad, int n_bus, void* stream);
 /* Start voltages from the network's standardised outputs y[rows x ldy]:
  * bus b takes Va = y[va_index[b]] * y_std + y_mean when va_index[b] >= 0
  * (pv and pq buses), else the angle of vinit[b]; Vm likewise through

@@ -133,3 +133,28 @@ def test_fit_matches_a_torch_fp32_reference_fit():
     with torch.no_grad():
         theirs = float(((ref(Xc) - Tc) ** 2).mean())
     assert abs(ours - theirs) < 0.2 * theirs + 0.01, (ours, theirs)
+
+
+def test_fused_inputs_equal_the_torch_path(g118):
+    """gs2g_mlp_features (one kernel: injections, outage contributions,
+    standardisation, bf16, padding) against the same inputs built from
+    torch ops (features() then device_inputs()), for injection rows with
+    one or two trips each and for trip-only rows."""
+    import torch
+    from gpusim2grid_b200.synthetic import injection_scenarios, n1_branches
+    from gpusim2grid_b200.warmstart import LearnedStart
+    ls = LearnedStart(g118, hidden=128, layers=1, seed=0)
+    rng = np.random.default_rng(4)
+    ls.net.set_stats(rng.standard_normal(ls.n_in), rng.uniform(0.5, 2.0, ls.n_in), np.zeros(ls.dim), np.ones(ls.dim))
+    p, q = injection_scenarios(g118, 37, seed=3)
+    sb = torch.as_tensor((p + 1j * q) / g118.sn_mva, device="cuda")
+    cand = n1_branches(g118)
+    trips = [[int(cand[r % cand.size])] + ([int(cand[(3 * r) % cand.size])] if r % 3 == 0 else []) for r in range(37)]
+    for s_rows, t_rows in ((sb, trips), (None, trips), (sb, None)):
+        ref = ls.net.device_inputs(ls.features(s_rows, t_rows, 37))
+        X, n = ls.inputs(s_rows, t_rows, 37)
+        assert n == 37 and X.shape == ref.shape
+        a, b = X.float(), ref.float()
+        # equal up to the fp32 summation order of two trips at one bus (one bf16 step at most)
+        assert torch.all((a - b).abs() <= 2 ** -7 * b.abs().clamp(min=1e-3))
+        assert torch.all(X[37:] == 0) and torch.all(X[:, ls.n_in:] == 0)
