@@ -28,7 +28,15 @@ namespace mlp {
 
 constexpr int GT = 128;     // tile M = tile N
 constexpr int GK = 64;      // K per stage
-constexpr int STAGES = 3;
+// operand ring depth: a stage is reloaded once the MMAs of the k-tile before
+// it have completed (STAGES - 2 k-tiles of operands in flight).  6 stages
+// (one CTA per SM) measured no faster than 3 (two CTAs per SM fit): with
+// 128 x 128 tiles the operands are re-read from L2 at about 3.7 TB/s, which
+// bounds the kernel before the ring depth does
+#ifndef GS2G_GEMM_STAGES
+#define GS2G_GEMM_STAGES 3
+#endif
+constexpr int STAGES = GS2G_GEMM_STAGES;
 constexpr int GEMM_THREADS = 128;
 constexpr int TILE_BYTES = GT * GK * 2;  // one operand tile per stage (16 KB)
 constexpr int GEMM_SMEM = STAGES * 2 * TILE_BYTES + 1024;
