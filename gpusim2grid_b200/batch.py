@@ -141,6 +141,22 @@ class _BatchSweep:
         self._s.set_handle_disconnected(self._handle_disconnected)
 
     @property
+    def results_to_host(self):
+        """True: every later ``compute()`` also writes each row's final
+        voltages into the page-locked buffer that ``results_view()`` returns,
+        from the kernels as the row leaves, so the transfer of V to the host
+        overlaps the sweep and ``results_view()`` copies only the residuals,
+        statuses and iterations.  The device results are unchanged.  Default
+        False (no counterpart in the reference, whose results stay on the
+        device)."""
+        return getattr(self, "_results_to_host", False)
+
+    @results_to_host.setter
+    def results_to_host(self, value):
+        self._results_to_host = bool(value)
+        self._s.set_results_mirror(self._results_to_host)
+
+    @property
     def start(self):
         """'base' (the converged base case, default), 'flat' (``Vinit``),
         'rows' (``set_start_voltages``) or 'learned' (``set_learned_start``)."""
@@ -426,7 +442,8 @@ class _BatchSweep:
     def results_view(self):
         """(V, residuals, status, iterations) of the last ``compute()`` as
         numpy views of page-locked host memory the session owns, filled by
-        one DMA per array: no further host copy.  Valid until the next
+        one DMA per array (V already written by the kernels under
+        ``results_to_host``): no further host copy.  Valid until the next
         ``compute()`` or ``results_view()`` -- the lifetime of the reference's
         ``V_results`` device buffer; copy what must outlive it."""
         if not self._ran:

@@ -388,6 +388,10 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
     __syncthreads();
     return;
   }
+  if (a.v_mirror != nullptr) {
+    double2* vm = reinterpret_cast<double2*>(a.v_mirror) + (int64_t)row * n;
+    for (int i = tid; i < n; i += BS) vm[i] = V[i];
+  }
   const int status = sl.act == 2 ? ROW_CONVERGED : (sl.act == 3 ? ROW_DIVERGED : ROW_MAX_ITER);
   if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
   if (tid == 0) {

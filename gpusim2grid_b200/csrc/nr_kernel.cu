@@ -812,6 +812,10 @@ __device__ __noinline__ void skip_row_outputs(const SweepArgs a, const int row, 
   const int tid = threadIdx.x;
   double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
   for (int i = tid; i < n; i += BS) vout[i] = make_double2(NAN, NAN);
+  if (a.v_mirror != nullptr) {
+    double2* vm = reinterpret_cast<double2*>(a.v_mirror) + (int64_t)row * n;
+    for (int i = tid; i < n; i += BS) vm[i] = make_double2(NAN, NAN);
+  }
   if (a.loading_out != nullptr) {
     for (int l = tid; l < a.n_branch; l += BS) a.loading_out[(int64_t)row * a.n_branch + l] = NAN;
     if (tid == 0) {
@@ -1199,6 +1203,10 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
     if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
 
     for (int i = tid; i < n; i += BS) vout[i] = V[i];
+    if (a.v_mirror != nullptr) {
+      double2* vm = reinterpret_cast<double2*>(a.v_mirror) + (int64_t)row * n;
+      for (int i = tid; i < n; i += BS) vm[i] = V[i];
+    }
     if (tid == 0) {
       a.res_out[row] = nrm;
       a.status_out[row] = status;

@@ -142,6 +142,7 @@ struct SweepArgs {
   float* maxload_out;     // [n_rows]
   // outputs
   double* v_out;          // [n_rows * n_bus] complex
+  double* v_mirror;       // nullptr, or a host-mapped copy of v_out that gets each row's final V as it leaves
   double* res_out;        // [n_rows]
   int* status_out;        // [n_rows]
   int* iters_out;         // [n_rows]

@@ -143,6 +143,10 @@ struct gs2g_session {
   // pinned host copy of the last run's results (gs2g_get_results_host)
   void* h_res = nullptr;
   size_t h_res_bytes = 0;
+  // results mirror (gs2g_session_set_results_mirror): runs write each row's
+  // final V into h_res as the row leaves; mirror_valid once a full run did
+  bool mirror_on = false;
+  bool mirror_valid = false;
   mutable cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
 
@@ -444,6 +448,7 @@ struct OutBufs {
   int* status;
   int* iters;
   int* factors = nullptr;
+  double* v_mirror = nullptr;  // device address of a pinned host copy of v (nullptr: none)
 };
 
 // Launch arguments of one grid's rows (everything but the queue, the
@@ -474,6 +479,7 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.round_k = o.iters_per_round > 0 ? o.iters_per_round : 1;
   a.step_first = o.step_then_check != 0 && !o.fixed_iters;
   a.v_out = out.v;
+  a.v_mirror = out.v_mirror;
   a.res_out = out.res;
   a.status_out = out.status;
   a.iters_out = out.iters;
@@ -753,6 +759,15 @@ int gs2g_session_set_handle_disconnected(gs2g_session* s, int on) {
   if (on != 0 && on != 1) throw std::invalid_argument("session_set_handle_disconnected: on must be 0 or 1");
   if (s->handle_disconnected != on) s->rows_dirty = true;
   s->handle_disconnected = on;
+  GS2G_CATCH
+}
+
+int gs2g_session_set_results_mirror(gs2g_session* s, int on) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_set_results_mirror: NULL session");
+  if (on != 0 && on != 1) throw std::invalid_argument("session_set_results_mirror: on must be 0 or 1");
+  s->mirror_on = on != 0;
+  if (!s->mirror_on) s->mirror_valid = false;
   GS2G_CATCH
 }
 
@@ -1303,6 +1318,21 @@ void ensure_base_factor(gs2g_session* s, int prec) {
   s->tm.base_setup_bytes = (int64_t)(s->d_base_ws.n + s->d_base_inv.n + s->d_base_fwv.n + s->d_base_bwv.n);
 }
 
+// The pinned result buffer for `nr` rows: V [nr x n] complex, then the
+// residuals, statuses and iterations.  Grows only (a grown buffer loses its
+// contents, and with them a valid mirror).
+void ensure_host_results(gs2g_session* s, size_t nr) {
+  const size_t n = s->n_bus;
+  const size_t total = std::max<size_t>(nr * n * 2 * sizeof(double) + nr * (sizeof(double) + 2 * sizeof(int)), 16);
+  if (s->h_res_bytes >= total) return;
+  s->mirror_valid = false;
+  if (s->h_res) ck(cudaFreeHost(s->h_res), "free pinned results");
+  s->h_res = nullptr;
+  s->h_res_bytes = 0;
+  ck(cudaHostAlloc(&s->h_res, total, cudaHostAllocMapped), "pinned results");
+  s->h_res_bytes = total;
+}
+
 RunPrep prepare_rows(gs2g_session* s, const gs2g_run_opts& o) {
   if (o.refactor_policy == GS2G_REFACTOR_BASE_CHORD) ensure_base_factor(s, o.precision);
   const int nr = s->n_rows;
@@ -1330,6 +1360,12 @@ RunPrep prepare_rows(gs2g_session* s, const gs2g_run_opts& o) {
   s->d_factors.ensure((size_t)std::max(nr, 1) * sizeof(int));
   OutBufs ob{s->d_v_out.as<double>(), s->d_res.as<double>(), s->d_status.as<int>(), s->d_iters.as<int>(),
              s->d_factors.as<int>()};
+  if (s->mirror_on && nr > 0) {
+    ensure_host_results(s, nr);
+    void* d = nullptr;
+    ck(cudaHostGetDevicePointer(&d, s->h_res, 0), "results mirror address");
+    ob.v_mirror = static_cast<double*>(d);
+  }
   return RunPrep{nr, v0, v0s, sb, sbs, ob};
 }
 }  // namespace
@@ -1342,10 +1378,12 @@ int gs2g_run(gs2g_session* s, const gs2g_run_opts* o_) {
   auto t0 = std::chrono::steady_clock::now();
   assemble_rows(s);
   s->tm.upload_ms = ms_since(t0);
+  s->mirror_valid = false;
   const RunPrep rp = prepare_rows(s, o);
   const int nr = rp.nr;
   s->tm.kernel_ms = launch(s, o, nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob, o.n_ctas);
   s->last_rows_run = nr;
+  s->mirror_valid = rp.ob.v_mirror != nullptr;
   s->tm.total_ms = ms_since(t0);
   s->tm.total_iters = -1;
   GS2G_CATCH
@@ -1365,6 +1403,9 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
     if (rows[i] < 0 || rows[i] >= s->n_rows) throw std::invalid_argument("run_subset: row index out of range");
   s->tm.upload_ms = ms_since(t0);
   const RunPrep rp = prepare_rows(s, o);
+  // the subset's rows reach the mirror only when it is on (same rows, so
+  // the buffer is not regrown)
+  if (rp.ob.v_mirror == nullptr) s->mirror_valid = false;
   s->d_row_map.ensure(std::max(n_sub, 1) * sizeof(int));
   if (n_sub) ck(cudaMemcpy(s->d_row_map.p, rows, n_sub * sizeof(int), cudaMemcpyHostToDevice), "upload row map");
   gs2g::SweepArgs a = make_args(s, o, n_sub, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
@@ -1414,6 +1455,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   for (int i = 0; i < n_sessions; ++i) {
     gs2g_session* s = sessions[i];
     assemble_rows(s);
+    s->mirror_valid = false;
     const RunPrep rp = prepare_rows(s, o);
     ge[i].P = s->dplan;
     ge[i].a = make_args(s, o, rp.nr, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
@@ -1510,6 +1552,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
   for (int i = 0; i < n_sessions; ++i) {
     gs2g_session* s = sessions[i];
     s->last_rows_run = begin[i + 1] - begin[i];
+    s->mirror_valid = s->mirror_on && s->last_rows_run > 0;
     s->tm.kernel_ms = ms;
     s->tm.upload_ms = upload_ms;
     s->tm.total_ms = ms_since(t0);
@@ -1600,17 +1643,12 @@ int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int**
   DeviceGuard g(s->device);
   const size_t nr = s->last_rows_run, n = s->n_bus;
   const size_t bv = nr * n * 2 * sizeof(double), br = nr * sizeof(double), bi = nr * sizeof(int);
-  const size_t o_r = bv, o_s = o_r + br, o_i = o_s + bi, total = std::max<size_t>(o_i + bi, 16);
-  if (s->h_res_bytes < total) {
-    if (s->h_res) ck(cudaFreeHost(s->h_res), "free pinned results");
-    s->h_res = nullptr;
-    s->h_res_bytes = 0;
-    ck(cudaMallocHost(&s->h_res, total), "pinned results");
-    s->h_res_bytes = total;
-  }
+  const size_t o_r = bv, o_s = o_r + br, o_i = o_s + bi;
+  ensure_host_results(s, nr);
   char* h = static_cast<char*>(s->h_res);
   if (nr) {
-    ck(cudaMemcpyAsync(h, s->d_v_out.p, bv, cudaMemcpyDeviceToHost, s->stream), "read results");
+    // with a valid mirror the kernels already wrote V here
+    if (!s->mirror_valid) ck(cudaMemcpyAsync(h, s->d_v_out.p, bv, cudaMemcpyDeviceToHost, s->stream), "read results");
     ck(cudaMemcpyAsync(h + o_r, s->d_res.p, br, cudaMemcpyDeviceToHost, s->stream), "read residuals");
     ck(cudaMemcpyAsync(h + o_s, s->d_status.p, bi, cudaMemcpyDeviceToHost, s->stream), "read status");
     ck(cudaMemcpyAsync(h + o_i, s->d_iters.p, bi, cudaMemcpyDeviceToHost, s->stream), "read iters");

@@ -277,6 +277,15 @@ int gs2g_get_branch_loading(const gs2g_session* s, float* loading, int* n_violat
  * V_results device buffer (src/gpusim2grid/contingency_analysis/gpu_facade.py:1203)
  * and of its DLPack exports.  No counterpart for the pinned copy itself. */
 int gs2g_get_results_host(gs2g_session* s, double** v, double** residuals, int** status, int** iters);
+/* Results mirror: on = 1 makes every later run (gs2g_run, gs2g_run_subset,
+ * gs2g_run_multi) also write each row's final voltages straight into the
+ * page-locked buffer gs2g_get_results_host returns, from the kernels, as
+ * the row leaves -- the device-to-host transfer of V overlaps the sweep,
+ * and gs2g_get_results_host then copies only the residuals, statuses and
+ * iterations.  A run overwrites that buffer while it runs.  The device
+ * results (gs2g_get_results, the DLPack exports) are unchanged.  Default 0.
+ * No counterpart in the reference (its results stay on the device). */
+int gs2g_session_set_results_mirror(gs2g_session* s, int on);
 /* Batched adjoint of the last run: for every row r of it, lam[r] = J_r^-T
  * rhs[r], J_r the row's Jacobian (FP64) at its converged voltage, with its
  * branch trips and masked buses; the sensitivity of the converged state to

@@ -157,6 +157,33 @@ def test_results_view_equals_the_owned_copies(g118):
     assert V.shape == (20, g118.n_bus) and not V.flags.owndata
 
 
+@pytest.mark.parametrize("precision,strategy", [("fp64", "refactor_every"), ("mixed", "base_chord")])
+def test_results_to_host_mirror_equals_the_device_results(g118, precision, strategy):
+    """results_to_host: the kernels write each row's final V into the
+    page-locked buffer as it leaves; equal, NaNs included, to the device
+    results, for islanded rows (NaN), split rows (masked NaN buses) and
+    solved rows, over batches of changing size and after switching off."""
+    m = g118.n_branch
+    bridges = np.setdiff1d(np.arange(m), n1_branches(g118))
+    rows = [[int(b)] for b in n1_branches(g118)[:30]] + [[int(b)] for b in bridges[:4]]
+    ca = _ca(g118, precision=precision, strategy=strategy)
+    ca.results_to_host = True
+    for hd, rr in ((False, rows), (True, rows[:7] + rows[-3:]), (True, rows)):
+        ca.handle_disconnected_grid = hd
+        ca.add_contingencies_by_branch_id(rr)
+        ca.compute()
+        V, res, st, it = ca.results_view()
+        np.testing.assert_array_equal(V, ca.V_results)
+        np.testing.assert_array_equal(st, ca.get_row_status())
+        np.testing.assert_array_equal(res, ca.last_residuals())
+        np.testing.assert_array_equal(it, ca.get_row_iterations())
+        assert np.isnan(V[-1]).any()
+    ca.results_to_host = False
+    ca.add_contingencies_by_branch_id(rows[:5])
+    ca.compute()
+    np.testing.assert_array_equal(ca.results_view()[0], ca.V_results)
+
+
 @pytest.mark.parametrize("precision,strategy,tol_v", [("fp64", "refactor_every", 1e-9),
                                                       ("mixed", "base_chord", 1e-6)])
 def test_handle_disconnected_grid_vs_oracle(g118, precision, strategy, tol_v):

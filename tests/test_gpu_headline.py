@@ -47,9 +47,12 @@ def test_cfg1_benched_path_every_row_vs_oracle(g2000):
     ca.set_branch_data(*g2000.branch_data())
     ca.add_contingencies_by_branch_id(rows)
     ca.set_learned_start(ls)
+    ca.results_to_host = True
     ca.compute()
     Vo, so, _, _ = oracle_rows(g2000, trips=rows)
     _check(ca.V_results, ca.get_row_status(), ca.last_residuals(), Vo, so)
+    # the kernels' host copy of V (chord rows, hand-offs, fallback) equals the device results
+    np.testing.assert_array_equal(ca.results_view()[0], ca.V_results)
     assert int((so == RowStatus.NOT_SIMULATED).sum()) == len(bridges)
     # the path the bench measures: nearly every step on the shared base factor
     assert ca.session.timings()["chord_steps"] > 0.9 * ca.get_row_iterations().sum()
