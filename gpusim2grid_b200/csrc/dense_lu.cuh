@@ -114,9 +114,12 @@ __device__ __forceinline__ void stage_slab(T* sA, T* sB, const T* A, int lda, co
 // A_SMEM / B_SMEM: that operand already sits in shared memory (stride
 // lda / ldb) and is read in place; otherwise it streams from global memory.
 // ---------------------------------------------------------------------------
+// With parts > 1 the CTA computes the output tiles part, part + parts, ...
+// (the CTAs of a cluster split them); a tile's arithmetic does not depend on
+// which CTA computes it.
 template <int MODE, bool A_SMEM, bool B_SMEM>
 __device__ void gemm(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int M, int N, int K,
-                     double* stages) {
+                     double* stages, int part = 0, int parts = 1) {
   using CF = Cfg<double>;
   using SM = Smem<double>;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -124,10 +127,12 @@ __device__ void gemm(double* C, int ldc, const double* A, int lda, const double*
   const int g = lane >> 2, q = lane & 3;
   const int n_tj = (N + CF::TNt - 1) / CF::TNt;
   const int n_sl = (K + KC - 1) / KC;
-  const int n_items = ((M + CF::TMt - 1) / CF::TMt) * n_tj * n_sl;
+  const int n_tiles = ((M + CF::TMt - 1) / CF::TMt) * n_tj;
+  const int my_tiles = part < n_tiles ? (n_tiles - part + parts - 1) / parts : 0;
+  const int n_items = my_tiles * n_sl;
   if (n_items == 0) return;
   auto coords = [&](int item, int& i0, int& j0, int& kc) {
-    const int tile = item / n_sl;
+    const int tile = part + (item / n_sl) * parts;
     kc = (item % n_sl) * KC;
     i0 = (tile / n_tj) * CF::TMt;
     j0 = (tile % n_tj) * CF::TNt;
@@ -520,6 +525,65 @@ __device__ void lu(T* A, int n, int ld, T* smem, double pfloor) {
       gemm<0, false, false>(A22, ld, A21, ld, A12, ld, m, m, kb, stages);    // A22 -= L21 U12
     }
     __syncthreads();
+  }
+}
+
+// Barrier over every thread of every CTA of the cluster, ordering the
+// memory accesses before it (global and distributed shared) before those
+// after it.  Block-uniform calls only.
+__device__ __forceinline__ void cluster_barrier() {
+  __threadfence();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// The same FP64 LU as lu(), by the `parts` CTAs of a cluster together (this
+// CTA has rank `part`); A in global memory, every CTA with its own scratch.
+// Every CTA factors and inverts the 64 x 64 diagonal block itself (cheap,
+// and each needs it in its own shared memory); the tiles of L21, U12 and the
+// trailing update are split by rank, and three cluster barriers per panel
+// order the stages.  Each element goes through the same operations in the
+// same order as in lu(), so the factor is bit-identical.  Every CTA of the
+// cluster must call it with the same n.
+__device__ void lu_cluster(double* A, int n, int ld, double* smem, double pfloor, int part, int parts) {
+  using SM = Smem<double>;
+  double* D = smem;
+  double* Inv = D + SM::d_elems;
+  double* stages = Inv + SM::i_elems;
+  const int tid = threadIdx.x;
+  for (int k0 = 0; k0 < n; k0 += KP) {
+    const int kb = min(KP, n - k0);
+    double* Akk = A + (int64_t)k0 * ld + k0;
+    for (int idx = tid; idx < KP * KP; idx += BS) {
+      const int r = idx / KP, c = idx % KP;
+      D[r * SD + c] = (r < kb && c < kb) ? Akk[(int64_t)r * ld + c] : (r == c ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    diag_lu(D, pfloor);
+    cluster_barrier();  // every CTA holds the block: rank 0 may write it back below
+    const int m = n - k0 - kb;
+    if (m > 0) {
+      double* A21 = A + (int64_t)(k0 + kb) * ld + k0;
+      double* A12 = A + (int64_t)k0 * ld + k0 + kb;
+      diag_inverse<true>(D, Inv, SI_U);
+      gemm<1, false, true>(A21, ld, A21, ld, Inv, SI_U, m, kb, kb, stages, part, parts);  // L21 = A21 U11^-1
+      __syncthreads();
+      diag_inverse<false>(D, Inv, SI_L);
+      gemm<1, true, false>(A12, ld, Inv, SI_L, A12, ld, kb, m, kb, stages, part, parts);  // U12 = L11^-1 A12
+    }
+    if (part == 0)
+      for (int idx = tid; idx < kb * kb; idx += BS) {
+        const int r = idx / kb, c = idx % kb;
+        Akk[(int64_t)r * ld + c] = D[r * SD + c];
+      }
+    cluster_barrier();  // L21, U12 and the diagonal block complete
+    if (m > 0) {
+      double* A21 = A + (int64_t)(k0 + kb) * ld + k0;
+      double* A12 = A + (int64_t)k0 * ld + k0 + kb;
+      double* A22 = A + (int64_t)(k0 + kb) * ld + k0 + kb;
+      gemm<0, false, false>(A22, ld, A21, ld, A12, ld, m, m, kb, stages, part, parts);  // A22 -= L21 U12
+    }
+    cluster_barrier();  // A22 complete
   }
 }
 

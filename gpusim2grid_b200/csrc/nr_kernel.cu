@@ -114,9 +114,11 @@ __device__ __forceinline__ T schur_entry(const T* __restrict__ HV, int4 rec) {
 // once), four groups per lane in flight: their entry records are loaded
 // together, then their factor values.
 template <typename T>
-__device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__ HV, T* __restrict__ S) {
+__device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__ HV, T* __restrict__ S, int part = 0,
+                                          int parts = 1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int ti = warp; ti < P.nt; ti += NWARP) {
+  // with parts > 1 the CTAs of a cluster take every parts-th warp's rows
+  for (int ti = part * NWARP + warp; ti < P.nt; ti += parts * NWARP) {
     T* Srow = S + (int64_t)ti * P.ld;
     const int g0 = P.sg_ptr[ti], g1 = P.sg_ptr[ti + 1];
     for (int gb = g0; gb < g1; gb += 128) {
@@ -154,6 +156,15 @@ __device__ __forceinline__ void dense_lu(T* S, int n, int ld, T* smem, double pf
     gs2g::dense32::lu(S, n, ld, smem, pfloor);
   else
     dense::lu<T>(S, n, ld, smem, pfloor);
+}
+// The same factorization by the `parts` CTAs of a cluster (this CTA: rank
+// `part`), bit-identical to dense_lu.
+template <typename T>
+__device__ __forceinline__ void dense_lu_cluster(T* S, int n, int ld, T* smem, double pfloor, int part, int parts) {
+  if constexpr (sizeof(T) == 4)
+    gs2g::dense32::lu_cluster(S, n, ld, smem, pfloor, part, parts);
+  else
+    dense::lu_cluster(S, n, ld, smem, pfloor, part, parts);
 }
 template <typename T>
 __host__ __device__ constexpr int dense_smem_elems() {
@@ -1127,27 +1138,25 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       }
 
       prof.mark(PH_HEAD);
+      if (cl != nullptr && P.nt > 0) {
+        // the cluster's other CTAs join: post the command, two barriers
+        // (posted; read by all), then the Schur update split by tail rows
+        // (a barrier) and the shared dense factorization
+        if (tid == 0) *cl->cmd = CLUSTER_CMD_LU;
+        dense::cluster_barrier();
+        dense::cluster_barrier();
+        schur_update<T>(P, HV, S, 0, cl->parts);
+        dense::cluster_barrier();
+        prof.mark(PH_SCHUR);
+        dense_lu_cluster<T>(S, P.nt, P.ld, s_dense, a.pivot_floor, 0, cl->parts);
+      } else {
       // ---- Schur update of the dense tail ----------------------------------
       schur_update<T>(P, HV, S);
       __syncthreads();
 
       prof.mark(PH_SCHUR);
       // ---- dense tail LU --------------------------------------------------
-      if (P.nt > 0) {
-        if constexpr (sizeof(T) == 4) {
-          if (cl != nullptr) {
-            // the cluster's other CTAs join: post the command, two barriers
-            // (posted; read by all), then the shared factorization
-            if (tid == 0) *cl->cmd = CLUSTER_CMD_LU;
-            gs2g::dense32::cluster_sync_all();
-            gs2g::dense32::cluster_sync_all();
-            gs2g::dense32::lu_cluster(S, P.nt, P.ld, s_dense, a.pivot_floor, 0, cl->parts);
-          } else {
-            dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
-          }
-        } else {
-          dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
-        }
+      if (P.nt > 0) dense_lu<T>(S, P.nt, P.ld, s_dense, a.pivot_floor);
       }
       fHV = HV;
       fS = S;
@@ -1268,23 +1277,25 @@ __device__ __forceinline__ int ld_shared_rank0(const int* p) {
 }
 
 // The single-row sweep with a cluster of HANDOFF_CLUSTER CTAs per row (FP32
-// factors): the leading CTA (rank 0) runs the row's whole Newton loop in its
-// workspace as sweep_kernel does, and the other CTAs join each of its dense
-// tail LUs (dense32::lu_cluster), the one step whose work grows as the cube
-// of the tail.  For the few rows the chord sweep hands off, whose LUs would
-// otherwise each run on one SM after every other row has finished.  When
-// the rows outnumber the clusters, every CTA takes rows of its own instead.
+// or FP64 factors): the leading CTA (rank 0) runs the row's whole Newton
+// loop in its workspace as sweep_kernel does, and the other CTAs join each
+// of its factorizations from the Schur update of the dense tail on (split
+// by tail rows) through the dense tail LU (dense_lu_cluster), the steps
+// whose work grows fastest with the tail.  For the few rows the chord sweep
+// hands off and the few rows of an FP64 re-solve, whose factorizations
+// would otherwise each run on one SM after every other row has finished.
+// When the rows outnumber the clusters, every CTA takes rows of its own.
 // Protocol, all through cluster barriers (every CTA passes the same number):
 // per row, the leader takes a queue entry and publishes it (barrier), every
-// CTA reads it (barrier); then for each dense LU the leader posts
-// CLUSTER_CMD_LU (barrier, read, barrier) and all factor together; after the
-// row it posts CLUSTER_CMD_DONE (barrier, read, barrier).
+// CTA reads it (barrier); then for each factorization the leader posts
+// CLUSTER_CMD_LU (barrier, read, barrier), all update their Schur rows
+// (barrier) and factor together; after the row it posts CLUSTER_CMD_DONE
+// (barrier, read, barrier).
 constexpr int HANDOFF_CLUSTER = 8;
 
 template <typename T>
 __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
     sweep_kernel_cluster(const DevPlan P, const SweepArgs a) {
-  static_assert(sizeof(T) == 4, "the cluster LU is the FP32 one");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_row;
   __shared__ int s_cmd;
@@ -1323,26 +1334,31 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
   // the row lives in the leader's workspace
   char* ws = a.workspace + (int64_t)(blockIdx.x - rank) * a.ws_stride;
   T* S = reinterpret_cast<T*>(ws + ws_layout<T>(P).S);
+  const T* HV = reinterpret_cast<const T*>(ws + ws_layout<T>(P).HV);
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0 && rank == 0);
   const ClusterLu cl{&s_cmd, HANDOFF_CLUSTER};
   for (;;) {
     if (rank == 0 && threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
-    dense32::cluster_sync_all();
+    dense::cluster_barrier();
     const int q = ld_shared_rank0(&s_row);
-    dense32::cluster_sync_all();
+    dense::cluster_barrier();
     if (q >= n_rows) break;
     if (rank == 0) {
       solve_row<T>(P, a, a.row_map != nullptr ? a.row_map[q] : q, ws, sh, prof, &cl);
       if (threadIdx.x == 0) s_cmd = CLUSTER_CMD_DONE;
-      dense32::cluster_sync_all();
-      dense32::cluster_sync_all();
+      dense::cluster_barrier();
+      dense::cluster_barrier();
     } else {
       for (;;) {
-        dense32::cluster_sync_all();
+        dense::cluster_barrier();
         const int cmd = ld_shared_rank0(&s_cmd);
-        dense32::cluster_sync_all();
+        dense::cluster_barrier();
         if (cmd != CLUSTER_CMD_LU) break;
-        dense32::lu_cluster(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, HANDOFF_CLUSTER);
+        // the leader's head factor and scattered tail are complete (posted
+        // after them); its Schur rows, a barrier, then the shared LU
+        schur_update<T>(P, HV, S, rank, HANDOFF_CLUSTER);
+        dense::cluster_barrier();
+        dense_lu_cluster<T>(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, HANDOFF_CLUSTER);
       }
     }
   }
@@ -1438,6 +1454,9 @@ cudaError_t opt_in_smem() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(sweep_kernel_cluster<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem_bytes<float>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_kernel_cluster<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem_bytes<double>());
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_kernel_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               smem_bytes<double>());
@@ -1545,13 +1564,16 @@ int launch_adjoint(const DevPlan& P, const SweepArgs& a, const double* rhs, doub
 
 int handoff_cluster_size() { return HANDOFF_CLUSTER; }
 
-int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int n_ctas, void* stream) {
+int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n_ctas <= 0 || n_ctas % HANDOFF_CLUSTER != 0 || a.inverse_out != nullptr || a.factor_only)
     return (int)cudaErrorInvalidValue;
   const cudaError_t e = opt_in_smem();
   if (e != cudaSuccess) return (int)e;
-  sweep_kernel_cluster<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
+  if (prec == 1)
+    sweep_kernel_cluster<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
+  else
+    sweep_kernel_cluster<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(P, a);
   return (int)cudaGetLastError();
 }
 

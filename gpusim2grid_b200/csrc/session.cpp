@@ -131,7 +131,7 @@ struct gs2g_session {
   DevBuf d_handoff;        // rows the chord sweep hands to the single-row sweep
   DevBuf d_chord_steps;    // Newton steps the last chord sweep took on the base factor
   int chord = 2;           // policy 2: 0 single-row sweep, 1 chord sweep, 2 chord sweep with Broyden steps
-  int handoff_cluster = 1;  // mixed precision: the chord sweep's hand-offs run with a cluster of CTAs per row
+  int handoff_cluster = 1;  // the chord sweep's hand-offs and small subsets run with a cluster of CTAs per row
   int base_factor_prec = -1;  // precision it was computed in (-1: none or stale)
   // base-solve outputs (kept apart from the batch results)
   DevBuf b_v, b_res, b_status, b_iters;
@@ -587,15 +587,15 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.alt_v0 = nullptr;
     a.alt_s = nullptr;
   }
-  // hand-offs in mixed precision with a dense tail worth sharing: a cluster
-  // of CTAs per row (the rows are few and each of their LUs would otherwise
-  // run on one SM after every other row has finished)
+  // hand-offs with a dense tail worth sharing: a cluster of CTAs per row
+  // (the rows are few and each of their factorizations would otherwise run
+  // on one SM after every other row has finished)
   const int csize = gs2g::handoff_cluster_size();
-  const bool cluster = chord && s->handoff_cluster && o.precision == GS2G_PREC_MIXED && s->dplan.nt >= 64 &&
-                       n_ctas >= csize;
+  const bool cluster = chord && s->handoff_cluster && s->dplan.nt >= 64 && n_ctas >= csize;
   if (n_rows > 0 && cluster) {
     const int n_cl = std::max(1, std::min(n_ctas / csize, n_rows));
-    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, n_cl * csize, s->stream), "hand-off cluster launch");
+    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, n_cl * csize, s->stream),
+       "hand-off cluster launch");
   } else if (n_rows > 0) {
     ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
   }
@@ -1411,7 +1411,11 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   gs2g::SweepArgs a = make_args(s, o, n_sub, rp.v0, rp.v0s, rp.sb, rp.sbs, true, rp.ob);
   a.row_map = s->d_row_map.as<int>();
   int n_ctas = o.n_ctas > 0 ? o.n_ctas : gs2g::sweep_ctas(o.precision, s->device);
-  n_ctas = std::max(1, std::min(n_ctas, std::max(n_sub, 1)));
+  // few rows with a dense tail worth sharing (an FP64 re-solve of the rows
+  // a mixed sweep did not converge): a cluster of CTAs per row
+  const int csize = gs2g::handoff_cluster_size();
+  const bool cluster = s->handoff_cluster && s->dplan.nt >= 64 && n_sub > 0 && (int64_t)n_sub * csize <= n_ctas;
+  n_ctas = cluster ? n_sub * csize : std::max(1, std::min(n_ctas, std::max(n_sub, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
   s->d_ws.ensure((size_t)wsb * n_ctas);
   s->d_queue.ensure(3 * sizeof(int));
@@ -1421,7 +1425,10 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   a.n_rescued = s->d_queue.as<int>() + 1;
   ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
-  if (n_sub > 0) ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "subset launch");
+  if (n_sub > 0 && cluster)
+    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, n_ctas, s->stream), "subset cluster launch");
+  else if (n_sub > 0)
+    ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "subset launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");
   ck(cudaStreamSynchronize(s->stream), "subset sweep");
   float ms = 0;

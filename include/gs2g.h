@@ -176,12 +176,15 @@ int gs2g_session_replan(gs2g_session* s, int tail_policy, double dense_rate, int
  * convergence); mode 1: plain chord steps, the same decisions as the
  * single-row sweep; mode 0: every row in the single-row sweep. */
 int gs2g_session_set_chord(gs2g_session* s, int mode);
-/* Hand-offs of the chord sweep in mixed precision (rows that factor their
- * own Jacobian): cluster = 1 (default) runs each such row on a cluster of 8
- * CTAs, the leading CTA running the row and all 8 sharing each of its dense
- * tail LUs (bit-identical to the one-CTA factorization); 0 runs each on one
- * CTA.  Grids whose dense tail is under 64 always use one CTA.  No
- * counterpart in the reference (its batch LU has no per-row kernel). */
+/* Rows that factor their own Jacobian after a chord sweep (its hand-offs),
+ * and the rows of a gs2g_run_subset when there are few of them (at most one
+ * per 8 CTAs of a full launch: the FP64 re-solve of the rows a mixed sweep
+ * did not converge): cluster = 1 (default) runs each such row on a cluster
+ * of 8 CTAs, the leading CTA running the row and all 8 sharing each of its
+ * Schur updates and dense tail LUs (bit-identical to the one-CTA
+ * factorization, FP32 and FP64); 0 runs each on one CTA.  Grids whose
+ * dense tail is under 64 always use one CTA.  No counterpart in the
+ * reference (its batch LU has no per-row kernel). */
 int gs2g_session_set_handoff(gs2g_session* s, int cluster);
 /* handle_disconnected_grid (the reference's facade option,
  * src/gpusim2grid/contingency_analysis/gpu_facade.py:349, :544): on = 1

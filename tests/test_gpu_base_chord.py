@@ -70,21 +70,22 @@ def test_device_rows_match_host_definitions(g118):
     assert isinstance(sbus, torch.Tensor) and sbus.is_cuda
 
 
-@pytest.mark.parametrize("name,kind", [("case2000_synth", "n1"), ("case2000_synth", "heavy"),
-                                       ("case6500_synth", "heavy")])
-def test_cluster_handoffs_equal_one_cta_handoffs(name, kind):
+@pytest.mark.parametrize("name,kind,precision", [("case2000_synth", "n1", "mixed"), ("case2000_synth", "heavy", "mixed"),
+                                                 ("case6500_synth", "heavy", "mixed"), ("case2000_synth", "n1", "fp64"),
+                                                 ("case2000_synth", "heavy", "fp64")])
+def test_cluster_handoffs_equal_one_cta_handoffs(name, kind, precision):
     """The chord sweep's hand-offs (rows that factor their own Jacobian) run
-    on a cluster of CTAs per row in mixed precision when every such row can
-    have a cluster (the N-1 sweep: about a dozen rows), all CTAs of the
-    cluster sharing each dense tail LU; with more hand-offs than clusters
-    (heavily loaded scenarios) every CTA takes rows of its own.  The shared
-    factorization is bit-identical to the one-CTA one, so every output must
-    be too."""
+    on a cluster of CTAs per row when every such row can have a cluster (the
+    N-1 sweep: about a dozen rows), all CTAs of the cluster sharing each
+    Schur update and dense tail LU (FP32 or FP64); with more hand-offs than
+    clusters (heavily loaded scenarios) every CTA takes rows of its own.  The
+    shared factorization is bit-identical to the one-CTA one, so every output
+    must be too."""
     from gpusim2grid_b200.synthetic import grid_by_name, scenario_outages
     g = grid_by_name(name, 0)
     out = []
     for cluster in (0, 1):
-        kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", tol=1e-8,
+        kw = dict(init_from_n_powerflow=False, precision=precision, nb_iter=10, scheduling="continuous", tol=1e-8,
                   start="base", strategy="base_chord")
         if kind == "n1":
             sw = ContingencyAnalysisGPU(g.as_tuple(), **kw)
@@ -107,3 +108,34 @@ def test_cluster_handoffs_equal_one_cta_handoffs(name, kind):
     np.testing.assert_array_equal(i0, i1)
     np.testing.assert_array_equal(f0, f1)
     np.testing.assert_array_equal(V0, V1)
+
+
+@pytest.mark.parametrize("name", ["case2000_synth", "case6500_synth"])
+def test_fp64_subset_on_clusters_equals_one_cta(name):
+    """A small FP64 re-solve (gs2g_run_subset with at most one row per 8 CTAs:
+    the fallback of rows a mixed sweep did not converge) runs each row on a
+    cluster of 8 CTAs sharing its Schur updates and dense LUs; bit-identical
+    to the one-CTA rows and to the same rows of a full FP64 run."""
+    from gpusim2grid_b200._native import lib
+    from gpusim2grid_b200.synthetic import grid_by_name
+    g = grid_by_name(name, 0)
+    rows = [[int(b)] for b in n1_branches(g)[:24]]
+    sub = np.array([1, 5, 11, 17, 23], dtype=np.int32)
+    ca = ContingencyAnalysisGPU(g.as_tuple(), init_from_n_powerflow=False, precision="fp64", nb_iter=10,
+                                scheduling="continuous", tol=1e-8, start="flat")
+    ca.set_branch_data(*g.branch_data())
+    ca.add_contingencies_by_branch_id(rows)
+    ca.compute()
+    full = ca.V_results, ca.get_row_status(), ca.get_row_iterations()
+    s = ca.session
+    out = []
+    for cluster in (0, 1):
+        s.set_handoff(cluster)
+        s.run(10, 1e-8, False, lib.PREC_FP64, lib.START_VINIT, refactor=lib.REFACTOR_EVERY)
+        s.run_subset(sub, 10, 1e-8, False, lib.PREC_FP64, lib.START_VINIT, refactor=lib.REFACTOR_EVERY)
+        V, res, st, it = s.results()
+        out.append((V[sub], st[sub], it[sub]))
+    for k in range(3):
+        np.testing.assert_array_equal(out[0][k], out[1][k])
+        np.testing.assert_array_equal(out[1][k], full[k][sub])
+    assert np.all(out[1][1] == 0)
