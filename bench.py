@@ -488,14 +488,26 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
         # mixed precision from flat (separates the strategy from the start)
         mixed_flat_value, _, _, _ = arm(lib.PREC_MIXED, lib.REFACTOR_ADAPTIVE, lib.START_VINIT)
         if strat == lib.REFACTOR_BASE_CHORD:
-            # the same sweep from the base case's V without the network: what
-            # the learned start adds over the method without it
-            bv, _, stb, itb = arm(lib.PREC_MIXED, strat, lib.START_BASE, ratio, reuse)
+            # the same step from the base case's V without the network (sweep
+            # and FP64 re-solve of the rows left unconverged): what the
+            # learned start adds over the method without it
+            def base_step():
+                s.run(MAX_ITER, TOL, False, lib.PREC_MIXED, lib.START_BASE, 0.0, 0, False, strat, ratio, reuse)
+                return s.timings()["kernel_ms"] + ca.fp64_fallback()
+
+            base_step()
+            ms_b = []
+            for _ in range(max(1, min(steps, 3))):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                ms_b.append(base_step())
+            _, _, stb, itb = s.results()
+            bv = int((stb == 0).sum()) / (np.mean(ms_b) / 1e3)
             base_start = {"value": round(bv, 1), "newton_iters_total": int(itb.sum()),
-                          "rows_converged": int((stb == 0).sum()),
+                          "rows_converged": int((stb == 0).sum()), "rows_fp64_fallback": ca.fallback_rows,
                           "learned_over_base_start": round(value / world / bv, 3),
                           "note": "same rows, precision and strategy, every row starting from the converged base "
-                                  "case (no network; sweep time only)"}
+                                  "case: the sweep and the FP64 re-solve of unconverged rows, without the network"}
 
     # phase split of the measured arm (one extra profiled run, not timed)
     if learned:

@@ -94,8 +94,8 @@ class _BatchSweep:
         self.start = start
         self.strategy = strategy
         self.handle_disconnected_grid = handle_disconnected_grid
-        self.refactor_ratio = 0.3
-        self.max_reuse = 3
+        self._refactor_ratio = None  # None: the strategy's default
+        self._max_reuse = None
         # mixed precision, continuous schedule: rows that end MAX_ITER or
         # DIVERGED are re-solved in plain FP64 from Vinit, whose verdict stands
         self.fallback = "fp64"
@@ -249,6 +249,32 @@ class _BatchSweep:
         and V0 on the device, wall), n_rescued (rows restarted), n_base_start
         (rows that began from the base case: its mismatch was the smaller)."""
         return dict(self._warm)
+
+    @property
+    def refactor_ratio(self):
+        """Contraction per step below which a row keeps its factor ('adaptive':
+        its own LU, default 0.3; 'base_chord': the shared base factor, default
+        0.7 -- a step on it is cheap, several rows share each factor read).
+        Learned runs use ``set_learned_start``'s values."""
+        if self._refactor_ratio is not None:
+            return self._refactor_ratio
+        return 0.7 if self._strategy == "base_chord" else 0.3
+
+    @refactor_ratio.setter
+    def refactor_ratio(self, value):
+        self._refactor_ratio = None if value is None else float(value)
+
+    @property
+    def max_reuse(self):
+        """Steps on one factor at most (defaults: 3 'adaptive', 8
+        'base_chord'); see ``refactor_ratio``."""
+        if self._max_reuse is not None:
+            return self._max_reuse
+        return 8 if self._strategy == "base_chord" else 3
+
+    @max_reuse.setter
+    def max_reuse(self, value):
+        self._max_reuse = None if value is None else int(value)
 
     @property
     def strategy(self):

@@ -53,6 +53,18 @@
 #define GS2G_CHORD_ROWS 4
 #endif
 constexpr int CK = GS2G_CHORD_ROWS;  // rows per CTA
+
+// Unrolling of the chord loops whose loads form dependent chains (index ->
+// right-hand side): the head and tail solves' entry loops and the dense
+// product's column loop.  Build-time; the defaults were measured fastest.
+#ifndef GS2G_CHORD_SOLVE_UNROLL
+#define GS2G_CHORD_SOLVE_UNROLL 4
+#endif
+#ifndef GS2G_CHORD_DENSE_UNROLL
+#define GS2G_CHORD_DENSE_UNROLL 8
+#endif
+#define GS2G_PRAGMA(x) _Pragma(#x)
+#define GS2G_UNROLL(n) GS2G_PRAGMA(unroll n)
 constexpr int CB_MAX = 10;  // Broyden steps kept per row (the memory restarts beyond)
 
 // the CK right-hand sides of one unknown, loaded as one vector (or two)
@@ -300,6 +312,7 @@ __device__ __noinline__ void chord_head_fw(const DevPlan P, const T* __restrict_
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int i = P.lev_piv[q0];
       SlotVec<T> acc = y[i];
+      GS2G_UNROLL(GS2G_CHORD_SOLVE_UNROLL)
       for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fwv[q], y[P.fw_col[q]]);
       y[i] = acc;
     }
@@ -313,6 +326,7 @@ __device__ __noinline__ void chord_tail_fw(const DevPlan P, const T* __restrict_
   for (int ti = threadIdx.x; ti < P.nt; ti += BS) {
     const int i = P.p + ti;
     SlotVec<T> acc = y[i];
+    GS2G_UNROLL(GS2G_CHORD_SOLVE_UNROLL)
     for (int q = P.fw_ptr[i]; q < P.fw_ptr[i + 1]; ++q) fms_slots(acc, fwv[q], y[P.fw_col[q]]);
     y[i] = acc;
   }
@@ -337,7 +351,7 @@ __device__ __noinline__ void chord_dense(const DevPlan P, const T* __restrict__ 
       for (int s = 0; s < CK; ++s) acc[u].v[s] = T(0);
     const int nr = min(4, (nt - r0 - tid + BS - 1) / BS);  // rows of this thread in the pass (may be <= 0)
     const T* base = Sinv + r0 + tid;
-#pragma unroll 2
+    GS2G_UNROLL(GS2G_CHORD_DENSE_UNROLL)
     for (int j = 0; j < nt; ++j) {
       const SlotVec<T> yj = ys[j];
       const T* col = base + (int64_t)j * P.dim;
@@ -361,6 +375,7 @@ __device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict_
     for (int q0 = P.lev_piv_ptr[lv] + threadIdx.x; q0 < P.lev_piv_ptr[lv + 1]; q0 += BS) {
       const int k = P.lev_piv[q0];
       SlotVec<T> acc = y[k];
+      GS2G_UNROLL(GS2G_CHORD_SOLVE_UNROLL)
       for (int q = P.bw_ptr[k]; q < P.bw_ptr[k + 1]; ++q) fms_slots(acc, bwv[q], y[P.bw_row[q]]);
       const T d = fHV[k];
 #pragma unroll

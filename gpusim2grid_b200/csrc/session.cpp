@@ -495,8 +495,12 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
     a.base_fwv = s->d_base_fwv.as<char>();
     a.base_bwv = s->d_base_bwv.as<char>();
   }
-  a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : 0.3;
-  a.max_reuse = o.max_reuse > 0 ? o.max_reuse : 3;
+  // defaults: a step on the shared base factor is cheap (several rows share
+  // each factor read), so base_chord keeps it longer than adaptive keeps a
+  // row's own LU
+  const bool chord_policy = o.refactor_policy == GS2G_REFACTOR_BASE_CHORD;
+  a.refactor_ratio = o.refactor_ratio > 0 ? o.refactor_ratio : (chord_policy ? 0.7 : 0.3);
+  a.max_reuse = o.max_reuse > 0 ? o.max_reuse : (chord_policy ? 8 : 3);
   a.factors_out = out.factors;
   // rescue (per-row starts, continuous schedule): with a base case the row
   // starts from the base V when that has the smaller mismatch, and an

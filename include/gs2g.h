@@ -84,8 +84,8 @@ typedef struct gs2g_run_opts {
    * max_reuse steps (the reference's 'direct_iter0_only' idea, made adaptive);
    * the FP64 mismatch still converges every row to tol. */
   int refactor_policy;
-  double refactor_ratio; /* adaptive: <= 0 selects 0.3 */
-  int max_reuse;         /* adaptive: <= 0 selects 3 */
+  double refactor_ratio; /* <= 0 selects 0.3 (adaptive) or 0.7 (base_chord) */
+  int max_reuse;         /* <= 0 selects 3 (adaptive) or 8 (base_chord) */
   /* 1: with GS2G_START_ROWS and the continuous schedule, guard each row's
    * given start (a learned or otherwise predicted one) against a bad
    * prediction.  With a base case, a row whose mismatch at its given start
