@@ -113,6 +113,54 @@ __device__ __forceinline__ T schur_entry(const T* __restrict__ HV, int4 rec) {
 // (each lane sums every contribution to one entry S[ti][col] and writes it
 // once), four groups per lane in flight: their entry records are loaded
 // together, then their factor values.
+// Sparse head LU, level by level, in place on the head factor values HV.
+// With parts > 1 the `parts` CTAs of a cluster (this one: rank `part`) split
+// each level's tasks and pass cluster barriers instead of block barriers;
+// a task's arithmetic does not depend on who runs it.
+template <typename T>
+__device__ __noinline__ void head_lu(const DevPlan P, T* HV, const double pfloor, const int part, const int parts) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gwarp = part * NWARP + warp, nwarps = parts * NWARP;
+  const int gtid = part * BS + tid, nthreads = parts * BS;
+  auto barrier = [&]() {
+    if (parts > 1)
+      dense::cluster_barrier();
+    else
+      __syncthreads();
+  };
+  for (int lv = 0; lv < P.n_levels; ++lv) {
+    const int t0 = P.lev_ptr[lv], tb = P.lev_big[lv], t1 = P.lev_ptr[lv + 1];
+    // long tasks: one warp each, products split over the lanes
+    for (int t = t0 + gwarp; t < tb; t += nwarps) {
+      const int out = P.task_out[t];
+      const int q1 = P.task_pend[t];
+      T acc_p = T(0);
+      for (int q = P.task_pbeg[t] + lane; q < q1; q += 32) acc_p += HV[P.pair_l[q]] * HV[P.pair_u[q]];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc_p += __shfl_xor_sync(0xffffffffu, acc_p, o);
+      if (lane == 0) {
+        T acc = (P.task_has_a[t] ? HV[out] : T(0)) - acc_p;
+        if (out < P.p) acc = clamp_pivot(acc, pfloor);
+        HV[out] = acc;
+      }
+    }
+    for (int t = tb + gtid; t < t1; t += nthreads) {
+      const int out = P.task_out[t];
+      T acc = P.task_has_a[t] ? HV[out] : T(0);
+      const int q1 = P.task_pend[t];
+      for (int q = P.task_pbeg[t]; q < q1; ++q) acc -= HV[P.pair_l[q]] * HV[P.pair_u[q]];
+      if (out < P.p) acc = clamp_pivot(acc, pfloor);
+      HV[out] = acc;
+    }
+    barrier();
+    for (int t = t0 + gtid; t < t1; t += nthreads) {
+      const int dg = P.task_diag[t];
+      if (dg >= 0) HV[P.task_out[t]] /= HV[dg];
+    }
+    barrier();
+  }
+}
+
 template <typename T>
 __device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__ HV, T* __restrict__ S, int part = 0,
                                           int parts = 1) {
@@ -1101,50 +1149,22 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       __syncthreads();
 
       prof.mark(PH_FILL);
-      // ---- sparse head LU, level by level --------------------------------
-      for (int lv = 0; lv < P.n_levels; ++lv) {
-        const int t0 = P.lev_ptr[lv], tb = P.lev_big[lv], t1 = P.lev_ptr[lv + 1];
-        {
-          // long tasks: one warp each, products split over the lanes
-          const int lane = tid & 31, warp = tid >> 5;
-          for (int t = t0 + warp; t < tb; t += NWARP) {
-            const int out = P.task_out[t];
-            const int q1 = P.task_pend[t];
-            T part = T(0);
-            for (int q = P.task_pbeg[t] + lane; q < q1; q += 32) part += HV[P.pair_l[q]] * HV[P.pair_u[q]];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-            if (lane == 0) {
-              T acc = (P.task_has_a[t] ? HV[out] : T(0)) - part;
-              if (out < P.p) acc = clamp_pivot(acc, a.pivot_floor);
-              HV[out] = acc;
-            }
-          }
-        }
-        for (int t = tb + tid; t < t1; t += BS) {
-          const int out = P.task_out[t];
-          T acc = P.task_has_a[t] ? HV[out] : T(0);
-          const int q1 = P.task_pend[t];
-          for (int q = P.task_pbeg[t]; q < q1; ++q) acc -= HV[P.pair_l[q]] * HV[P.pair_u[q]];
-          if (out < P.p) acc = clamp_pivot(acc, a.pivot_floor);
-          HV[out] = acc;
-        }
-        __syncthreads();
-        for (int t = t0 + tid; t < t1; t += BS) {
-          const int dg = P.task_diag[t];
-          if (dg >= 0) HV[P.task_out[t]] /= HV[dg];
-        }
-        __syncthreads();
-      }
-
-      prof.mark(PH_HEAD);
-      if (cl != nullptr && P.nt > 0) {
+      // ---- sparse head LU, level by level (with a cluster: all its CTAs) ---
+      const bool shared_factor = cl != nullptr && P.nt > 0;
+      if (shared_factor) {
         // the cluster's other CTAs join: post the command, two barriers
-        // (posted; read by all), then the Schur update split by tail rows
-        // (a barrier) and the shared dense factorization
+        // (posted; read by all); the head factor's values and the scattered
+        // tail are complete before the first of them
         if (tid == 0) *cl->cmd = CLUSTER_CMD_LU;
         dense::cluster_barrier();
         dense::cluster_barrier();
+      }
+      head_lu<T>(P, HV, a.pivot_floor, 0, shared_factor ? cl->parts : 1);
+
+      prof.mark(PH_HEAD);
+      if (shared_factor) {
+        // the Schur update split by tail rows (a barrier), then the shared
+        // dense factorization
         schur_update<T>(P, HV, S, 0, cl->parts);
         dense::cluster_barrier();
         prof.mark(PH_SCHUR);
@@ -1279,18 +1299,19 @@ __device__ __forceinline__ int ld_shared_rank0(const int* p) {
 // The single-row sweep with a cluster of HANDOFF_CLUSTER CTAs per row (FP32
 // or FP64 factors): the leading CTA (rank 0) runs the row's whole Newton
 // loop in its workspace as sweep_kernel does, and the other CTAs join each
-// of its factorizations from the Schur update of the dense tail on (split
-// by tail rows) through the dense tail LU (dense_lu_cluster), the steps
-// whose work grows fastest with the tail.  For the few rows the chord sweep
+// of its factorizations: the sparse head LU (each level's tasks split),
+// the Schur update of the dense tail (split by tail rows) and the dense tail
+// LU (dense_lu_cluster).  For the few rows the chord sweep
 // hands off and the few rows of an FP64 re-solve, whose factorizations
 // would otherwise each run on one SM after every other row has finished.
 // When the rows outnumber the clusters, every CTA takes rows of its own.
 // Protocol, all through cluster barriers (every CTA passes the same number):
 // per row, the leader takes a queue entry and publishes it (barrier), every
 // CTA reads it (barrier); then for each factorization the leader posts
-// CLUSTER_CMD_LU (barrier, read, barrier), all update their Schur rows
-// (barrier) and factor together; after the row it posts CLUSTER_CMD_DONE
-// (barrier, read, barrier).
+// CLUSTER_CMD_LU (barrier, read, barrier) once the Jacobian is scattered,
+// and all run the head LU (two barriers per level), their Schur rows
+// (barrier) and the dense LU together; after the row it posts
+// CLUSTER_CMD_DONE (barrier, read, barrier).
 constexpr int HANDOFF_CLUSTER = 8;
 
 template <typename T>
@@ -1334,7 +1355,7 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
   // the row lives in the leader's workspace
   char* ws = a.workspace + (int64_t)(blockIdx.x - rank) * a.ws_stride;
   T* S = reinterpret_cast<T*>(ws + ws_layout<T>(P).S);
-  const T* HV = reinterpret_cast<const T*>(ws + ws_layout<T>(P).HV);
+  T* HV = reinterpret_cast<T*>(ws + ws_layout<T>(P).HV);
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0 && rank == 0);
   const ClusterLu cl{&s_cmd, HANDOFF_CLUSTER};
   for (;;) {
@@ -1354,8 +1375,10 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
         const int cmd = ld_shared_rank0(&s_cmd);
         dense::cluster_barrier();
         if (cmd != CLUSTER_CMD_LU) break;
-        // the leader's head factor and scattered tail are complete (posted
-        // after them); its Schur rows, a barrier, then the shared LU
+        // the leader's Jacobian values are in place (posted after them): the
+        // head LU's share of each level, the Schur rows, a barrier, then the
+        // shared dense LU
+        head_lu<T>(P, HV, a.pivot_floor, rank, HANDOFF_CLUSTER);
         schur_update<T>(P, HV, S, rank, HANDOFF_CLUSTER);
         dense::cluster_barrier();
         dense_lu_cluster<T>(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, HANDOFF_CLUSTER);

@@ -209,8 +209,8 @@ class Session {
 
   void run_subset(IArr rows, int max_iter, double tol, bool fixed_iters, int precision, int start,
                   double pivot_floor, int n_ctas, int refactor, double refactor_ratio, int max_reuse, bool rescue,
-                  int iters_per_round) {
-    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, false, refactor,
+                  int iters_per_round, bool profile) {
+    gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
                                 refactor_ratio, max_reuse, rescue, iters_per_round);
     const int n = (int)rows.size();
     const int* rp = rows.data();
@@ -601,7 +601,7 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("run_subset", &Session::run_subset, py::arg("rows"), py::arg("max_iter"), py::arg("tol"),
            py::arg("fixed_iters"), py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0,
            py::arg("n_ctas") = 0, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
-           py::arg("rescue") = false, py::arg("iters_per_round") = 1)
+           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("profile") = false)
       .def("branch_loading", &Session::branch_loading)
       .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("set_handoff", &Session::set_handoff, py::arg("cluster"))

@@ -1427,6 +1427,11 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   a.workspace = s->d_ws.as<char>();
   a.ws_stride = wsb;
   a.n_rescued = s->d_queue.as<int>() + 1;
+  if (o.profile_phases) {
+    s->d_phase.ensure(gs2g::N_PHASES * sizeof(unsigned long long));
+    ck(cudaMemsetAsync(s->d_phase.p, 0, gs2g::N_PHASES * sizeof(unsigned long long), s->stream), "phase reset");
+    a.phase_cycles = s->d_phase.as<unsigned long long>();
+  }
   ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_sub > 0 && cluster)
@@ -1438,6 +1443,17 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   float ms = 0;
   ck(cudaEventElapsedTime(&ms, s->ev0, s->ev1), "event time");
   s->tm.kernel_ms = ms;
+  for (int q = 0; q < GS2G_N_PHASES; ++q) s->tm.phase_cycles[q] = s->tm.phase_share[q] = 0;
+  if (o.profile_phases) {
+    unsigned long long c[gs2g::N_PHASES];
+    ck(cudaMemcpy(c, s->d_phase.p, sizeof(c), cudaMemcpyDeviceToHost), "read phases");
+    double tot = 0;
+    for (int q = 0; q < gs2g::N_PHASES; ++q) tot += (double)c[q];
+    for (int q = 0; q < gs2g::N_PHASES; ++q) {
+      s->tm.phase_cycles[q] = (double)c[q];
+      s->tm.phase_share[q] = tot > 0 ? c[q] / tot : 0;
+    }
+  }
   s->tm.total_ms = ms_since(t0);
   s->tm.total_iters = -1;
   GS2G_CATCH
