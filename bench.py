@@ -808,19 +808,25 @@ def run_ours_multi(args):
         f.results_to_host = True
     gc.collect()
     gc.freeze()
-    e2e_s = []
+    e2e_s, e2e_parts = [], []
     for i in range(args.warmup + args.steps):
         if i == args.warmup:
-            e2e_s = []
+            e2e_s, e2e_parts = [], []
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for f, (g, trips, p, q) in zip(facades, parts):
             _set_rows(f, trips, p, q, g)
-        compute_many(facades)
+        t1 = time.perf_counter()
+        kms = compute_many(facades)
+        t2 = time.perf_counter()
         outs = [f.results_view()[:3] for f in facades]
         outs = [(v, st, r) for v, r, st in outs]
-        e2e_s.append(time.perf_counter() - t0)
+        t3 = time.perf_counter()
+        e2e_s.append(t3 - t0)
+        e2e_parts.append((t1 - t0, t2 - t1, t3 - t2, kms / 1e3))
     gc.unfreeze()
+    e2e_split = dict(zip(["rows_in_ms", "compute_ms", "results_out_ms", "kernel_ms"],
+                         [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
     n_conv_e2e = sum(int((o[1] == 0).sum()) for o in outs)
     e2e_value = world * n_conv_e2e / float(np.mean(e2e_s))
     h2d = sum(2 * p.nbytes + 4 * (len(t) + 1) + 4 * sum(len(x) for x in t) for _, t, p, _ in parts)
@@ -857,7 +863,7 @@ def run_ours_multi(args):
                              f"Newton step x steps, a step on the shared base factor without its factor read "
                              f"({chord_steps} of {steps_all} steps) = {launch_bytes}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "split": e2e_split},
         "gpu_launches": args.steps * per_step_launches,
         "clocks": clocks,
     }

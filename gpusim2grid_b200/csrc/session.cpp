@@ -97,6 +97,7 @@ struct gs2g_session {
   std::vector<double> yff, yft, ytf, ytt;
   std::vector<int> k_ff, k_tt, k_ft, k_tf;  // Ybus entry of each branch term
   std::vector<uint8_t> is_bridge;           // branch whose loss alone islands the grid
+  std::vector<uint64_t> cut_label;          // cycle-space label per branch (islanding pre-check)
   int base_components = 1;                  // connected components of the branch graph
   DevBuf d_br_from, d_br_to, d_br_y;        // branch data on the device (flows)
   DevBuf d_br_rate;                         // limits in per unit
@@ -266,7 +267,8 @@ void compute_bridges(gs2g_session* s) {
   }
   s->is_bridge.assign(m, 0);
   std::vector<int> tin(n, -1), low(n, 0), it(n, 0), pe(n, -1);
-  std::vector<int> stack;
+  std::vector<int> stack, post;
+  post.reserve(n);
   int timer = 0, comps = 0;
   for (int root = 0; root < n; ++root) {
     if (tin[root] >= 0) continue;
@@ -290,6 +292,7 @@ void compute_bridges(gs2g_session* s) {
         }
       } else {
         stack.pop_back();
+        post.push_back(v);
         if (!stack.empty()) {
           const int u = stack.back();
           low[u] = std::min(low[u], low[v]);
@@ -299,6 +302,60 @@ void compute_bridges(gs2g_session* s) {
     }
   }
   s->base_components = comps;
+
+  // Cycle-space labels: a pseudo-random 64-bit value per non-tree branch of
+  // the DFS forest, and for a tree branch the XOR of the values of the
+  // non-tree branches whose fundamental cycle runs through it (the XOR of
+  // the values incident to the subtree below it).  Every cycle crosses an
+  // edge cut an even number of times, so the labels of any cut XOR to zero:
+  // trips whose labels are linearly independent over GF(2) cannot contain a
+  // cut and leave the grid connected, with certainty; dependent labels only
+  // call for the exact check.  (Bridges are the branches labelled zero.)
+  s->cut_label.assign(m, 0);
+  std::vector<uint64_t> sub(n, 0);
+  auto mix = [](uint64_t x) {  // splitmix64 finaliser
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+  };
+  for (int l = 0; l < m; ++l) {
+    if (!edge(l)) continue;
+    const int f = s->br_from[l], t = s->br_to[l];
+    if (pe[f] == l || pe[t] == l) continue;  // tree branch
+    const uint64_t r = mix((uint64_t)l + 0x51ed27ull) | 1ull;
+    s->cut_label[l] = r;
+    sub[f] ^= r;
+    sub[t] ^= r;
+  }
+  for (const int v : post) {  // children before parents
+    const int l = pe[v];
+    if (l < 0) continue;
+    s->cut_label[l] = sub[v];
+    const int u = s->br_from[l] == v ? s->br_to[l] : s->br_from[l];
+    sub[u] ^= sub[v];
+  }
+}
+
+// True when the labels of the given branches are linearly independent over
+// GF(2) (no nonempty subset XORs to zero): removing them leaves the grid as
+// connected as it was.  Branches open at one end join nothing and are left
+// out.
+bool trips_keep_connected(const gs2g_session* s, const std::vector<int>& ids) {
+  uint64_t basis[64];
+  int nb = 0;
+  for (const int l : ids) {
+    if (s->br_from[l] < 0 || s->br_to[l] < 0) continue;
+    uint64_t x = s->cut_label[l];
+    for (int i = 0; i < nb && x; ++i) x = std::min(x, x ^ basis[i]);
+    if (x == 0) return false;
+    basis[nb++] = x;
+    // keep the basis sorted by leading bit, highest first, so the reduction
+    // above clears each basis vector's leading bit in turn
+    for (int i = nb - 1; i > 0 && basis[i] > basis[i - 1]; --i) std::swap(basis[i], basis[i - 1]);
+    if (nb == 64) return false;  // more trips than label bits: check exactly
+  }
+  return true;
 }
 
 void assemble_rows(gs2g_session* s) {
@@ -339,7 +396,7 @@ void assemble_rows(gs2g_session* s) {
       if (!uniq.empty()) {
         bool island = s->base_components > 1;
         for (size_t q = 0; q < uniq.size() && !island; ++q) island = s->is_bridge[uniq[q]] != 0;
-        if (!island && uniq.size() >= 2) {
+        if (!island && uniq.size() >= 2 && !trips_keep_connected(s, uniq)) {
           DSU d(n);
           size_t ui = 0;
           int comps = n;

@@ -135,6 +135,36 @@ def test_islanding_flags_every_single_and_some_double_outages(g118):
         assert (st[r] == RowStatus.NOT_SIMULATED) == islanded, (r, ids)
 
 
+@pytest.mark.parametrize("grid", ["g118", "g2000"])
+def test_islanding_flags_of_cut_pairs_and_triples(grid, request):
+    """Rows that trip two or three branches are pre-checked by the branches'
+    cycle-space labels (independent labels: connected for certain) and, when
+    the labels are dependent, by the exact connectivity check.  Cut pairs (the
+    two branches of a bus of degree 2), triples holding such a pair, random
+    pairs and triples: the flags must equal the oracle's connectivity check."""
+    g = request.getfixturevalue(grid)
+    m = g.n_branch
+    deg = np.bincount(np.concatenate([g.branch_from, g.branch_to]), minlength=g.n_bus)
+    rng = np.random.default_rng(17)
+    rows = []
+    for b in np.flatnonzero(deg == 2)[:40]:
+        pair = sorted(int(l) for l in np.flatnonzero((g.branch_from == b) | (g.branch_to == b)))
+        rows.append(pair)
+        rows.append(sorted(set(pair) | {int(rng.integers(m))}))
+    for _ in range(120):
+        rows.append(sorted(int(v) for v in rng.choice(m, 2, replace=False)))
+        rows.append(sorted(int(v) for v in rng.choice(m, 3, replace=False)))
+    ca = ContingencyAnalysisGPU(g.as_tuple(), init_from_n_powerflow=False, nb_iter=10, scheduling="continuous",
+                                start="flat", precision="mixed", strategy="base_chord")
+    ca.set_branch_data(*g.branch_data())
+    ca.add_contingencies_by_branch_id(rows)
+    ca.compute()
+    st = ca.get_row_status()
+    islanded = np.array([bool(O.islands(g.n_bus, g.branch_from, g.branch_to, ids)) for ids in rows])
+    assert islanded.sum() >= 20 and (~islanded).sum() >= 100
+    np.testing.assert_array_equal(st == RowStatus.NOT_SIMULATED, islanded)
+
+
 def test_set_injections_from_elements_needs_a_grid_object(g118):
     """Array-tuple mode has no loads or generators to map: RuntimeError, as in
     the reference (``injection_sweep/gpu_facade.py:394``)."""
