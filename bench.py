@@ -49,6 +49,8 @@ sys.path.insert(0, ROOT)
 
 # name -> (grid, row kind, rows, scenario seed, training-row mix)
 WORKLOADS = {
+    # one system solved again and again (the single-solve path, AcPfGPU / acpf_nr_gpu), 118-bus grid
+    "single_case118_synth": ("case118_synth", "single", 1, None, {}),
     # every non-islanding single outage of the 2000-bus grid at base injections
     "n1_sweep_case2000_synth": ("case2000_synth", "n1", None, None, dict(broad=0.5)),
     # 4096 load-scaling scenarios (global U(0.8,1.2) x per-bus lognormal(0,0.1)) on the 6500-bus grid
@@ -147,6 +149,8 @@ def _workload(name):
             parts.append((g, scenario_outages(g, n_rows, max_trips=2, seed=seed + 10 * i + 1), p, q))
         return parts
     g = grid_by_name(gname, 0)
+    if kind == "single":
+        return g, None, None, None
     cand = n1_branches(g)
     if kind == "n1":
         return g, [[int(b)] for b in cand], None, None
@@ -877,6 +881,98 @@ def run_ours_multi(args):
 
 
 # ---------------------------------------------------------------- reference arm
+def _single_cpu_rate(g, budget_s, threads):
+    """Solves/s of the compiled CPU NR (oracle/cpu_nr.cpp) on copies of one
+    system, ``threads`` host threads over the copies; about ``budget_s``
+    seconds."""
+    from oracle import cpu_nr
+    Y, V0, S, _, _, pv, pq = g.as_tuple()
+
+    def run(k):
+        sb = np.repeat(np.asarray(S, dtype=np.complex128)[None, :], k, axis=0)
+        t0 = time.perf_counter()
+        _, st, _, _, _ = cpu_nr.sweep(Y, V0, S, pv, pq, sbus_rows=sb, max_iter=MAX_ITER, tol=TOL, threads=threads)
+        return int((st == 0).sum()), time.perf_counter() - t0
+
+    conv, dt = run(16 * threads)
+    k = max(16 * threads, int(conv / dt * budget_s))
+    conv, dt = run(k)
+    return conv / dt, k
+
+
+def run_ours_single(args):
+    """The single-solve path: one system (AcPfGPU, the reference's acpf_nr_gpu
+    / AcPfGPU facade) solved again from Vinit each step, step-then-test
+    iteration as the reference's run_single_system_nr.  value: solves/s from
+    the session's device time; e2e: the facade's resolve() with the host
+    start voltage in and solve() with the host voltage out, wall time."""
+    import torch
+    from gpusim2grid_b200 import AcPfGPU, replicas
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    replicas.init("nccl", timeout_s=900)
+    g, _, _, _ = _workload(args.workload)
+    grid = g.as_tuple()
+    V0 = grid[1]
+    ac = AcPfGPU(grid, precision=args.precision, max_iter=MAX_ITER, tol=TOL, device=local,
+                 init_from_n_powerflow=False)
+    for _ in range(args.warmup):
+        ac.resolve(V0)
+    clk = ClockSampler(local)
+    clk.start()
+    replicas.barrier()
+    ks, its = [], []
+    for _ in range(args.steps):
+        t = ac.resolve(V0)
+        ks.append(t.t_kernel_ms)
+        its.append(t.nb_iter)
+    replicas.barrier()
+    clocks = clk.stop()
+    total_ms = replicas.max_over_ranks(float(np.sum(ks)), device="cuda")
+    value = world * args.steps / (total_ms / 1e3)
+    gc.collect()
+    e2e_s = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ac.resolve(V0)
+        V = ac.solve()
+        if i >= args.warmup:
+            e2e_s.append(time.perf_counter() - t0)
+    e2e_value = world / float(np.mean(e2e_s))
+    info = ac.session.info()
+    w = 4 if args.precision == "mixed" else 8
+    b_fact, b_iter = algorithmic_bytes(info, w)
+    it = int(np.mean(its))
+    achieved = (b_fact * it + b_iter * it) / (total_ms / args.steps / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 mismatch/V, f32 J/LU",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": args.workload, "grid": g.name, "rows": 1, "start": "flat", "precision": args.precision,
+                   "tol_pu": TOL, "max_iter": MAX_ITER, "schedule": "single solve: step, then test the mismatch "
+                   "before it", "parallelism": f"replicas x{world}", "l2": "inputs far below L2 (single solve)"},
+        "newton_iters": it,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "traffic": None,
+                     "note": f"peak {peak_kind}; one 118-bus system is a latency-bound chain of phases on one CTA: "
+                             f"algorithmic bytes = {b_fact} per LU + {b_iter} per step, one LU per step"},
+        "e2e": {"value": round(e2e_value, 1), "unit": "solves/s", "h2d_bytes_per_step": int(V0.nbytes),
+                "d2h_bytes_per_step": int(V.nbytes)},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        v, k = _single_cpu_rate(g, args.cpu_budget_s, 1)
+        line["cpu_baseline"] = {"value": round(v, 2), "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": f"{k} solves of the same system on one thread, flat start, compiled FP64 "
+                                          f"NR (oracle/cpu_nr.cpp)", "cpu_model": _cpu_model()}
+    replicas.finish()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def run_reference(args):
     """The reference's CPU path restated (the reference itself cannot be
     built here): the compiled FP64 Newton-Raphson of oracle/cpu_nr.cpp on
@@ -887,19 +983,31 @@ def run_reference(args):
     if rank != 0:
         return
     w = _workload(args.workload)
-    multi = isinstance(w, list)
-    parts = w if multi else [w]
-    bases = [CpuBaseline(g, trips, p, q, args.cpu_budget_s / len(parts)) for g, trips, p, q in parts]
+    if WORKLOADS[args.workload][1] == "single":
+        threads = _host_threads()
+        g = w[0]
+        for _ in range(args.warmup):
+            _single_cpu_rate(g, args.cpu_budget_s, threads)
+        runs = [_single_cpu_rate(g, args.cpu_budget_s, threads) for _ in range(args.steps)]
+        value = float(np.mean([r[0] for r in runs]))
+        n = 1
+        sample = (f"{runs[-1][1]} solves of the same system, OpenMP over the copies, flat start, compiled FP64 NR "
+                  f"(oracle/cpu_nr.cpp)")
+        bases = [type("T", (), {"threads": threads})()]
+    else:
+        multi = isinstance(w, list)
+        parts = w if multi else [w]
+        bases = [CpuBaseline(g, trips, p, q, args.cpu_budget_s / len(parts)) for g, trips, p, q in parts]
 
-    def one():
-        return len(bases) / sum(1.0 / max(b.measure(), 1e-12) for b in bases)
+        def one():
+            return len(bases) / sum(1.0 / max(b.measure(), 1e-12) for b in bases)
 
-    for _ in range(args.warmup):
-        one()
-    vals = [one() for _ in range(args.steps)]
-    value = float(np.mean(vals))
-    n = sum(b.n for b in bases)
-    sample = "; ".join(f"{g.name}: {b.sample}" for (g, _, _, _), b in zip(parts, bases))
+        for _ in range(args.warmup):
+            one()
+        vals = [one() for _ in range(args.steps)]
+        value = float(np.mean(vals))
+        n = sum(b.n for b in bases)
+        sample = "; ".join(f"{g.name}: {b.sample}" for (g, _, _, _), b in zip(parts, bases))
     print(json.dumps({
         "impl": "reference",
         "metric": METRIC,
@@ -922,6 +1030,8 @@ if __name__ == "__main__":
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif WORKLOADS[a.workload][1] == "single":
+        run_ours_single(a)
     elif WORKLOADS[a.workload][1] == "multi":
         run_ours_multi(a)
     else:

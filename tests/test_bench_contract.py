@@ -13,7 +13,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.mark.parametrize("workload", ["n1_sweep_case2000_synth", "injection_sweep_case6500_synth"])
+@pytest.mark.parametrize("workload", ["n1_sweep_case2000_synth", "injection_sweep_case6500_synth",
+                                      "single_case118_synth"])
 def test_reference_arm_json_line(workload):
     cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "0",
            "--cpu-budget-s", "0.5"]
