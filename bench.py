@@ -252,19 +252,22 @@ class ClockSampler:
         self._t.start()
 
     def _run_nvml(self):
+        while not self._stop.is_set():
+            self._sample_nvml()
+            self._stop.wait(0.01)
+
+    def _sample_nvml(self):
         nv, h = self._nvml
         bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while not self._stop.is_set():
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append([str(self.index), str(sm), str(mx), "",
-                                     *["Active" if r & b else "Not Active" for b in bits]])
-            except Exception:
-                pass
-            self._stop.wait(0.01)
+        try:
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append([str(self.index), str(sm), str(mx), "",
+                                 *["Active" if r & b else "Not Active" for b in bits]])
+        except Exception:
+            pass
 
     def _run(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -284,6 +287,9 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        if not self.samples and self._nvml:
+            # a timed region shorter than the first poll: one reading at its end
+            self._sample_nvml()
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]

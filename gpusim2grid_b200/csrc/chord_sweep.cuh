@@ -79,10 +79,11 @@ __device__ __forceinline__ void fms_slots(SlotVec<T>& acc, T a, const SlotVec<T>
   for (int s = 0; s < CK; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
 }
 
-// Workspace of one chord CTA: V [n] and F [dim] per slot, the interleaved
-// right-hand sides y [dim] x CK, then the Broyden steps [CK][CB_MAX][dim].
+// Workspace of one chord CTA: V [n] per slot, the interleaved right-hand
+// sides y [dim] x CK (the mismatch writes F there), then the Broyden steps
+// [CK][CB_MAX][dim].
 struct ChordWs {
-  int64_t V, F, y, S, total;
+  int64_t V, y, S, total;
 };
 
 template <typename T>
@@ -90,7 +91,6 @@ __host__ __device__ ChordWs chord_ws(const DevPlan& P) {
   ChordWs w;
   int64_t o = 0;
   w.V = o; o = align256(o + (int64_t)CK * P.n_bus * 16);
-  w.F = o; o = align256(o + (int64_t)CK * P.dim * 8);
   w.y = o; o = align256(o + (int64_t)P.dim * sizeof(SlotVec<T>));
   w.S = o; o = align256(o + (int64_t)CK * CB_MAX * P.dim * sizeof(T));
   w.total = o;
@@ -245,11 +245,16 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
 
 // F and ||F||inf of the slots in `mask` (bit s: slot s): one sweep over the
 // Ybus rows, each entry read once for all slots.  Row edits are applied as
-// corrections on the buses of the edited Ybus rows (edits subtract ev[e]
-// from Y at entry ek[e]).
+// corrections on the buses of the edited Ybus rows (edit e subtracts ev[e]
+// from Y at the entry of row er[e], column ec[e]).  F goes straight into the
+// slots' lanes of the interleaved right-hand sides y (the chord solve's
+// input, in T); lanes of slots outside `mask` are kept only where `keep`
+// has their bit (others are not read before they are written again).
+template <typename T>
 __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, const unsigned mask,
-                                            const ChordSlot* sl, const int* s_ne, const int (*s_ek)[MAX_EDITS],
-                                            const double2 (*s_ev)[MAX_EDITS], const double2* Vs, double* Fs,
+                                            const unsigned keep, const ChordSlot* sl, const int* s_ne,
+                                            const int (*s_er)[MAX_EDITS], const int (*s_ec)[MAX_EDITS],
+                                            const double2 (*s_ev)[MAX_EDITS], const double2* Vs, SlotVec<T>* y,
                                             double* nrm_out, double* s_red_slots) {
   const int n = P.n_bus;
   const double2* Y = reinterpret_cast<const double2*>(a.ybus);
@@ -274,27 +279,32 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
       }
     }
     const int fp = P.fP[i], fq = P.fQ[i];
+    SlotVec<T> rp{}, rq{};
+    if (keep) {
+      if (fp >= 0) rp = y[fp];
+      if (fq >= 0) rq = y[fq];
+    }
 #pragma unroll
     for (int s = 0; s < CK; ++s) {
       if (!(mask >> s & 1)) continue;
       const double2* V = Vs + (int64_t)s * n;
       for (int e = 0; e < s_ne[s]; ++e) {
-        const int k = s_ek[s][e];
-        if (P.y_row[k] != i) continue;
-        const double2 vj = V[P.y_indices[k]];
+        if (s_er[s][e] != i) continue;
+        const double2 vj = V[s_ec[s][e]];
         acc[s] = csub(acc[s], cmul(s_ev[s][e], vj));
       }
       const double2 sv = csub(cmul(V[i], conj2(acc[s])), sb[s][i]);
-      double* F = Fs + (int64_t)s * P.dim;
       if (fp >= 0) {
-        F[fp] = -sv.x;
+        rp.v[s] = (T)(-sv.x);
         lmax[s] = (isnan(sv.x) || isnan(lmax[s])) ? NAN : fmax(lmax[s], fabs(sv.x));
       }
       if (fq >= 0) {
-        F[fq] = -sv.y;
+        rq.v[s] = (T)(-sv.y);
         lmax[s] = (isnan(sv.y) || isnan(lmax[s])) ? NAN : fmax(lmax[s], fabs(sv.y));
       }
     }
+    if (fp >= 0) y[fp] = rp;
+    if (fq >= 0) y[fq] = rq;
   }
   block_nanmax_slots(lmax, s_red_slots);
   if (threadIdx.x == 0)
@@ -428,6 +438,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   __shared__ int s_pull, s_more;
   __shared__ int s_ne[CK];
   __shared__ int s_ek[CK][MAX_EDITS];
+  __shared__ int s_er[CK][MAX_EDITS];  // Ybus row and column of each edit
+  __shared__ int s_ec[CK][MAX_EDITS];
   __shared__ double2 s_ev[CK][MAX_EDITS];
   __shared__ double s_red[NWARP];
   __shared__ double s_red_slots[NWARP * CK];
@@ -443,7 +455,6 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   const ChordWs L = chord_ws<T>(P);
   char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   double2* Vs = reinterpret_cast<double2*>(ws + L.V);
-  double* Fs = reinterpret_cast<double*>(ws + L.F);
   SlotVec<T>* y = reinterpret_cast<SlotVec<T>*>(ws + L.y);
   T* St = reinterpret_cast<T*>(ws + L.S);
   SlotVec<T>* ys = reinterpret_cast<SlotVec<T>*>(smem_raw);
@@ -490,7 +501,10 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
             const int e0 = a.edit_ptr[row], e1 = a.edit_ptr[row + 1];
             ne = min(e1 - e0, MAX_EDITS);
             for (int e = 0; e < ne; ++e) {
-              s_ek[s][e] = a.edit_k[e0 + e];
+              const int k = a.edit_k[e0 + e];
+              s_ek[s][e] = k;
+              s_er[s][e] = P.y_row[k];
+              s_ec[s][e] = P.y_indices[k];
               s_ev[s][e] = reinterpret_cast<const double2*>(a.edit_val)[e0 + e];
             }
           }
@@ -523,7 +537,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     if (active == 0) break;
 
     // ---- mismatch of every slot, start selection for new rows --------------
-    chord_mismatch(P, a, active, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red_slots);
+    chord_mismatch<T>(P, a, active, 0u, sl, s_ne, s_er, s_ec, s_ev, Vs, y, s_nrm, s_red_slots);
     for (int s = 0; s < CK; ++s) {
       if (!(active >> s & 1) || !sl[s].fresh) continue;
       const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
@@ -542,7 +556,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = va[i];
         if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
         __syncthreads();
-        chord_mismatch(P, a, 1u << s, sl, s_ne, s_ek, s_ev, Vs, Fs, s_nrm, s_red_slots);
+        chord_mismatch<T>(P, a, 1u << s, active & ~(1u << s), sl, s_ne, s_er, s_ec, s_ev, Vs, y, s_nrm,
+                          s_red_slots);
       }
     }
     prof.mark(PH_MISMATCH);
@@ -582,14 +597,8 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     }
     if (solve == 0) continue;
 
-    // ---- one solve on the base factor for every remaining slot -------------
-    for (int i = tid; i < P.dim; i += BS) {
-      SlotVec<T> r;
-#pragma unroll
-      for (int s = 0; s < CK; ++s) r.v[s] = (solve >> s & 1) ? (T)Fs[(int64_t)s * P.dim + i] : T(0);
-      y[i] = r;
-    }
-    __syncthreads();
+    // ---- one solve on the base factor for every remaining slot (F is in y;
+    // the lanes of slots that left are not read) ------------------------------
     chord_head_fw<T>(P, fwv, y);
     prof.mark(PH_SOLVE);
     chord_tail_fw<T>(P, fwv, y);
