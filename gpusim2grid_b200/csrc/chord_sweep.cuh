@@ -79,8 +79,9 @@ __device__ __forceinline__ void fms_slots(SlotVec<T>& acc, T a, const SlotVec<T>
   for (int s = 0; s < CK; ++s) acc.v[s] = fma(-a, b.v[s], acc.v[s]);
 }
 
-// Workspace of one chord CTA: V [n] per slot, the interleaved right-hand
-// sides y [dim] x CK (the mismatch writes F there), then the Broyden steps
+// Workspace of one chord CTA: the slots' voltages interleaved (V [n] x CK,
+// slot s of bus i at i * CK + s), the interleaved right-hand sides
+// y [dim] x CK (the mismatch writes F there), then the Broyden steps
 // [CK][CB_MAX][dim].
 struct ChordWs {
   int64_t V, y, S, total;
@@ -273,7 +274,7 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
 #pragma unroll
       for (int s = 0; s < CK; ++s) {
         if (!(mask >> s & 1)) continue;
-        const double2 vj = Vs[(int64_t)s * n + j];
+        const double2 vj = Vs[(int64_t)j * CK + s];
         acc[s].x = fma(yk.x, vj.x, fma(-yk.y, vj.y, acc[s].x));
         acc[s].y = fma(yk.x, vj.y, fma(yk.y, vj.x, acc[s].y));
       }
@@ -287,13 +288,12 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
 #pragma unroll
     for (int s = 0; s < CK; ++s) {
       if (!(mask >> s & 1)) continue;
-      const double2* V = Vs + (int64_t)s * n;
       for (int e = 0; e < s_ne[s]; ++e) {
         if (s_er[s][e] != i) continue;
-        const double2 vj = V[s_ec[s][e]];
+        const double2 vj = Vs[(int64_t)s_ec[s][e] * CK + s];
         acc[s] = csub(acc[s], cmul(s_ev[s][e], vj));
       }
-      const double2 sv = csub(cmul(V[i], conj2(acc[s])), sb[s][i]);
+      const double2 sv = csub(cmul(Vs[(int64_t)i * CK + s], conj2(acc[s])), sb[s][i]);
       if (fp >= 0) {
         rp.v[s] = (T)(-sv.x);
         lmax[s] = (isnan(sv.x) || isnan(lmax[s])) ? NAN : fmax(lmax[s], fabs(sv.x));
@@ -396,14 +396,16 @@ __device__ __noinline__ void chord_head_bw(const DevPlan P, const T* __restrict_
   }
 }
 
-// Outputs of a slot's row as it leaves: V, and either the final status
-// (flows included) or the hand-off to the single-row kernel.
+// Outputs of a slot's row as it leaves: V (the slot's lane of the
+// interleaved voltages, V[i * CK]), and either the final status (flows
+// included, from the row's output copy) or the hand-off to the single-row
+// kernel.
 __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, const double2* V, const int n,
                                          double* s_red) {
   const int tid = threadIdx.x;
   const int row = sl.row;
   double2* vout = reinterpret_cast<double2*>(a.v_out) + (int64_t)row * n;
-  for (int i = tid; i < n; i += BS) vout[i] = V[i];
+  for (int i = tid; i < n; i += BS) vout[i] = V[(int64_t)i * CK];
   if (tid == 0 && a.n_chord_steps != nullptr) atomicAdd(a.n_chord_steps, (unsigned long long)sl.it);
   if (sl.act == 5) {
     if (tid == 0) {
@@ -415,10 +417,13 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   }
   if (a.v_mirror != nullptr) {
     double2* vm = reinterpret_cast<double2*>(a.v_mirror) + (int64_t)row * n;
-    for (int i = tid; i < n; i += BS) vm[i] = V[i];
+    for (int i = tid; i < n; i += BS) vm[i] = V[(int64_t)i * CK];
   }
   const int status = sl.act == 2 ? ROW_CONVERGED : (sl.act == 3 ? ROW_DIVERGED : ROW_MAX_ITER);
-  if (a.loading_out != nullptr) row_flows(a, row, V, status == ROW_CONVERGED, s_red);
+  if (a.loading_out != nullptr) {
+    __syncthreads();  // the row's output copy is complete
+    row_flows(a, row, vout, status == ROW_CONVERGED, s_red);
+  }
   if (tid == 0) {
     a.res_out[row] = sl.nrm;
     a.status_out[row] = status;
@@ -521,7 +526,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
           sl[s].last = INFINITY;
         }
         const double2* v0 = reinterpret_cast<const double2*>(a.v0) + (int64_t)row * a.v0_stride;
-        for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = v0[i];
+        for (int i = tid; i < n; i += BS) Vs[(int64_t)i * CK + s] = v0[i];
         __syncthreads();
         const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
         bool c = false;
@@ -553,7 +558,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         if (sw) sl[s].from_base = a.alt_v0 == a.rescue_v0;
       }
       if (sw) {
-        for (int i = tid; i < n; i += BS) Vs[(int64_t)s * n + i] = va[i];
+        for (int i = tid; i < n; i += BS) Vs[(int64_t)i * CK + s] = va[i];
         if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
         __syncthreads();
         chord_mismatch<T>(P, a, 1u << s, active & ~(1u << s), sl, s_ne, s_er, s_ec, s_ev, Vs, y, s_nrm,
@@ -591,7 +596,7 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         solve |= 1u << s;
         continue;
       }
-      chord_leave(a, sl[s], Vs + (int64_t)s * n, n, s_red);
+      chord_leave(a, sl[s], Vs + s, n, s_red);
       if (tid == 0) sl[s].row = -1;
       __syncthreads();
     }
@@ -620,13 +625,13 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
 #pragma unroll
       for (int s = 0; s < CK; ++s) {
         if (!(solve >> s & 1)) continue;
-        double2* V = Vs + (int64_t)s * n;
-        const double2 v = V[i];
+        double2* V = Vs + (int64_t)i * CK + s;
+        const double2 v = *V;
         const double vm = hypot(v.x, v.y) + (fq >= 0 ? (double)ym.v[s] : 0.0);
         const double va = atan2(v.y, v.x) + (fp >= 0 ? (double)ya.v[s] : 0.0);
         double sn, cs;
         sincos(va, &sn, &cs);
-        V[i] = make_double2(vm * cs, vm * sn);
+        *V = make_double2(vm * cs, vm * sn);
       }
     }
     if (tid == 0)
