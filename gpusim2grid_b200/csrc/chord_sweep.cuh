@@ -433,6 +433,62 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   __syncthreads();
 }
 
+// Outage compensation of the slots in `comp`, all in one pass:
+// y_s <- y_s - Z_s B_s (I + W_s B_s)^-1 y_s[R_s] (see setup_compensation and
+// apply_compensation, the one-row form).  The small solves run in parallel,
+// one warp's leading thread per slot; then one sweep over the unknowns
+// applies every slot's columns of the base inverse.
+template <typename T>
+__device__ __noinline__ void chord_compensation(const int dim, const unsigned comp, SlotVec<T>* y, const T* Minv,
+                                                const int (*s_cr)[1 + MAX_COMP],
+                                                const double (*s_cB)[MAX_COMP * MAX_COMP],
+                                                const double (*s_cLU)[MAX_COMP * MAX_COMP],
+                                                const int (*s_cpiv)[MAX_COMP], double (*s_cw)[MAX_COMP]) {
+  const int tid = threadIdx.x;
+  const int s0 = tid >> 5;
+  if (s0 < CK && (tid & 31) == 0 && (comp >> s0 & 1)) {
+    const int s = s0;
+    const int r = s_cr[s][0];
+    const int* R = s_cr[s] + 1;
+    double v[MAX_COMP];
+    for (int q = 0; q < r; ++q) v[q] = (double)y[R[q]].v[s];
+    const double* C = s_cLU[s];
+    for (int k = 0; k < r; ++k) {  // P v, then L, then U
+      const int pk = s_cpiv[s][k];
+      if (pk != k) {
+        const double t = v[k];
+        v[k] = v[pk];
+        v[pk] = t;
+      }
+    }
+    for (int i2 = 1; i2 < r; ++i2)
+      for (int k = 0; k < i2; ++k) v[i2] -= C[i2 * r + k] * v[k];
+    for (int i2 = r - 1; i2 >= 0; --i2) {
+      for (int k = i2 + 1; k < r; ++k) v[i2] -= C[i2 * r + k] * v[k];
+      v[i2] /= C[i2 * r + i2];
+    }
+    for (int q = 0; q < r; ++q) {  // w = B v
+      double acc = 0.0;
+      for (int c = 0; c < r; ++c) acc += s_cB[s][q * r + c] * v[c];
+      s_cw[s][q] = acc;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < dim; i += BS) {
+    SlotVec<T> yi = y[i];
+#pragma unroll
+    for (int s = 0; s < CK; ++s) {
+      if (!(comp >> s & 1)) continue;
+      const int r = s_cr[s][0];
+      T acc = T(0);
+      for (int c = 0; c < r; ++c) acc += Minv[(int64_t)s_cr[s][1 + c] * dim + i] * (T)s_cw[s][c];
+      yi.v[s] -= acc;
+    }
+    y[i] = yi;
+  }
+  __syncthreads();
+}
+
 // The chord loop over the rows of one grid (queue a.queue, a.n_rows), until
 // that queue is exhausted and every slot has left.  Called by the
 // single-grid kernel once and by the multi-grid kernel once per grid.
@@ -611,8 +667,11 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     if (P.nt > 0) chord_dense<T>(P, Minv, y, ys);
     prof.mark(PH_SOLVE_DENSE);
     chord_head_bw<T>(P, fHV, bwv, y);
-    for (int s = 0; s < CK; ++s)
-      if ((solve >> s & 1) && sl[s].comp) apply_compensation<T>(P.dim, &y[0].v[s], Minv, shs(s), CK);
+    {
+      unsigned comp = 0;
+      for (int s = 0; s < CK; ++s) comp |= ((solve >> s & 1) && sl[s].comp ? 1u : 0u) << s;
+      if (comp) chord_compensation<T>(P.dim, comp, y, Minv, s_cr, s_cB, s_cLU, s_cpiv, s_cw);
+    }
     if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots);
     prof.mark(PH_SOLVE_BACK);
 
