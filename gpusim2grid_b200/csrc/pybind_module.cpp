@@ -229,6 +229,7 @@ class Session {
   void set_chord(int mode) { check(gs2g_session_set_chord(h(), mode)); }
   void set_handoff(int cluster) { check(gs2g_session_set_handoff(h(), cluster)); }
   void set_results_mirror(bool on) { check(gs2g_session_set_results_mirror(h(), on ? 1 : 0)); }
+  void set_row_order(bool on) { check(gs2g_session_set_row_order(h(), on ? 1 : 0)); }
   // adjoint: raw device pointers of rhs / lam [n_rows x dim_J] (caller-owned)
   void solve_jt(int n_rows, uintptr_t rhs, uintptr_t lam) {
     int rc;
@@ -606,6 +607,7 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("set_handoff", &Session::set_handoff, py::arg("cluster"))
       .def("set_results_mirror", &Session::set_results_mirror, py::arg("on"))
+      .def("set_row_order", &Session::set_row_order, py::arg("on"))
       .def("solve_jt", &Session::solve_jt, py::arg("n_rows"), py::arg("rhs"), py::arg("lam"))
       .def("set_handle_disconnected", &Session::set_handle_disconnected, py::arg("on"))
       .def("replan", &Session::replan, py::arg("tail_policy") = 1, py::arg("dense_rate") = 0.0,

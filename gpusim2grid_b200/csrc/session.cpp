@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -109,6 +110,12 @@ struct gs2g_session {
   int n_ctg = 0;
   std::vector<int> ctg_ptr, ctg_ids;
   int n_inj = 0;  // injection rows, already in d_sbus_rows (set_injections uploads them)
+  std::vector<double> inj_key;  // per injection row: sum |dP| + |dQ| against the base Sbus
+  // longest rows first: the queue takes rows by a difficulty estimate
+  // (gs2g_session_set_row_order); d_row_order is that permutation
+  int row_order = 1;
+  DevBuf d_row_order;
+  bool rows_have_order = false;
   int n_start = 0;
   DevBuf d_v0rows;
   bool rows_dirty = true;
@@ -358,6 +365,48 @@ bool trips_keep_connected(const gs2g_session* s, const std::vector<int>& ids) {
   return true;
 }
 
+// The order in which the row queue takes the rows: by a difficulty estimate,
+// largest first, so that rows needing many steps start early and the
+// persistent sweep does not end on a tail of a few long rows (a row's
+// results do not depend on when it runs).  Estimate: the row's distance
+// from the base injections (sum |dP| + |dQ|) plus, per tripped branch, its
+// flow at the base voltage (max |S_from|, |S_to|): both are the mismatch a
+// row starts with at the base case.  Off, or without any estimate, the
+// queue takes the rows in order.
+void order_rows(gs2g_session* s, int nr) {
+  s->rows_have_order = false;
+  if (!s->row_order || nr < 2) return;
+  std::vector<double> key(nr, 0.0);
+  bool any = false;
+  if (s->n_inj == nr && (int)s->inj_key.size() == nr) {
+    key = s->inj_key;
+    any = true;
+  }
+  if (s->n_ctg == nr && s->has_base && !s->yff.empty()) {
+    const int m = s->n_branch;
+    std::vector<double> fk(m, 0.0);
+    const double* V = s->base_v.data();
+    for (int l = 0; l < m; ++l) {
+      const int f = s->br_from[l], t = s->br_to[l];
+      const std::complex<double> vf = f >= 0 ? std::complex<double>(V[2 * f], V[2 * f + 1]) : 0.0;
+      const std::complex<double> vt = t >= 0 ? std::complex<double>(V[2 * t], V[2 * t + 1]) : 0.0;
+      auto c = [&](const std::vector<double>& y) { return std::complex<double>(y[2 * l], y[2 * l + 1]); };
+      const std::complex<double> i_f = c(s->yff) * vf + c(s->yft) * vt, i_t = c(s->ytf) * vf + c(s->ytt) * vt;
+      fk[l] = std::max(std::abs(vf * std::conj(i_f)), std::abs(vt * std::conj(i_t)));
+    }
+    for (int r = 0; r < nr; ++r)
+      for (int q = s->ctg_ptr[r]; q < s->ctg_ptr[r + 1]; ++q) key[r] += fk[s->ctg_ids[q]];
+    any = true;
+  }
+  if (!any) return;
+  std::vector<int> order(nr);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] > key[y]; });
+  s->d_row_order.ensure((size_t)nr * sizeof(int));
+  ck(cudaMemcpy(s->d_row_order.p, order.data(), (size_t)nr * sizeof(int), cudaMemcpyHostToDevice), "upload row order");
+  s->rows_have_order = true;
+}
+
 void assemble_rows(gs2g_session* s) {
   if (!s->rows_dirty) return;
   const int n = s->n_bus;
@@ -496,6 +545,7 @@ void assemble_rows(gs2g_session* s) {
       s->rows_have_skip = true;
     }
   }
+  order_rows(s, nr);
   s->rows_dirty = false;
 }
 
@@ -528,6 +578,7 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.row_skip = use_rows && s->rows_have_skip ? s->d_row_skip.as<int>() : nullptr;
   a.mask_ptr = use_rows && s->rows_have_mask ? s->d_mask_ptr.as<int>() : nullptr;
   a.mask_bus = use_rows && s->rows_have_mask ? s->d_mask_bus.as<int>() : nullptr;
+  a.row_map = use_rows && s->rows_have_order ? s->d_row_order.as<int>() : nullptr;
   a.max_iter = o.max_iter;
   a.tol = o.tol;
   a.fixed_iters = o.fixed_iters;
@@ -829,6 +880,15 @@ int gs2g_session_set_results_mirror(gs2g_session* s, int on) {
   if (on != 0 && on != 1) throw std::invalid_argument("session_set_results_mirror: on must be 0 or 1");
   s->mirror_on = on != 0;
   if (!s->mirror_on) s->mirror_valid = false;
+  GS2G_CATCH
+}
+
+int gs2g_session_set_row_order(gs2g_session* s, int on) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("session_set_row_order: NULL session");
+  if (on != 0 && on != 1) throw std::invalid_argument("session_set_row_order: on must be 0 or 1");
+  if (s->row_order != on) s->rows_dirty = true;
+  s->row_order = on;
   GS2G_CATCH
 }
 
@@ -1152,15 +1212,38 @@ int gs2g_set_injections(gs2g_session* s, int n_rows, const double* p_mw, const d
     // Sbus = (p + jq) / sn_mva, interleaved straight into pinned chunks that
     // are copied to the device while the next chunk is converted
     const double inv = 1.0 / sn_mva;
+    // each row's distance from the base injections, sum over buses of
+    // |dP| + |dQ| (the row-order key), accumulated in fixed point while the
+    // rows are converted
+    const size_t n = s->n_bus;
+    std::unique_ptr<std::atomic<int64_t>[]> keyfx(new std::atomic<int64_t>[n_rows]);
+    for (int r = 0; r < n_rows; ++r) keyfx[r].store(0, std::memory_order_relaxed);
+    const double* sb = s->sbus.data();
+    constexpr double kFix = 1e9;
     h2d_staged(s, s->d_sbus_rows.p, m * 2 * sizeof(double), [&](double* dst, size_t off, size_t len) {
       const size_t q0 = off / (2 * sizeof(double)), nq = len / (2 * sizeof(double));
       CopyPool::get().parallel_for(nq, size_t(1) << 16, [&](size_t b, size_t e) {
+        size_t row = (q0 + b) / n, bus = (q0 + b) % n;
+        double acc = 0.0;
         for (size_t q = b; q < e; ++q) {
-          dst[2 * q] = p_mw[q0 + q] * inv;
-          dst[2 * q + 1] = q_mvar[q0 + q] * inv;
+          const double pr = p_mw[q0 + q] * inv, qr = q_mvar[q0 + q] * inv;
+          dst[2 * q] = pr;
+          dst[2 * q + 1] = qr;
+          acc += std::fabs(pr - sb[2 * bus]) + std::fabs(qr - sb[2 * bus + 1]);
+          if (++bus == n) {
+            keyfx[row].fetch_add((int64_t)std::llround(std::min(acc, 1e9) * kFix), std::memory_order_relaxed);
+            acc = 0.0;
+            bus = 0;
+            ++row;
+          }
         }
+        if (bus != 0) keyfx[row].fetch_add((int64_t)std::llround(std::min(acc, 1e9) * kFix), std::memory_order_relaxed);
       });
     });
+    s->inj_key.resize(n_rows);
+    for (int r = 0; r < n_rows; ++r) s->inj_key[r] = (double)keyfx[r].load(std::memory_order_relaxed) / kFix;
+  } else {
+    s->inj_key.clear();
   }
   s->n_inj = n_rows;
   s->rows_dirty = true;

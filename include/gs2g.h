@@ -186,6 +186,14 @@ int gs2g_session_set_chord(gs2g_session* s, int mode);
  * dense tail is under 64 always use one CTA.  No counterpart in the
  * reference (its batch LU has no per-row kernel). */
 int gs2g_session_set_handoff(gs2g_session* s, int cluster);
+/* Order in which the persistent sweeps take the rows: on = 1 (default) by a
+ * difficulty estimate, largest first -- the row's distance from the base
+ * injections (sum over buses of |dP| + |dQ|, from gs2g_set_injections) plus
+ * the base-case flow of each branch it trips -- so that rows needing many
+ * steps start early and a sweep does not end on a tail of a few long rows;
+ * 0: in row order.  Results are written per row and do not depend on the
+ * order.  No counterpart in the reference (its rounds take rows in order). */
+int gs2g_session_set_row_order(gs2g_session* s, int on);
 /* handle_disconnected_grid (the reference's facade option,
  * src/gpusim2grid/contingency_analysis/gpu_facade.py:349, :544): on = 1
  * solves a row whose trips split the grid on its largest component -- the

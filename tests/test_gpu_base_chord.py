@@ -139,3 +139,35 @@ def test_fp64_subset_on_clusters_equals_one_cta(name):
         np.testing.assert_array_equal(out[0][k], out[1][k])
         np.testing.assert_array_equal(out[1][k], full[k][sub])
     assert np.all(out[1][1] == 0)
+
+
+@pytest.mark.parametrize("kind", ["n1", "scenario"])
+def test_row_order_leaves_results_unchanged(kind):
+    """The sweeps take the rows largest difficulty estimate first (distance
+    from the base injections, base flow of the tripped branches); a row's
+    results do not depend on when it runs, so they equal the in-order run
+    bit for bit, hand-offs, islanded rows and the FP64 fallback included."""
+    from gpusim2grid_b200.synthetic import grid_by_name, scenario_outages
+    g = grid_by_name("case2000_synth", 0)
+    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", tol=1e-8,
+              start="base", strategy="base_chord")
+    if kind == "n1":
+        sw = ContingencyAnalysisGPU(g.as_tuple(), **kw)
+        sw.set_branch_data(*g.branch_data())
+        bridges = np.setdiff1d(np.arange(g.n_branch), n1_branches(g))[:3]
+        sw.add_contingencies_by_branch_id([[int(b)] for b in n1_branches(g)] + [[int(b)] for b in bridges])
+    else:
+        n = 1024
+        p, q = injection_scenarios(g, n, seed=41)
+        sw = ScenarioSweepGPU(g.as_tuple(), **kw)
+        sw.set_branch_data(*g.branch_data())
+        sw.set_injections(1.2 * p, 1.2 * q, g.sn_mva)
+        sw.set_topology(scenario_outages(g, n, max_trips=2, seed=42))
+    out = []
+    for order in (0, 1):
+        sw.session.set_row_order(order)
+        sw.compute()
+        out.append((sw.V_results, sw.get_row_status(), sw.get_row_iterations(), sw.get_row_factorizations()))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+    assert out[0][3].sum() > 0
