@@ -1312,10 +1312,18 @@ __device__ __forceinline__ int ld_shared_rank0(const int* p) {
 // and all run the head LU (two barriers per level), their Schur rows
 // (barrier) and the dense LU together; after the row it posts
 // CLUSTER_CMD_DONE (barrier, read, barrier).
-constexpr int HANDOFF_CLUSTER = 8;
+// Largest cluster a row gets (16 needs the non-portable cluster-size opt-in;
+// the launch picks 16 or 8 by the number of rows, see launch_sweep_cluster).
+constexpr int HANDOFF_CLUSTER = 16;
+
+__device__ __forceinline__ unsigned cluster_nctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
 
 template <typename T>
-__global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
+__global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
     sweep_kernel_cluster(const DevPlan P, const SweepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_row;
@@ -1333,9 +1341,10 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
   const RowShared<T> sh{&s_ne, s_ek, s_ev, s_red, s_blk, reinterpret_cast<T*>(smem_raw), s_cr, s_cB, s_cLU, s_cpiv,
                         s_cw};
   const int rank = (int)cluster_ctarank();
+  const int parts = (int)cluster_nctarank();  // the launch's cluster size
   const int n_rows = a.n_rows_dev != nullptr ? *a.n_rows_dev : a.n_rows;
   PhaseProf prof;
-  if ((int64_t)n_rows * HANDOFF_CLUSTER > gridDim.x) {
+  if ((int64_t)n_rows * parts > gridDim.x) {
     // more rows than clusters: sharing the LUs would leave rows waiting for a
     // cluster, so every CTA runs rows of its own, as sweep_kernel does (the
     // choice is the same for the whole grid: no cluster barrier is used)
@@ -1357,7 +1366,7 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
   T* S = reinterpret_cast<T*>(ws + ws_layout<T>(P).S);
   T* HV = reinterpret_cast<T*>(ws + ws_layout<T>(P).HV);
   prof.init(a.phase_cycles != nullptr && threadIdx.x == 0 && rank == 0);
-  const ClusterLu cl{&s_cmd, HANDOFF_CLUSTER};
+  const ClusterLu cl{&s_cmd, parts};
   for (;;) {
     if (rank == 0 && threadIdx.x == 0) s_row = atomicAdd(a.queue, 1);
     dense::cluster_barrier();
@@ -1378,10 +1387,10 @@ __global__ void __cluster_dims__(HANDOFF_CLUSTER, 1, 1) __launch_bounds__(BS, GS
         // the leader's Jacobian values are in place (posted after them): the
         // head LU's share of each level, the Schur rows, a barrier, then the
         // shared dense LU
-        head_lu<T>(P, HV, a.pivot_floor, rank, HANDOFF_CLUSTER);
-        schur_update<T>(P, HV, S, rank, HANDOFF_CLUSTER);
+        head_lu<T>(P, HV, a.pivot_floor, rank, parts);
+        schur_update<T>(P, HV, S, rank, parts);
         dense::cluster_barrier();
-        dense_lu_cluster<T>(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, HANDOFF_CLUSTER);
+        dense_lu_cluster<T>(S, P.nt, P.ld, reinterpret_cast<T*>(smem_raw), a.pivot_floor, rank, parts);
       }
     }
   }
@@ -1480,6 +1489,10 @@ cudaError_t opt_in_smem() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(sweep_kernel_cluster<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem_bytes<double>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_kernel_cluster<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_kernel_cluster<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_kernel_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               smem_bytes<double>());
@@ -1587,16 +1600,30 @@ int launch_adjoint(const DevPlan& P, const SweepArgs& a, const double* rhs, doub
 
 int handoff_cluster_size() { return HANDOFF_CLUSTER; }
 
-int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {
+int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int prec, int cluster, int n_ctas, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (n_ctas <= 0 || n_ctas % HANDOFF_CLUSTER != 0 || a.inverse_out != nullptr || a.factor_only)
+  if ((cluster != 8 && cluster != 16) || n_ctas <= 0 || n_ctas % cluster != 0 || a.inverse_out != nullptr ||
+      a.factor_only)
     return (int)cudaErrorInvalidValue;
-  const cudaError_t e = opt_in_smem();
+  cudaError_t e = opt_in_smem();
   if (e != cudaSuccess) return (int)e;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)n_ctas, 1, 1);
+  cfg.blockDim = dim3(BS, 1, 1);
+  cfg.dynamicSmemBytes = prec == 1 ? smem_bytes<float>() : smem_bytes<double>();
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   if (prec == 1)
-    sweep_kernel_cluster<float><<<n_ctas, BS, smem_bytes<float>(), st>>>(P, a);
+    e = cudaLaunchKernelEx(&cfg, sweep_kernel_cluster<float>, P, a);
   else
-    sweep_kernel_cluster<double><<<n_ctas, BS, smem_bytes<double>(), st>>>(P, a);
+    e = cudaLaunchKernelEx(&cfg, sweep_kernel_cluster<double>, P, a);
+  if (e != cudaSuccess) return (int)e;
   return (int)cudaGetLastError();
 }
 

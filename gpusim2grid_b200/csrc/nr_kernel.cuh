@@ -194,10 +194,10 @@ int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
 int sweep_ctas(int prec, int device);
 
 // The single-row sweep (prec 1: FP32 factors, 0: FP64) with a cluster of
-// handoff_cluster_size() CTAs per row: the cluster's leading CTA runs the
-// row (its workspace: the leader's block index times ws_stride), and all of
-// them share each of its Schur updates and dense tail LUs.  n_ctas a
-// multiple of the cluster size.
+// `cluster` CTAs per row (8, or 16 up to handoff_cluster_size()): the
+// cluster's leading CTA runs the row (its workspace: the leader's block
+// index times ws_stride), and all of them share each of its head LUs, Schur
+// updates and dense tail LUs.  n_ctas a multiple of the cluster size.
 int handoff_cluster_size();
 
 // Batched adjoint (FP64): lam[r] = J_r^-T rhs[r] for the a.n_rows rows of a
@@ -207,7 +207,7 @@ int handoff_cluster_size();
 // J layout.  Workspace a.workspace / a.ws_stride (double layout), queue
 // zeroed by the caller.
 int launch_adjoint(const DevPlan& P, const SweepArgs& a, const double* rhs, double* lam, int n_ctas, void* stream);
-int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream);
+int launch_sweep_cluster(const DevPlan& P, const SweepArgs& a, int prec, int cluster, int n_ctas, void* stream);
 
 // Several grids in one persistent launch (see sweep_kernel_multi): the plan
 // and the per-grid launch arguments of each grid (SweepArgs fields n_rows,

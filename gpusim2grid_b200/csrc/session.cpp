@@ -638,6 +638,15 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   return a;
 }
 
+// Cluster size for `rows` rows that each get a cluster within `n_ctas`
+// CTAs: 16, else 8, else 0 (one CTA per row).
+int cluster_for(int rows, int n_ctas) {
+  if (rows <= 0) return 0;
+  for (int c = gs2g::handoff_cluster_size(); c >= 8; c /= 2)
+    if ((int64_t)rows * c <= n_ctas) return c;
+  return 0;
+}
+
 float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* v0, int64_t v0_stride,
              const double* sbus, int64_t sbus_stride, bool use_rows, const OutBufs& out, int n_ctas_req) {
   gs2g::SweepArgs a = make_args(s, o, n_rows, v0, v0_stride, sbus, sbus_stride, use_rows, out);
@@ -674,6 +683,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
   s->d_chord_steps.ensure(sizeof(unsigned long long));
   ck(cudaMemsetAsync(s->d_chord_steps.p, 0, sizeof(unsigned long long), s->stream), "step count reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
+  int n_next = n_rows;  // rows of the single-row launch (the hand-offs after a chord sweep)
   if (chord) {
     gs2g::SweepArgs c = a;
     c.ws_stride = cwsb;
@@ -683,6 +693,10 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     c.broyden = s->chord == 2;
     ck((cudaError_t)gs2g::launch_chord(s->dplan, c, o.precision, n_chord, s->stream), "chord sweep launch");
     ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
+    // how many rows were handed off decides the next launch's shape
+    ck(cudaMemcpyAsync(&n_next, s->d_queue.as<int>() + 3, sizeof(int), cudaMemcpyDeviceToHost, s->stream),
+       "hand-off count");
+    ck(cudaStreamSynchronize(s->stream), "chord sweep");
     // the hand-offs continue from where the chord sweep left them: their V
     // (v_out) and step count (iters_out), on their own factor (policy 1)
     a.row_map = s->d_handoff.as<int>();
@@ -699,17 +713,17 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.alt_v0 = nullptr;
     a.alt_s = nullptr;
   }
-  // hand-offs with a dense tail worth sharing: a cluster of CTAs per row
-  // (the rows are few and each of their factorizations would otherwise run
-  // on one SM after every other row has finished)
-  const int csize = gs2g::handoff_cluster_size();
-  const bool cluster = chord && s->handoff_cluster && s->dplan.nt >= 64 && n_ctas >= csize;
-  if (n_rows > 0 && cluster) {
-    const int n_cl = std::max(1, std::min(n_ctas / csize, n_rows));
-    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, n_cl * csize, s->stream),
+  // hand-offs with a dense tail worth sharing: a cluster of 16 (or 8) CTAs
+  // per row when every row gets one (the rows are few and each of their
+  // factorizations would otherwise run on one SM after every other row has
+  // finished)
+  const int csize = chord && s->handoff_cluster && s->dplan.nt >= 64 ? cluster_for(n_next, n_ctas) : 0;
+  if (n_next > 0 && csize > 0) {
+    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, csize, n_next * csize, s->stream),
        "hand-off cluster launch");
-  } else if (n_rows > 0) {
-    ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "sweep launch");
+  } else if (n_next > 0) {
+    ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, std::min(n_ctas, n_next), s->stream),
+       "sweep launch");
   }
   ck(cudaEventRecord(s->ev1, s->stream), "event");
   ck(cudaStreamSynchronize(s->stream), "sweep");
@@ -1557,8 +1571,8 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   int n_ctas = o.n_ctas > 0 ? o.n_ctas : gs2g::sweep_ctas(o.precision, s->device);
   // few rows with a dense tail worth sharing (an FP64 re-solve of the rows
   // a mixed sweep did not converge): a cluster of CTAs per row
-  const int csize = gs2g::handoff_cluster_size();
-  const bool cluster = s->handoff_cluster && s->dplan.nt >= 64 && n_sub > 0 && (int64_t)n_sub * csize <= n_ctas;
+  const int csize = s->handoff_cluster && s->dplan.nt >= 64 ? cluster_for(n_sub, n_ctas) : 0;
+  const bool cluster = n_sub > 0 && csize > 0;
   n_ctas = cluster ? n_sub * csize : std::max(1, std::min(n_ctas, std::max(n_sub, 1)));
   const int64_t wsb = gs2g::workspace_bytes(s->dplan, o.precision);
   s->d_ws.ensure((size_t)wsb * n_ctas);
@@ -1575,7 +1589,8 @@ int gs2g_run_subset(gs2g_session* s, const gs2g_run_opts* o_, int n_sub, const i
   ck(cudaMemsetAsync(s->d_queue.p, 0, 3 * sizeof(int), s->stream), "queue reset");
   ck(cudaEventRecord(s->ev0, s->stream), "event");
   if (n_sub > 0 && cluster)
-    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, n_ctas, s->stream), "subset cluster launch");
+    ck((cudaError_t)gs2g::launch_sweep_cluster(s->dplan, a, o.precision, csize, n_ctas, s->stream),
+       "subset cluster launch");
   else if (n_sub > 0)
     ck((cudaError_t)gs2g::launch_sweep(s->dplan, a, o.precision, n_ctas, s->stream), "subset launch");
   ck(cudaEventRecord(s->ev1, s->stream), "event");

@@ -180,11 +180,12 @@ int gs2g_session_set_chord(gs2g_session* s, int mode);
  * and the rows of a gs2g_run_subset when there are few of them (at most one
  * per 8 CTAs of a full launch: the FP64 re-solve of the rows a mixed sweep
  * did not converge): cluster = 1 (default) runs each such row on a cluster
- * of 8 CTAs, the leading CTA running the row and all 8 sharing each of its
- * Schur updates and dense tail LUs (bit-identical to the one-CTA
- * factorization, FP32 and FP64); 0 runs each on one CTA.  Grids whose
- * dense tail is under 64 always use one CTA.  No counterpart in the
- * reference (its batch LU has no per-row kernel). */
+ * of 16 CTAs (8 when 16 per row do not fit in one launch), the leading CTA
+ * running the row and all of them sharing each of its head LUs, Schur
+ * updates and dense tail LUs (bit-identical to the one-CTA factorization,
+ * FP32 and FP64); 0 runs each on one CTA.  Grids whose dense tail is under
+ * 64 always use one CTA.  No counterpart in the reference (its batch LU has
+ * no per-row kernel). */
 int gs2g_session_set_handoff(gs2g_session* s, int cluster);
 /* Order in which the persistent sweeps take the rows: on = 1 (default) by a
  * difficulty estimate, largest first -- the row's distance from the base
