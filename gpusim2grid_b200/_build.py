@@ -30,7 +30,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["nr_kernel.cu", "mlp_kernels.cu"]
 CPP_SOURCES = ["plan.cpp", "session.cpp"]
-HEADERS = ["nr_kernel.cuh", "chord_sweep.cuh", "adjoint.cuh", "plan.hpp", "dense_lu.cuh", "dense_lu_f32.cuh"]
+HEADERS = ["nr_kernel.cuh", "chord_sweep.cuh", "adjoint.cuh", "plan.hpp", "dense_lu.cuh", "dense_lu_f32.cuh",
+           "dense_lu_f64.cuh"]
 
 
 def _stale(target: Path, deps) -> bool:

@@ -25,6 +25,7 @@
 
 #include "dense_lu.cuh"
 #include "dense_lu_f32.cuh"
+#include "dense_lu_f64.cuh"
 
 #include <cmath>
 #include <cstdint>
@@ -196,12 +197,19 @@ __device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__
   }
 }
 
-// Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on the
-// DMMA tiles of dense_lu.cuh; both use the dynamic shared memory as scratch.
+// Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on its
+// FP64 counterpart (dense_lu_f64.cuh; GS2G_FP64_LU=0 selects the older
+// DMMA-tile LU of dense_lu.cuh); all use the dynamic shared memory as
+// scratch.
+#ifndef GS2G_FP64_LU
+#define GS2G_FP64_LU 1
+#endif
 template <typename T>
 __device__ __forceinline__ void dense_lu(T* S, int n, int ld, T* smem, double pfloor) {
   if constexpr (sizeof(T) == 4)
     gs2g::dense32::lu(S, n, ld, smem, pfloor);
+  else if constexpr (GS2G_FP64_LU == 1)
+    gs2g::dense64::lu(S, n, ld, smem, pfloor);
   else
     dense::lu<T>(S, n, ld, smem, pfloor);
 }
@@ -211,9 +219,12 @@ template <typename T>
 __device__ __forceinline__ void dense_lu_cluster(T* S, int n, int ld, T* smem, double pfloor, int part, int parts) {
   if constexpr (sizeof(T) == 4)
     gs2g::dense32::lu_cluster(S, n, ld, smem, pfloor, part, parts);
+  else if constexpr (GS2G_FP64_LU == 1)
+    gs2g::dense64::lu_cluster(S, n, ld, smem, pfloor, part, parts);
   else
     dense::lu_cluster(S, n, ld, smem, pfloor, part, parts);
 }
+static_assert(gs2g::dense64::Smem::elems <= dense::Smem<double>::elems, "FP64 LU scratch within the FP64 smem");
 template <typename T>
 __host__ __device__ constexpr int dense_smem_elems() {
   return sizeof(T) == 4 ? gs2g::dense32::Smem::elems : dense::Smem<T>::elems;
@@ -1450,7 +1461,10 @@ __global__ void __launch_bounds__(BS, GS2G_MIN_CTAS_PER_SM)
       cur = g;
     }
     const int lr = row - row_begin[g];
-    solve_row<T>(s_grid.P, s_grid.a, (s_grid.a.row_map != nullptr ? s_grid.a.row_map[lr] : lr) | flag, ws, sh, prof);
+    // a queue position goes through the grid's row order; a hand-off entry
+    // is already the grid's row
+    const int srow = row_list == nullptr && s_grid.a.row_map != nullptr ? s_grid.a.row_map[lr] : lr;
+    solve_row<T>(s_grid.P, s_grid.a, srow | flag, ws, sh, prof);
   }
 }
 

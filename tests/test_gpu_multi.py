@@ -64,3 +64,28 @@ def test_multi_grid_rejects_mismatched_options():
     b, _, _ = _sweep(g, 8, "fp64", 2)
     with pytest.raises(ValueError):
         compute_many([a, b])
+
+
+def test_multi_grid_row_order_leaves_results_unchanged():
+    """The rows of every grid are taken largest difficulty estimate first in
+    the multi-grid launch too; hand-offs (session rows) are not re-mapped.
+    Results equal the in-order launch bit for bit."""
+    from gpusim2grid_b200 import compute_many
+    out = []
+    for order in (0, 1):
+        sweeps = []
+        for name, n, seed in (("case118_synth", 48, 3), ("case2000_synth", 40, 5)):
+            g = grid_by_name(name, 0)
+            p, q = injection_scenarios(g, n, seed=seed)
+            sw = ScenarioSweepGPU(g.as_tuple(), init_from_n_powerflow=False, precision="mixed", nb_iter=10,
+                                  scheduling="continuous", tol=1e-8, start="base", strategy="base_chord")
+            sw.set_branch_data(*g.branch_data())
+            sw.set_injections(1.2 * p, 1.2 * q, g.sn_mva)
+            sw.set_topology(scenario_outages(g, n, max_trips=2, seed=seed + 1))
+            sw.session.set_row_order(order)
+            sweeps.append(sw)
+        compute_many(sweeps)
+        out.append([(sw.V_results, sw.get_row_status(), sw.get_row_iterations()) for sw in sweeps])
+    for a, b in zip(*out):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
