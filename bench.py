@@ -63,6 +63,7 @@ WORKLOADS = {
                                                     "multi", 2048, 3, dict(broad=1.0, p_outage=0.9)),
 }
 MAX_ITER, TOL = 10, 1e-8
+LOAD_SCALE = 1.0  # --load-scale: heavier (or lighter) loading of every grid
 METRIC = "Converged AC PF solves/s on 1 B200: learned+mixed vs plain FP64 NR @1e-8 pu"
 
 def _args():
@@ -91,6 +92,9 @@ def _args():
                          "(0: leave it out)")
     ap.add_argument("--cfg2-train-rows", type=int, default=20000)
     ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--load-scale", type=float, default=1.0,
+                    help="multiply every grid's loads (and the generation following them): the strategy under "
+                         "heavier loading (1.0: the configs' grids)")
     ap.add_argument("--hidden", type=int, default=1024)
     ap.add_argument("--tune-rates", type=float, nargs="*", default=[40.0, 160.0, 320.0],
                     help="dense/scatter cost ratios the plan autotuner tries (none: keep the default plan)")
@@ -138,7 +142,14 @@ def _workload(name):
     """(grid, trips or None, p_mw or None, q_mvar or None) of a named workload;
     for the heterogeneous workload, a list of such tuples (one per grid)."""
     syn = _synthetic()
-    grid_by_name, injection_scenarios = syn.grid_by_name, syn.injection_scenarios
+    injection_scenarios = syn.injection_scenarios
+
+    def grid_by_name(name, seed):
+        # the configs' grid, its loads (and the generation following them)
+        # times --load-scale
+        n_bus, n_branch, n_pv, n_load, n_trafo, scale = syn.GRID_SPECS[name]
+        return syn.make_grid(n_bus, n_branch, n_pv, n_load, n_trafo, seed=seed, name=name,
+                             load_scale=scale * LOAD_SCALE)
     n1_branches, scenario_outages = syn.n1_branches, syn.scenario_outages
     gname, kind, n_rows, seed, _ = WORKLOADS[name]
     if kind == "multi":
@@ -596,7 +607,8 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": workload, "grid": gname, "rows": n, "start": args.start,
                    "precision": args.precision, "strategy": _strategy(args, trips), "tol_pu": TOL, "max_iter": MAX_ITER,
-                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}",
+                   "load_scale": LOAD_SCALE},
         "rows_converged": n_conv, "rows_rescued": n_rescued, "rows_fp64_fallback": fallback_rows,
         "newton_iters_total": total_iters,
         "lu_factorizations_total": total_factors, "mean_iters": round(total_iters / max(n, 1), 3),
@@ -1034,6 +1046,7 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = _args()
+    LOAD_SCALE = float(a.load_scale)
     if a.impl == "reference":
         run_reference(a)
     elif WORKLOADS[a.workload][1] == "single":
