@@ -320,6 +320,19 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+AGREE_PU = 1e-6  # the metric's agreement bar with the FP64 flat-start answer
+
+
+def _counted(V, st, V64, st64):
+    """Rows that count for the metric: converged here and in plain FP64 NR
+    from flat, to the same solution (max |dV| <= AGREE_PU)."""
+    ok = (np.asarray(st) == 0) & (np.asarray(st64) == 0)
+    if not ok.any():
+        return 0
+    dv = np.abs(np.asarray(V)[ok] - np.asarray(V64)[ok]).max(axis=1)
+    return int((dv <= AGREE_PU).sum())
+
+
 def algorithmic_bytes(info, w):
     """Minimum bytes (shared structure amortised to zero) of one LU
     factorization of one row (J write and read, factor write) and of one
@@ -504,6 +517,10 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
     ok = (st == 0) & (st64 == 0)
     agree = float(np.abs(V_w[ok] - V64[ok]).max()) if ok.any() else None
     same_flags = bool(np.array_equal(st == 0, st64 == 0))
+    # the metric counts a row when it converged here and in plain FP64 from
+    # flat, to the same solution (|dV| <= 1e-6 pu)
+    n_counted = _counted(V_w, st, V64, st64)
+    value = world * n_counted * steps / (total_ms / 1e3)
     mixed_flat_value = base_start = None
     if learned and args.precision == "mixed":
         # mixed precision from flat (separates the strategy from the start)
@@ -522,8 +539,8 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
                 flush.fill_(1.0)
                 torch.cuda.synchronize()
                 ms_b.append(base_step())
-            _, _, stb, itb = s.results()
-            bv = int((stb == 0).sum()) / (np.mean(ms_b) / 1e3)
+            Vb_, _, stb, itb = s.results()
+            bv = _counted(Vb_, stb, V64, st64) / (np.mean(ms_b) / 1e3)
             base_start = {"value": round(bv, 1), "newton_iters_total": int(itb.sum()),
                           "rows_converged": int((stb == 0).sum()), "rows_fp64_fallback": ca.fallback_rows,
                           "learned_over_base_start": round(value / world / bv, 3),
@@ -568,7 +585,7 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
             e2e_s.append(t3 - t0)
             e2e_parts.append((t1 - t0, t2 - t1, t3 - t2, ca.timings.t_kernel_ms / 1e3))
         gc.unfreeze()
-        e2e_value = world * int((stt == 0).sum()) / float(np.mean(e2e_s))
+        e2e_value = world * _counted(V, stt, V64, st64) / float(np.mean(e2e_s))
         e2e_split = dict(zip(["rows_in_ms", "compute_ms", "results_out_ms", "kernel_ms"],
                              [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
         n_ids = sum(len(r_) for r_ in trips) if trips is not None else 0
@@ -609,7 +626,8 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
                    "precision": args.precision, "strategy": _strategy(args, trips), "tol_pu": TOL, "max_iter": MAX_ITER,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}",
                    "load_scale": LOAD_SCALE},
-        "rows_converged": n_conv, "rows_rescued": n_rescued, "rows_fp64_fallback": fallback_rows,
+        "rows_converged": n_conv, "rows_counted": n_counted, "rows_rescued": n_rescued,
+        "rows_fp64_fallback": fallback_rows,
         "newton_iters_total": total_iters,
         "lu_factorizations_total": total_factors, "mean_iters": round(total_iters / max(n, 1), 3),
         "iters_hist": iters_hist,
@@ -647,7 +665,7 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
 # the driver-visible second configuration of the default line: the 6500-bus
 # injection sweep (the north star's ">= 3x" names it beside the N-1 sweep)
 CFG2 = "injection_sweep_case6500_synth"
-CFG2_KEYS = ("value", "ms_per_step", "rows_converged", "newton_iters_total", "lu_factorizations_total",
+CFG2_KEYS = ("value", "ms_per_step", "rows_converged", "rows_counted", "newton_iters_total", "lu_factorizations_total",
              "rows_fp64_fallback", "ms_split", "fp64_flat_value", "speedup_vs_fp64_flat", "mixed_flat_value",
              "base_start_value", "agreement_with_fp64", "training", "setup", "plan", "roofline", "clocks")
 
@@ -812,6 +830,10 @@ def run_ours_multi(args):
         return sum(int((x[2] == 0).sum()) for x in r_) / (np.mean(ms_) / 1e3), r_
 
     fp64_value, res64 = flat_arm(lib.PREC_FP64, lib.REFACTOR_EVERY)
+    # the metric counts a row when it converged here and in plain FP64 from
+    # flat, to the same solution
+    n_counted = sum(_counted(r[0], r[2], r64[0], r64[2]) for r, r64 in zip(res, res64))
+    value = world * n_counted * args.steps / (total_ms / 1e3)
     agree, same, mism = 0.0, True, {}
     for (g, _, _, _), r, r64 in zip(parts, res, res64):
         ok = (r[2] == 0) & (r64[2] == 0)
@@ -849,7 +871,7 @@ def run_ours_multi(args):
     gc.unfreeze()
     e2e_split = dict(zip(["rows_in_ms", "compute_ms", "results_out_ms", "kernel_ms"],
                          [round(float(x) * 1e3, 2) for x in np.mean(np.array(e2e_parts), axis=0)]))
-    n_conv_e2e = sum(int((o[1] == 0).sum()) for o in outs)
+    n_conv_e2e = sum(_counted(o[0], o[1], r64[0], r64[2]) for o, r64 in zip(outs, res64))
     e2e_value = world * n_conv_e2e / float(np.mean(e2e_s))
     h2d = sum(2 * p.nbytes + 4 * (len(t) + 1) + 4 * sum(len(x) for x in t) for _, t, p, _ in parts)
     d2h = sum(o[0].nbytes + o[1].nbytes + o[2].nbytes for o in outs)
@@ -869,7 +891,8 @@ def run_ours_multi(args):
                    "rows_per_grid": n_rows, "start": args.start, "precision": args.precision,
                    "strategy": args.strategy, "tol_pu": TOL, "max_iter": MAX_ITER, "launch": "one persistent launch",
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
-        "rows_converged": n_conv, "rows_fp64_fallback": fallback_rows, "mean_iters": round(float(iters.mean()), 3),
+        "rows_converged": n_conv, "rows_counted": n_counted, "rows_fp64_fallback": fallback_rows,
+        "mean_iters": round(float(iters.mean()), 3),
         "iters_hist": {int(k): int(v) for k, v in zip(*np.unique(iters, return_counts=True))},
         "ms_split": {"features_mlp_v0": round(float(np.mean(pre)), 4), "sweep_kernel": round(float(np.mean(ker)), 4)},
         "fp64_flat_value": round(fp64_value, 1),
