@@ -492,7 +492,7 @@ __device__ __noinline__ void chord_compensation(const int dim, const unsigned co
 // The chord loop over the rows of one grid (queue a.queue, a.n_rows), until
 // that queue is exhausted and every slot has left.  Called by the
 // single-grid kernel once and by the multi-grid kernel once per grid.
-template <typename T>
+template <typename T, bool Y_SMEM = false>
 __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a, PhaseProf& prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChordSlot sl[CK];
@@ -516,9 +516,11 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
   const ChordWs L = chord_ws<T>(P);
   char* ws = a.workspace + (int64_t)blockIdx.x * a.ws_stride;
   double2* Vs = reinterpret_cast<double2*>(ws + L.V);
-  SlotVec<T>* y = reinterpret_cast<SlotVec<T>*>(ws + L.y);
-  T* St = reinterpret_cast<T*>(ws + L.S);
   SlotVec<T>* ys = reinterpret_cast<SlotVec<T>*>(smem_raw);
+  // the right-hand sides in the workspace, or (Y_SMEM) in shared memory
+  // after the tail copy ys
+  SlotVec<T>* y = Y_SMEM ? ys + (P.nt > 0 ? P.nt : 1) : reinterpret_cast<SlotVec<T>*>(ws + L.y);
+  T* St = reinterpret_cast<T*>(ws + L.S);
   const WsLayout BL = ws_layout<T>(P);  // layout of the base factor's workspace
   const T* fHV = reinterpret_cast<const T*>(a.base_ws + BL.HV);
   const T* fwv = reinterpret_cast<const T*>(a.base_fwv);
@@ -713,6 +715,17 @@ __global__ void __launch_bounds__(BS, GS2G_CHORD_CTAS_PER_SM) chord_kernel(const
   prof.flush(a.phase_cycles);
 }
 
+// The same chord sweep with the right-hand sides in shared memory (for grids
+// whose dim x 4 values fit beside the tail copy): every solve's gathers are
+// shared-memory loads, at 2 CTAs per SM instead of 3.
+template <typename T>
+__global__ void __launch_bounds__(BS, 2) chord_kernel_ysmem(const DevPlan P, const SweepArgs a) {
+  PhaseProf prof;
+  prof.init(a.phase_cycles != nullptr && threadIdx.x == 0);
+  chord_body<T, true>(P, a, prof);
+  prof.flush(a.phase_cycles);
+}
+
 // Multi-grid chord sweep: a CTA binds its slots to one grid at a time (the
 // slots share that grid's base factor), draining the grids' own queues in
 // cyclic order from grid blockIdx.x % n_grids, so the CTAs spread over the
@@ -739,4 +752,20 @@ __global__ void __launch_bounds__(BS, GS2G_CHORD_CTAS_PER_SM)
 template <typename T>
 int chord_smem_bytes(const DevPlan& P) {
   return (int)(sizeof(SlotVec<T>) * (size_t)(P.nt > 0 ? P.nt : 1));
+}
+// dynamic shared memory of chord_kernel_ysmem: the tail copy, then y
+template <typename T>
+int chord_smem_bytes_ysmem(const DevPlan& P) {
+  return chord_smem_bytes<T>(P) + (int)(sizeof(SlotVec<T>) * (size_t)P.dim);
+}
+// Right-hand sides in shared memory when they fit in this budget, which
+// leaves room for 2 CTAs per SM (build-time; 0 keeps them in the workspace).
+// Measured on the 2000-bus grid (67 KB): N-1 sweep -3 %, injection sweep
+// -10 %, bit-identical.
+#ifndef GS2G_CHORD_YSMEM_BYTES
+#define GS2G_CHORD_YSMEM_BYTES (84 * 1024)
+#endif
+template <typename T>
+bool chord_use_ysmem(const DevPlan& P) {
+  return sizeof(T) == 4 && chord_smem_bytes_ysmem<T>(P) <= GS2G_CHORD_YSMEM_BYTES;
 }

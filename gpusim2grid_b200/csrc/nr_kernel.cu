@@ -1559,7 +1559,12 @@ int chord_ctas(const DevPlan& P, int prec, int device) {
   int n_sm = 0;
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
   int per_sm = 0;
-  if (prec == 1) {
+  if (prec == 1 && chord_use_ysmem<float>(P)) {
+    cudaFuncSetAttribute(chord_kernel_ysmem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         chord_smem_bytes_ysmem<float>(P));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chord_kernel_ysmem<float>, BS,
+                                                  chord_smem_bytes_ysmem<float>(P));
+  } else if (prec == 1) {
     chord_opt_in<float>(P);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chord_kernel<float>, BS, chord_smem_bytes<float>(P));
   } else {
@@ -1575,6 +1580,13 @@ int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, voi
   if (n_ctas <= 0 || a.base_ws == nullptr || a.base_inv == nullptr || a.base_fwv == nullptr ||
       a.base_bwv == nullptr || a.handoff == nullptr || a.n_handoff == nullptr || a.fixed_iters)
     return (int)cudaErrorInvalidValue;
+  if (prec == 1 && chord_use_ysmem<float>(P)) {
+    const int sm = chord_smem_bytes_ysmem<float>(P);
+    cudaError_t e = cudaFuncSetAttribute(chord_kernel_ysmem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return (int)e;
+    chord_kernel_ysmem<float><<<n_ctas, BS, sm, st>>>(P, a);
+    return (int)cudaGetLastError();
+  }
   cudaError_t e = prec == 1 ? chord_opt_in<float>(P) : chord_opt_in<double>(P);
   if (e != cudaSuccess) return (int)e;
   if (prec == 1)
