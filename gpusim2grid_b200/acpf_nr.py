@@ -35,15 +35,25 @@ class AcPfGPU:
         Trust ``Vinit`` as already solved: validate ``||F(Vinit)||inf < tol``
         once (``RuntimeError`` otherwise) and skip the Newton loop.  With False
         the GPU iterates from ``Vinit``.
+    scaling_max_voltage_change, max_dVa, max_dVm
+        The reference's MaxVoltageChange step scaling: True multiplies every
+        Newton step by alpha <= 1 so that max|dtheta| <= max_dVa and
+        max|dVm| <= max_dVm (defaults 0.5 rad / 0.1 pu).  None / False: off.
     """
 
     def __init__(self, grid, *, precision="fp64", max_iter=10, tol=1e-8, device=None,
-                 init_from_n_powerflow=True, **_ignored):
+                 init_from_n_powerflow=True, scaling_max_voltage_change=None, max_dVa=None, max_dVm=None,
+                 **_ignored):
         d = grid_arrays(grid)
         self._d = d
         self._prec = resolve_precision(precision)
         self.max_iter = int(max_iter)
         self.tol = float(tol)
+        # MaxVoltageChange step scaling (src/gpusim2grid/acpf_nr/gpu_facade.py:100-121):
+        # None (no grid configuration to inherit in array-tuple mode) is off
+        self._scaling = dict(step_scaling=bool(scaling_max_voltage_change),
+                             max_dva=0.0 if max_dVa is None else float(max_dVa),
+                             max_dvm=0.0 if max_dVm is None else float(max_dVm))
         self._s = make_session(d, device)
         self._vm_fixed = None
         self._sbus = d["Sbus"].copy()
@@ -68,7 +78,7 @@ class AcPfGPU:
         # a free-running solve takes the reference's single-solve order: each
         # step is taken, then the mismatch before it decides convergence
         self._s.run(int(max_iter), float(self.tol if tol is None else tol), bool(fixed), self._prec,
-                    lib.START_ROWS, step_then_check=not fixed)
+                    lib.START_ROWS, step_then_check=not fixed, **self._scaling)
         tm = self._s.timings()
         _, res, st, it = self._s.results()
         return AcPfTimings(converged=int(st[0]) == RowStatus.CONVERGED, nb_iter=int(it[0]),

@@ -70,9 +70,13 @@ def _ids_csr(rows):
 class _BatchSweep:
     def __init__(self, grid, *, init_from_n_powerflow=True, precision="fp64", nb_iter=4, max_iter_base=10,
                  tol_base=1e-8, device=None, scheduling=None, nb_iter_per_round=1, tol=None, start="base",
-                 strategy="refactor_every", handle_disconnected_grid=False, **_ignored):
+                 strategy="refactor_every", handle_disconnected_grid=False, scaling_max_voltage_change=None,
+                 max_dVa=None, max_dVm=None, **_ignored):
         d = grid_arrays(grid)
         self._d = d
+        self.scaling_max_voltage_change = scaling_max_voltage_change
+        self.max_dVa = max_dVa
+        self.max_dVm = max_dVm
         self._prec = resolve_precision(precision)
         self.nb_iter = int(nb_iter)
         self.scheduling = resolve_scheduling("chunked" if scheduling is None else scheduling)
@@ -251,6 +255,27 @@ class _BatchSweep:
         return dict(self._warm)
 
     @property
+    def scaling_max_voltage_change(self):
+        """The reference's MaxVoltageChange step scaling
+        (``src/gpusim2grid/contingency_analysis/gpu_facade.py:203-226``): True
+        multiplies every Newton step by alpha <= 1 so that max|dtheta| <=
+        ``max_dVa`` and max|dVm| <= ``max_dVm`` (defaults 0.5 rad / 0.1 pu),
+        damping steps taken far from the solution so that they do not land on
+        another power-flow root.  In array-tuple mode there is no grid
+        configuration to inherit, so None (default) means off.  Under
+        ``base_chord`` a row whose chord step would be scaled moves to its own
+        factor, where its steps are scaled."""
+        return self._scaling
+
+    @scaling_max_voltage_change.setter
+    def scaling_max_voltage_change(self, value):
+        self._scaling = bool(value) if value is not None else False
+
+    def _scaling_kw(self):
+        return dict(step_scaling=self._scaling, max_dva=float(self.max_dVa) if self.max_dVa is not None else 0.0,
+                    max_dvm=float(self.max_dVm) if self.max_dVm is not None else 0.0)
+
+    @property
     def refactor_ratio(self):
         """Contraction per step below which a row keeps its factor ('adaptive':
         its own LU, default 0.3; 'base_chord': the shared base factor, default
@@ -359,7 +384,7 @@ class _BatchSweep:
             self._warm = dict(predict_ms=(time.perf_counter() - t0) * 1e3)
             ratio, reuse = self._learned_opts
         self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False,
-                    _STRATEGY[self._strategy], ratio, reuse, rescue, self.nb_iter_per_round)
+                    _STRATEGY[self._strategy], ratio, reuse, rescue, self.nb_iter_per_round, **self._scaling_kw())
         tm = self._s.timings()
         if self._start == "learned":
             self._warm["n_rescued"] = int(tm["n_rescued"])
@@ -387,7 +412,7 @@ class _BatchSweep:
             return 0.0
         rows = bad.to(torch.int32).cpu().numpy()
         self._s.run_subset(rows, self.nb_iter, self.tol, False, lib.PREC_FP64, lib.START_VINIT, 0.0, n_ctas,
-                           lib.REFACTOR_EVERY, 0.0, 0, False, self.nb_iter_per_round)
+                           lib.REFACTOR_EVERY, 0.0, 0, False, self.nb_iter_per_round, **self._scaling_kw())
         self._fallback_rows = int(rows.size)
         self._host = None
         return float(self._s.timings()["kernel_ms"])
@@ -622,10 +647,10 @@ def compute_many(sweeps, batch_size=0):
         raise ValueError("compute_many needs at least one sweep")
     f0 = sweeps[0]
     for f in sweeps[1:]:
-        if (f._prec, f.nb_iter, f.tol, f.scheduling, f._strategy, f.nb_iter_per_round) != (
-                f0._prec, f0.nb_iter, f0.tol, f0.scheduling, f0._strategy, f0.nb_iter_per_round):
-            raise ValueError("compute_many: precision, nb_iter, tol, scheduling, strategy and nb_iter_per_round "
-                             "must agree")
+        if (f._prec, f.nb_iter, f.tol, f.scheduling, f._strategy, f.nb_iter_per_round, f._scaling_kw()) != (
+                f0._prec, f0.nb_iter, f0.tol, f0.scheduling, f0._strategy, f0.nb_iter_per_round, f0._scaling_kw()):
+            raise ValueError("compute_many: precision, nb_iter, tol, scheduling, strategy, nb_iter_per_round and "
+                             "the step scaling must agree")
     starts = {f._start for f in sweeps}
     if len(starts) != 1:
         raise ValueError("compute_many: every sweep must use the same start")
@@ -643,7 +668,7 @@ def compute_many(sweeps, batch_size=0):
         ratio, reuse = f0._learned_opts
     lib.run_multi([f._s for f in sweeps], f0.nb_iter, f0.tol, f0.scheduling == "chunked", f0._prec, _START[start],
                   0.0, max(int(batch_size), 0), False, _STRATEGY[f0._strategy], ratio, reuse,
-                  start in ("rows", "learned"), f0.nb_iter_per_round)
+                  start in ("rows", "learned"), f0.nb_iter_per_round, **f0._scaling_kw())
     kernel_ms = sweeps[0]._s.timings()["kernel_ms"]
     for f in sweeps:
         f._ran = True

@@ -677,6 +677,37 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots);
     prof.mark(PH_SOLVE_BACK);
 
+    // ---- step scaling (MaxVoltageChange): a slot whose chord step would be
+    // scaled leaves the chord before the step, for its own factor, where
+    // its steps are scaled (the Broyden recursion assumes full steps) ------
+    if (a.step_scaling) {
+      double mdt[CK] = {}, mdv[CK] = {};  // fmax skips NaN entries
+      for (int i = tid; i < n; i += BS) {
+        const int fp = P.fP[i], fq = P.fQ[i];
+        const SlotVec<T> ya = fp >= 0 ? y[fp] : SlotVec<T>{};
+        const SlotVec<T> ym = fq >= 0 ? y[fq] : SlotVec<T>{};
+#pragma unroll
+        for (int s = 0; s < CK; ++s) {
+          if (fp >= 0) mdt[s] = fmax(mdt[s], fabs((double)ya.v[s]));
+          if (fq >= 0) mdv[s] = fmax(mdv[s], fabs((double)ym.v[s]));
+        }
+      }
+      block_nanmax_slots(mdt, s_red_slots);
+      block_nanmax_slots(mdv, s_red_slots);
+      unsigned scaled = 0;  // the same on every thread (the maxima are broadcast)
+      for (int s = 0; s < CK; ++s)
+        if ((solve >> s & 1) && step_alpha(mdt[s], mdv[s], a.max_dva, a.max_dvm) < 1.0) scaled |= 1u << s;
+      solve &= ~scaled;
+      for (int s = 0; s < CK; ++s) {
+        if (!(scaled >> s & 1)) continue;
+        if (tid == 0) sl[s].act = 5;
+        __syncthreads();
+        chord_leave(a, sl[s], Vs + s, n, s_red);
+        if (tid == 0) sl[s].row = -1;
+        __syncthreads();
+      }
+    }
+
     // ---- V update (FP64, polar) ---------------------------------------------
     for (int i = tid; i < n; i += BS) {
       const int fp = P.fP[i], fq = P.fQ[i];

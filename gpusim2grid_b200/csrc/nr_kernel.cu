@@ -197,6 +197,16 @@ __device__ __noinline__ void schur_update(const DevPlan P, const T* __restrict__
   }
 }
 
+// The MaxVoltageChange scale of a Newton step with max|dtheta| = mdt and
+// max|dVm| = mdv (apply_step_scale_kernel, acpf_nr_kernels.cu:708-726): 1
+// unless a maximum exceeds its bound.
+__device__ __forceinline__ double step_alpha(double mdt, double mdv, double max_dva, double max_dvm) {
+  double alpha = 1.0;
+  if (mdt > max_dva) alpha = fmin(alpha, max_dva / mdt);
+  if (mdv > max_dvm) alpha = fmin(alpha, max_dvm / mdv);
+  return alpha;
+}
+
 // Dense tail LU: FP32 on the SIMT kernel of dense_lu_f32.cuh, FP64 on its
 // FP64 counterpart (dense_lu_f64.cuh; GS2G_FP64_LU=0 selects the older
 // DMMA-tile LU of dense_lu.cuh); all use the dynamic shared memory as
@@ -1203,12 +1213,25 @@ __device__ __forceinline__ void solve_row(const DevPlan& P, const SweepArgs& a, 
       // rows still on the base factor apply its dense tail through the base inverse
       apply_factor<T>(P, fHV, fS, y, s_blk, s_dense, prof, fHV != HV ? Minv : nullptr);
       if (comp_on) apply_compensation<T>(P.dim, y, Minv, sh);
+      // ---- step scaling (MaxVoltageChange, acpf_nr_kernels.cu:677-726) -----
+      double alpha = 1.0;
+      if (a.step_scaling) {
+        double mdt = 0.0, mdv = 0.0;  // fmax skips NaN entries
+        for (int i = tid; i < n; i += BS) {
+          const int fp = P.fP[i], fq = P.fQ[i];
+          if (fp >= 0) mdt = fmax(mdt, fabs((double)y[fp]));
+          if (fq >= 0) mdv = fmax(mdv, fabs((double)y[fq]));
+        }
+        mdt = block_nanmax(mdt, s_red);
+        mdv = block_nanmax(mdv, s_red);
+        alpha = step_alpha(mdt, mdv, a.max_dva, a.max_dvm);
+      }
       // ---- V update (FP64, polar) -----------------------------------------
       for (int i = tid; i < n; i += BS) {
         const int fp = P.fP[i], fq = P.fQ[i];
         if (fp < 0 && fq < 0) continue;
-        const double dva = fp >= 0 ? (double)y[fp] : 0.0;
-        const double dvm = fq >= 0 ? (double)y[fq] : 0.0;
+        const double dva = fp >= 0 ? alpha * (double)y[fp] : 0.0;
+        const double dvm = fq >= 0 ? alpha * (double)y[fq] : 0.0;
         const double2 v = V[i];
         const double vm = hypot(v.x, v.y) + dvm;
         const double va = atan2(v.y, v.x) + dva;

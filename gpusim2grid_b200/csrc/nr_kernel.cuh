@@ -143,6 +143,8 @@ struct SweepArgs {
   // outputs
   double* v_out;          // [n_rows * n_bus] complex
   double* v_mirror;       // nullptr, or a host-mapped copy of v_out that gets each row's final V as it leaves
+  int step_scaling;       // MaxVoltageChange: steps scaled so max|dtheta| <= max_dva, max|dVm| <= max_dvm
+  double max_dva, max_dvm;
   double* res_out;        // [n_rows]
   int* status_out;        // [n_rows]
   int* iters_out;         // [n_rows]

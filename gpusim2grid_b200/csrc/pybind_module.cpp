@@ -92,7 +92,8 @@ void check(int rc) {
 gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor,
                         int n_ctas, bool profile = false, int refactor = 0, double refactor_ratio = 0.0,
                         int max_reuse = 0, bool rescue = false, int iters_per_round = 1,
-                        bool step_then_check = false) {
+                        bool step_then_check = false, bool step_scaling = false, double max_dva = 0.0,
+                        double max_dvm = 0.0) {
   gs2g_run_opts o{};
   o.max_iter = max_iter;
   o.tol = tol;
@@ -108,6 +109,9 @@ gs2g_run_opts make_opts(int max_iter, double tol, bool fixed_iters, int precisio
   o.rescue = rescue ? 1 : 0;
   o.iters_per_round = iters_per_round;
   o.step_then_check = step_then_check ? 1 : 0;
+  o.step_scaling = step_scaling ? 1 : 0;
+  o.max_dva = max_dva;
+  o.max_dvm = max_dvm;
   return o;
 }
 
@@ -209,9 +213,10 @@ class Session {
 
   void run_subset(IArr rows, int max_iter, double tol, bool fixed_iters, int precision, int start,
                   double pivot_floor, int n_ctas, int refactor, double refactor_ratio, int max_reuse, bool rescue,
-                  int iters_per_round, bool profile) {
+                  int iters_per_round, bool profile, bool step_scaling, double max_dva, double max_dvm) {
     gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                                refactor_ratio, max_reuse, rescue, iters_per_round);
+                                refactor_ratio, max_reuse, rescue, iters_per_round, false, step_scaling, max_dva,
+                                max_dvm);
     const int n = (int)rows.size();
     const int* rp = rows.data();
     int rc;
@@ -283,9 +288,10 @@ class Session {
 
   void run(int max_iter, double tol, bool fixed_iters, int precision, int start, double pivot_floor, int n_ctas,
            bool profile, int refactor, double refactor_ratio, int max_reuse, bool rescue, int iters_per_round,
-           bool step_then_check) {
+           bool step_then_check, bool step_scaling, double max_dva, double max_dvm) {
     gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                                refactor_ratio, max_reuse, rescue, iters_per_round, step_then_check);
+                                refactor_ratio, max_reuse, rescue, iters_per_round, step_then_check, step_scaling,
+                                max_dva, max_dvm);
     int rc;
     {
       py::gil_scoped_release nogil;
@@ -487,14 +493,15 @@ py::dict plan_info(int n_bus, IArr indptr, IArr indices, IArr pv, IArr pq, int t
 // Several sessions' current rows in one persistent launch (gs2g_run_multi).
 void run_multi(const std::vector<Session*>& sessions, int max_iter, double tol, bool fixed_iters, int precision,
                int start, double pivot_floor, int n_ctas, bool profile, int refactor, double refactor_ratio,
-               int max_reuse, bool rescue, int iters_per_round) {
+               int max_reuse, bool rescue, int iters_per_round, bool step_scaling, double max_dva,
+               double max_dvm) {
   std::vector<gs2g_session*> hs;
   for (Session* s : sessions) {
     if (!s) throw py::value_error("run_multi: None in the session list");
     hs.push_back(reinterpret_cast<gs2g_session*>(s->handle()));
   }
   gs2g_run_opts o = make_opts(max_iter, tol, fixed_iters, precision, start, pivot_floor, n_ctas, profile, refactor,
-                              refactor_ratio, max_reuse, rescue, iters_per_round);
+                              refactor_ratio, max_reuse, rescue, iters_per_round, false, step_scaling, max_dva, max_dvm);
   int rc;
   {
     py::gil_scoped_release nogil;
@@ -582,7 +589,8 @@ PYBIND11_MODULE(_gs2g, m) {
   m.def("run_multi", &run_multi, py::arg("sessions"), py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"),
         py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0,
         py::arg("profile") = false, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0,
-        py::arg("max_reuse") = 0, py::arg("rescue") = false, py::arg("iters_per_round") = 1);
+        py::arg("max_reuse") = 0, py::arg("rescue") = false, py::arg("iters_per_round") = 1,
+        py::arg("step_scaling") = false, py::arg("max_dva") = 0.0, py::arg("max_dvm") = 0.0);
   py::class_<Session>(m, "Session")
       .def(py::init<int, int, IArr, IArr, CArr, CArr, CArr, IArr, IArr, int>(), py::arg("device"), py::arg("n_bus"),
            py::arg("indptr"), py::arg("indices"), py::arg("data"), py::arg("vinit"), py::arg("sbus"), py::arg("pv"),
@@ -602,7 +610,8 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("run_subset", &Session::run_subset, py::arg("rows"), py::arg("max_iter"), py::arg("tol"),
            py::arg("fixed_iters"), py::arg("precision"), py::arg("start"), py::arg("pivot_floor") = 0.0,
            py::arg("n_ctas") = 0, py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
-           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("profile") = false)
+           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("profile") = false,
+           py::arg("step_scaling") = false, py::arg("max_dva") = 0.0, py::arg("max_dvm") = 0.0)
       .def("branch_loading", &Session::branch_loading)
       .def("set_chord", &Session::set_chord, py::arg("mode"))
       .def("set_handoff", &Session::set_handoff, py::arg("cluster"))
@@ -620,7 +629,8 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("run", &Session::run, py::arg("max_iter"), py::arg("tol"), py::arg("fixed_iters"), py::arg("precision"),
            py::arg("start"), py::arg("pivot_floor") = 0.0, py::arg("n_ctas") = 0, py::arg("profile") = false,
            py::arg("refactor") = 0, py::arg("refactor_ratio") = 0.0, py::arg("max_reuse") = 0,
-           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("step_then_check") = false)
+           py::arg("rescue") = false, py::arg("iters_per_round") = 1, py::arg("step_then_check") = false,
+           py::arg("step_scaling") = false, py::arg("max_dva") = 0.0, py::arg("max_dvm") = 0.0)
       .def("factor_counts", &Session::factor_counts)
       .def("n_rows", &Session::n_rows)
       .def("results", &Session::results)

@@ -586,6 +586,9 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
     throw std::invalid_argument("iters_per_round must be <= " + std::to_string(kMaxItersPerRound));
   a.round_k = o.iters_per_round > 0 ? o.iters_per_round : 1;
   a.step_first = o.step_then_check != 0 && !o.fixed_iters;
+  a.step_scaling = o.step_scaling != 0;
+  a.max_dva = o.max_dva > 0 ? o.max_dva : 0.5;
+  a.max_dvm = o.max_dvm > 0 ? o.max_dvm : 0.1;
   a.v_out = out.v;
   a.v_mirror = out.v_mirror;
   a.res_out = out.res;

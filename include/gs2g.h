@@ -112,6 +112,19 @@ typedef struct gs2g_run_opts {
    * never passes the test within max_iter steps ends MAX_ITER (DIVERGED
    * when its last mismatch is not finite).  Continuous schedule only. */
   int step_then_check;
+  /* 1: the reference's MaxVoltageChange step scaling
+   * (reduce_step_norms_kernel / apply_step_scale_kernel,
+   * src/_cpp/acpf_nr_kernels.cu:677-726; facade option
+   * scaling_max_voltage_change, src/gpusim2grid/acpf_nr/gpu_facade.py:100-121):
+   * every Newton step is multiplied by alpha = min(1, max_dva / max|dtheta|,
+   * max_dvm / max|dVm|) before it is applied, which keeps a step from far
+   * away (a flat start, a heavily loaded row) from jumping to another
+   * power-flow solution.  Under GS2G_REFACTOR_BASE_CHORD a row whose chord
+   * step would be scaled leaves the chord for its own factor, where its
+   * steps are scaled.  0 (default): full steps. */
+  int step_scaling;
+  double max_dva; /* radians; <= 0 selects 0.5 */
+  double max_dvm; /* per unit; <= 0 selects 0.1 */
 } gs2g_run_opts;
 
 #define GS2G_REFACTOR_EVERY 0
@@ -349,8 +362,9 @@ int gs2g_sync(gs2g_session* s);
  *   pivot_floor, refactor_policy (GS2G_REFACTOR_EVERY or _ADAPTIVE only;
  *   GS2G_REFACTOR_BASE_CHORD needs session buffers and is rejected),
  *   refactor_ratio, max_reuse, rescue, iters_per_round and step_then_check;
- *   start, n_ctas and profile_phases are ignored (the rows start from v0, the
- *   CTA count is what fits the scratch, no phase counters).
+ *   start, n_ctas, profile_phases and the step scaling (step_scaling,
+ *   max_dva, max_dvm) are ignored (the rows start from v0, the CTA count is
+ *   what fits the scratch, no phase counters, full steps).
  *   The device address of the scratch array is looked up once per device
  *   and kept for the life of the process: after cudaDeviceReset (or any
  *   re-creation of the device's primary context) this entry point must not

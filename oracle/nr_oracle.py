@@ -97,12 +97,29 @@ def nan_inf_norm(F):
     return float(np.max(np.abs(F)))
 
 
-def newton_step(Y, V, F, pvpq, pq):
+def step_scale(dx, n_pvpq, max_dva, max_dvm):
+    """The MaxVoltageChange step scaling (reduce_step_norms_kernel +
+    apply_step_scale_kernel, ``src/_cpp/acpf_nr_kernels.cu:677-726``): the
+    whole step times alpha = min(1, max_dVa / max|dtheta|, max_dVm / max|dVm|),
+    applied only when a maximum exceeds its bound."""
+    dth, dvm = np.abs(dx[:n_pvpq]), np.abs(dx[n_pvpq:])
+    mdt = float(dth.max()) if dth.size else 0.0
+    mdv = float(dvm.max()) if dvm.size else 0.0
+    alpha = 1.0
+    if mdt > max_dva:
+        alpha = min(alpha, max_dva / mdt)
+    if mdv > max_dvm:
+        alpha = min(alpha, max_dvm / mdv)
+    return dx if alpha == 1.0 else dx * alpha
+
+
+def newton_step(Y, V, F, pvpq, pq, scaling=None):
     """One full Newton step from V with mismatch F: J at V, dx = J^-1 F, then
     the polar update (acpf_nr.cu nr_iter_step: SpMV, fill F, fill J,
     factorize, solve, update V).  A step that cannot be taken (a non-finite
     mismatch or a singular J) leaves every unknown NaN, as NaN propagates
-    through the reference's solve."""
+    through the reference's solve.  ``scaling`` = (max_dVa, max_dVm) turns on
+    the MaxVoltageChange step scaling (``step_scale``)."""
     if np.all(np.isfinite(F)):
         J = jacobian(Y, V, pvpq, pq)
         try:
@@ -112,10 +129,12 @@ def newton_step(Y, V, F, pvpq, pq):
             dx = np.full(F.size, np.nan)
     else:
         dx = np.full(F.size, np.nan)
+    if scaling is not None and np.all(np.isfinite(dx)):
+        dx = step_scale(dx, pvpq.size, *scaling)
     return update_v(V, dx, pvpq, pq)
 
 
-def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1):
+def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1, scaling=None):
     """One NR solve under one of the reference's three schedules.
 
     mode="continuous" (``src/_cpp/contingency/batch_pf_driver.cu:2691-2724``):
@@ -133,7 +152,8 @@ def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1)
     after it; no pass within ``max_iter`` steps is MAX_ITER (DIVERGED when the
     last mismatch is not finite).  ``residual`` is the last mismatch
     evaluated (for a converged single solve: the one that passed).
-    "converge" is an alias of "continuous".
+    "converge" is an alias of "continuous".  ``scaling`` = (max_dVa, max_dVm)
+    scales every step (``step_scale``).
 
     Returns (V, status, iters, residual).
     """
@@ -163,7 +183,7 @@ def nr_solve(Y, V0, Sbus, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1)
                 return V, CONVERGED, it, nrm
             if it >= max_iter:
                 return V, MAX_ITER, it, nrm
-        V = newton_step(Y, V, F, pvpq, pq_)
+        V = newton_step(Y, V, F, pvpq, pq_, scaling)
         it += 1
         if mode == "single" and nrm < tol:
             return V, CONVERGED, it, nrm
@@ -221,7 +241,7 @@ def main_component(n_bus, f, t, branch_ids):
 
 
 def contingency_sweep(Y, V0, Sbus, pv, pq, branch_rows, f, t, yff, yft, ytf, ytt,
-                      max_iter=10, tol=1e-8, mode="continuous", k=1, handle_disconnected=False):
+                      max_iter=10, tol=1e-8, mode="continuous", k=1, handle_disconnected=False, scaling=None):
     """Solve every row (a list of tripped-branch lists).  Islanding rows are
     NOT_SIMULATED with NaN voltages (contingency_analysis_helper.cpp:634-651),
     or, with ``handle_disconnected``, solved on their largest component with
@@ -249,15 +269,15 @@ def contingency_sweep(Y, V0, Sbus, pv, pq, branch_rows, f, t, yff, yft, ytf, ytt
                 continue
         Yr = trip_branches(Y, ids, f, t, yff, yft, ytf, ytt)
         if live is None:
-            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode, k)
+            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv, pq, max_iter, tol, mode, k, scaling)
         else:
-            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv[live[pv]], pq[live[pq]], max_iter, tol, mode, k)
+            V, st, it, nrm = nr_solve(Yr, V0, Sbus, pv[live[pv]], pq[live[pq]], max_iter, tol, mode, k, scaling)
             V = np.where(live, V, np.nan + 0j)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
 
 
-def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1):
+def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="continuous", k=1, scaling=None):
     """Solve one row per Sbus row."""
     B, n = Sbus_rows.shape
     out_V = np.empty((B, n), dtype=np.complex128)
@@ -265,7 +285,7 @@ def injection_sweep(Y, V0, Sbus_rows, pv, pq, max_iter=10, tol=1e-8, mode="conti
     iters = np.empty(B, dtype=np.int32)
     res = np.empty(B)
     for r in range(B):
-        V, st, it, nrm = nr_solve(Y, V0, Sbus_rows[r], pv, pq, max_iter, tol, mode, k)
+        V, st, it, nrm = nr_solve(Y, V0, Sbus_rows[r], pv, pq, max_iter, tol, mode, k, scaling)
         out_V[r], status[r], iters[r], res[r] = V, st, it, nrm
     return out_V, status, iters, res
 

@@ -70,12 +70,15 @@ def test_ctypes_layouts_match_the_header(tmp_path):
     src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "gs2g.h"\n'
                    'int main(void) { printf("%zu %zu %zu %zu\\n", sizeof(gs2g_run_opts), '
                    'offsetof(gs2g_run_opts, iters_per_round), offsetof(gs2g_run_opts, step_then_check), '
-                   'sizeof(gs2g_timings)); return 0; }\n')
+                   'sizeof(gs2g_timings)); printf("%zu %zu\\n", offsetof(gs2g_run_opts, step_scaling), '
+                   'offsetof(gs2g_run_opts, max_dvm)); return 0; }\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
-    size, off_k, off_s, _ = map(int, subprocess.run([str(exe)], capture_output=True, text=True,
-                                                    check=True).stdout.split())
+    size, off_k, off_s, _, off_sc, off_vm = map(int, subprocess.run([str(exe)], capture_output=True, text=True,
+                                                                    check=True).stdout.split())
     assert ctypes.sizeof(RunOpts) == size
     assert RunOpts.iters_per_round.offset == off_k and RunOpts.step_then_check.offset == off_s
+    assert RunOpts.step_scaling.offset == off_sc and RunOpts.max_dvm.offset == off_vm
     doc = open(os.path.join(os.path.dirname(HEADER), "..", "INTEGRATION.md")).read()
-    assert '("iters_per_round", I), ("step_then_check", I)' in doc
+    assert '("iters_per_round", I), ("step_then_check", I),' in doc
+    assert '("step_scaling", I), ("max_dva", D), ("max_dvm", D)' in doc

@@ -194,3 +194,19 @@ def test_disconnected_rows_solve_their_largest_component(g118):
     for r in np.flatnonzero(~solved):
         live = O.main_component(g118.n_bus, g118.branch_from, g118.branch_to, rows[r])
         assert not live[g118.slack] and st[r] == O.NOT_SIMULATED
+
+
+def test_step_scaling_restates_max_voltage_change(g118):
+    """The MaxVoltageChange scaling (acpf_nr_kernels.cu:677-726): the whole
+    step times min(1, max_dVa / max|dtheta|, max_dVm / max|dVm|), applied only
+    when a bound is exceeded; damped solves reach the same solution in more
+    steps."""
+    dx = np.array([0.3, -0.05, 0.02, -0.2])  # two angles, then two magnitudes
+    np.testing.assert_array_equal(O.step_scale(dx, 2, 0.5, 0.25), dx)
+    np.testing.assert_allclose(O.step_scale(dx, 2, 0.1, 0.25), dx * (0.1 / 0.3))
+    np.testing.assert_allclose(O.step_scale(dx, 2, 0.5, 0.05), dx * (0.05 / 0.2))
+    Y, V0, S, _, _, pv, pq = g118.as_tuple()
+    V1, st1, it1, _ = O.nr_solve(Y, V0, S, pv, pq, 20, 1e-10)
+    V2, st2, it2, _ = O.nr_solve(Y, V0, S, pv, pq, 20, 1e-10, scaling=(0.1, 0.03))
+    assert st1 == st2 == O.CONVERGED and it2 > it1
+    assert np.abs(V1 - V2).max() < 1e-9

@@ -29,7 +29,8 @@ class RunOpts(ctypes.Structure):
                 ("precision", ctypes.c_int), ("start", ctypes.c_int), ("pivot_floor", ctypes.c_double),
                 ("n_ctas", ctypes.c_int), ("profile_phases", ctypes.c_int), ("refactor_policy", ctypes.c_int),
                 ("refactor_ratio", ctypes.c_double), ("max_reuse", ctypes.c_int), ("rescue", ctypes.c_int),
-                ("iters_per_round", ctypes.c_int), ("step_then_check", ctypes.c_int)]
+                ("iters_per_round", ctypes.c_int), ("step_then_check", ctypes.c_int),
+                ("step_scaling", ctypes.c_int), ("max_dva", ctypes.c_double), ("max_dvm", ctypes.c_double)]
 
 
 def _capi():
