@@ -157,13 +157,37 @@ __device__ __forceinline__ void block_sum_slots(double v[CK], double* s_red_slot
   __syncthreads();
 }
 
-// Broyden correction of the slots in `mask`: y holds z = H0 F per slot on
-// entry and the step s_{nb} on exit, which is also stored as the slot's
-// next Broyden step (with its squared norm).  St: the CTA's steps
+// Outage compensation of one unknown's right-hand sides (slots in `comp`):
+// y_s[i] -= sum_c Minv[R_s[c], i] w_s[c], with w_s from chord_comp_solve.
+template <typename T>
+__device__ __forceinline__ void comp_apply(const int i, const int dim, const unsigned comp, SlotVec<T>& yi,
+                                           const T* Minv, const int (*s_cr)[1 + MAX_COMP],
+                                           const double (*s_cw)[MAX_COMP]) {
+#pragma unroll
+  for (int s = 0; s < CK; ++s) {
+    if (!(comp >> s & 1)) continue;
+    const int r = s_cr[s][0];
+    T acc = T(0);
+    for (int c = 0; c < r; ++c) acc += Minv[(int64_t)s_cr[s][1 + c] * dim + i] * (T)s_cw[s][c];
+    yi.v[s] -= acc;
+  }
+}
+
+// Broyden correction of the slots in `mask`: y holds x0 = M0^-1 F per slot on
+// entry (before the outage compensation of the slots in `comp`, which the
+// first pass applies) and the step s_{nb} on exit, which is also stored as
+// the slot's next Broyden step (with its squared norm).  St: the CTA's steps
 // [CK][CB_MAX][dim]; s_ss: their squared norms.
+//
+// Each pass over the unknowns reads one stored step per slot: the update
+// z += c_j s_{j+1} and the next coefficient's dot product s_{j+1} . z share
+// it (the dot is taken right after the update, on the same z), so n stored
+// steps take n + 1 passes; the arithmetic and its order are the recursion's.
 template <typename T>
 __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, ChordSlot* sl, SlotVec<T>* y, T* St,
-                                           double (*s_ss)[CB_MAX], double* s_red_slots) {
+                                           double (*s_ss)[CB_MAX], double* s_red_slots, const unsigned comp,
+                                           const T* Minv, const int (*s_cr)[1 + MAX_COMP],
+                                           const double (*s_cw)[MAX_COMP]) {
   const int tid = threadIdx.x;
   int nb[CK];
   int maxnb = 0;
@@ -174,42 +198,51 @@ __device__ __noinline__ void chord_broyden(const int dim, const unsigned mask, C
     maxnb = max(maxnb, nb[s]);
   }
   auto step = [&](int s, int j) { return St + ((int64_t)s * CB_MAX + j) * dim; };
-  for (int j = 0; j + 1 < maxnb; ++j) {
-    double d[CK] = {};
+  // pass 0: the compensation (z = H0 F complete), and d = s_0 . z of every
+  // slot holding steps (the first coefficient's, or the final one's when the
+  // slot holds one step)
+  double d[CK] = {};
+  if (maxnb > 0 || comp) {
     for (int i = tid; i < dim; i += BS) {
-      const SlotVec<T> z = y[i];
+      SlotVec<T> z = y[i];
+      if (comp) {
+        comp_apply(i, dim, comp, z, Minv, s_cr, s_cw);
+        y[i] = z;
+      }
 #pragma unroll
       for (int s = 0; s < CK; ++s)
-        if (j + 1 < nb[s]) d[s] += (double)step(s, j)[i] * (double)z.v[s];
+        if (nb[s] > 0) d[s] += (double)step(s, 0)[i] * (double)z.v[s];
     }
-    block_sum_slots(d, s_red_slots);
+    if (maxnb > 0) block_sum_slots(d, s_red_slots);
+    else __syncthreads();
+  }
+  // z += s_{j+1} (s_j . z) / |s_j|^2 for j < nb - 1; d ends as s_{nb-1} . z
+  for (int j = 0; j + 1 < maxnb; ++j) {
     T cf[CK];
 #pragma unroll
     for (int s = 0; s < CK; ++s) {
       const double ss = s_ss[s][j];
       cf[s] = (j + 1 < nb[s] && ss > 0.0) ? (T)(d[s] / ss) : T(0);
     }
+    double dn[CK] = {};
     for (int i = tid; i < dim; i += BS) {
       SlotVec<T> z = y[i];
 #pragma unroll
       for (int s = 0; s < CK; ++s)
-        if (j + 1 < nb[s]) z.v[s] = fma(cf[s], step(s, j + 1)[i], z.v[s]);
+        if (j + 1 < nb[s]) {
+          const T st = step(s, j + 1)[i];
+          z.v[s] = fma(cf[s], st, z.v[s]);
+          dn[s] += (double)st * (double)z.v[s];
+        }
       y[i] = z;
     }
-    __syncthreads();
+    block_sum_slots(dn, s_red_slots);
+#pragma unroll
+    for (int s = 0; s < CK; ++s)
+      if (j + 1 < nb[s]) d[s] = dn[s];
   }
   // s_{nb} = z / (1 - (s_{nb-1} . z) / |s_{nb-1}|^2); a vanishing denominator
   // (the update breaks down) restarts the memory with the plain step z
-  double d[CK] = {};
-  if (maxnb > 0) {
-    for (int i = tid; i < dim; i += BS) {
-      const SlotVec<T> z = y[i];
-#pragma unroll
-      for (int s = 0; s < CK; ++s)
-        if (nb[s] > 0) d[s] += (double)step(s, nb[s] - 1)[i] * (double)z.v[s];
-    }
-    block_sum_slots(d, s_red_slots);
-  }
   T sc[CK];
 #pragma unroll
   for (int s = 0; s < CK; ++s) {
@@ -311,6 +344,44 @@ __device__ __noinline__ void chord_mismatch(const DevPlan P, const SweepArgs a, 
 #pragma unroll
     for (int s = 0; s < CK; ++s)
       if (mask >> s & 1) nrm_out[s] = lmax[s];
+  __syncthreads();
+}
+
+// F and ||F||inf of slot s at the alternative start (the base V, already in
+// the slot's lane of Vs) without the sparse product: Ia = Y Va on the
+// unedited Ybus, shared by all rows and summed with chord_mismatch's fused
+// multiply-adds in its order, is corrected at the buses of the row's edited
+// Ybus rows exactly as chord_mismatch corrects its sums, so F and the norm
+// are bit-identical to chord_mismatch's for this slot.  Writes only the
+// slot's lane of y.
+template <typename T>
+__device__ __noinline__ void chord_mismatch_alt(const DevPlan P, const SweepArgs a, const int s, const ChordSlot* sl,
+                                                const int* s_ne, const int (*s_er)[MAX_EDITS],
+                                                const int (*s_ec)[MAX_EDITS], const double2 (*s_ev)[MAX_EDITS],
+                                                const double2* Vs, const double2* __restrict__ Ia, SlotVec<T>* y,
+                                                double* nrm_out, double* s_red) {
+  const double2* sb = reinterpret_cast<const double2*>(a.sbus) + (int64_t)(sl[s].row < 0 ? 0 : sl[s].row) * a.sbus_stride;
+  double lmax = 0.0;
+  for (int i = threadIdx.x; i < P.n_bus; i += BS) {
+    double2 acc = Ia[i];
+    for (int e = 0; e < s_ne[s]; ++e) {
+      if (s_er[s][e] != i) continue;
+      const double2 vj = Vs[(int64_t)s_ec[s][e] * CK + s];
+      acc = csub(acc, cmul(s_ev[s][e], vj));
+    }
+    const double2 sv = csub(cmul(Vs[(int64_t)i * CK + s], conj2(acc)), sb[i]);
+    const int fp = P.fP[i], fq = P.fQ[i];
+    if (fp >= 0) {
+      y[fp].v[s] = (T)(-sv.x);
+      lmax = (isnan(sv.x) || isnan(lmax)) ? NAN : fmax(lmax, fabs(sv.x));
+    }
+    if (fq >= 0) {
+      y[fq].v[s] = (T)(-sv.y);
+      lmax = (isnan(sv.y) || isnan(lmax)) ? NAN : fmax(lmax, fabs(sv.y));
+    }
+  }
+  lmax = block_nanmax(lmax, s_red);
+  if (threadIdx.x == 0) nrm_out[s] = lmax;
   __syncthreads();
 }
 
@@ -433,17 +504,19 @@ __device__ __noinline__ void chord_leave(const SweepArgs a, const ChordSlot sl, 
   __syncthreads();
 }
 
-// Outage compensation of the slots in `comp`, all in one pass:
+// Outage compensation of the slots in `comp`:
 // y_s <- y_s - Z_s B_s (I + W_s B_s)^-1 y_s[R_s] (see setup_compensation and
-// apply_compensation, the one-row form).  The small solves run in parallel,
-// one warp's leading thread per slot; then one sweep over the unknowns
-// applies every slot's columns of the base inverse.
+// apply_compensation, the one-row form).  First the small solves, in
+// parallel, one warp's leading thread per slot (w_s = B_s (I + W_s B_s)^-1
+// y_s[R_s] into s_cw); then one sweep over the unknowns applies every slot's
+// columns of the base inverse (comp_apply: chord_comp_apply, or the first
+// pass of chord_broyden).
 template <typename T>
-__device__ __noinline__ void chord_compensation(const int dim, const unsigned comp, SlotVec<T>* y, const T* Minv,
-                                                const int (*s_cr)[1 + MAX_COMP],
-                                                const double (*s_cB)[MAX_COMP * MAX_COMP],
-                                                const double (*s_cLU)[MAX_COMP * MAX_COMP],
-                                                const int (*s_cpiv)[MAX_COMP], double (*s_cw)[MAX_COMP]) {
+__device__ __noinline__ void chord_comp_solve(const unsigned comp, const SlotVec<T>* y,
+                                              const int (*s_cr)[1 + MAX_COMP],
+                                              const double (*s_cB)[MAX_COMP * MAX_COMP],
+                                              const double (*s_cLU)[MAX_COMP * MAX_COMP],
+                                              const int (*s_cpiv)[MAX_COMP], double (*s_cw)[MAX_COMP]) {
   const int tid = threadIdx.x;
   const int s0 = tid >> 5;
   if (s0 < CK && (tid & 31) == 0 && (comp >> s0 & 1)) {
@@ -474,16 +547,14 @@ __device__ __noinline__ void chord_compensation(const int dim, const unsigned co
     }
   }
   __syncthreads();
-  for (int i = tid; i < dim; i += BS) {
+}
+
+template <typename T>
+__device__ __noinline__ void chord_comp_apply(const int dim, const unsigned comp, SlotVec<T>* y, const T* Minv,
+                                              const int (*s_cr)[1 + MAX_COMP], const double (*s_cw)[MAX_COMP]) {
+  for (int i = threadIdx.x; i < dim; i += BS) {
     SlotVec<T> yi = y[i];
-#pragma unroll
-    for (int s = 0; s < CK; ++s) {
-      if (!(comp >> s & 1)) continue;
-      const int r = s_cr[s][0];
-      T acc = T(0);
-      for (int c = 0; c < r; ++c) acc += Minv[(int64_t)s_cr[s][1 + c] * dim + i] * (T)s_cw[s][c];
-      yi.v[s] -= acc;
-    }
+    comp_apply(i, dim, comp, yi, Minv, s_cr, s_cw);
     y[i] = yi;
   }
   __syncthreads();
@@ -619,8 +690,12 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         for (int i = tid; i < n; i += BS) Vs[(int64_t)i * CK + s] = va[i];
         if (tid == 0 && a.n_alt_start != nullptr) atomicAdd(a.n_alt_start, 1);
         __syncthreads();
-        chord_mismatch<T>(P, a, 1u << s, active & ~(1u << s), sl, s_ne, s_er, s_ec, s_ev, Vs, y, s_nrm,
-                          s_red_slots);
+        if (a.alt_i != nullptr)
+          chord_mismatch_alt<T>(P, a, s, sl, s_ne, s_er, s_ec, s_ev, Vs, reinterpret_cast<const double2*>(a.alt_i),
+                                y, s_nrm, s_red);
+        else
+          chord_mismatch<T>(P, a, 1u << s, active & ~(1u << s), sl, s_ne, s_er, s_ec, s_ev, Vs, y, s_nrm,
+                            s_red_slots);
       }
     }
     prof.mark(PH_MISMATCH);
@@ -672,9 +747,10 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
     {
       unsigned comp = 0;
       for (int s = 0; s < CK; ++s) comp |= ((solve >> s & 1) && sl[s].comp ? 1u : 0u) << s;
-      if (comp) chord_compensation<T>(P.dim, comp, y, Minv, s_cr, s_cB, s_cLU, s_cpiv, s_cw);
+      if (comp) chord_comp_solve<T>(comp, y, s_cr, s_cB, s_cLU, s_cpiv, s_cw);
+      if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots, comp, Minv, s_cr, s_cw);
+      else if (comp) chord_comp_apply<T>(P.dim, comp, y, Minv, s_cr, s_cw);
     }
-    if (a.broyden) chord_broyden<T>(P.dim, solve, sl, y, St, s_ss, s_red_slots);
     prof.mark(PH_SOLVE_BACK);
 
     // ---- step scaling (MaxVoltageChange): a slot whose chord step would be

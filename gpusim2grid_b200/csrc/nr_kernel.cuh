@@ -112,6 +112,9 @@ struct SweepArgs {
   // that follows the chord sweep on the same stream takes its hand-offs)
   const int* n_rows_dev;
   const double* alt_s;  // complex [n_bus] V conj(Y V) at alt_v0 on the unedited Ybus (nullptr: evaluate in full)
+  // complex [n_bus] Y V at alt_v0 on the unedited Ybus, summed over each
+  // Ybus row in the order of the sweep's mismatch (nullptr: evaluate in full)
+  const double* alt_i;
   int* n_alt_start;
   // chord sweep: Newton steps taken on the shared base factor, summed over rows
   unsigned long long* n_chord_steps;

@@ -91,6 +91,7 @@ struct gs2g_session {
   bool has_base = false;
   DevBuf d_ybus, d_vinit, d_sbus, d_basev;
   DevBuf d_bases;  // complex [n_bus] Vb conj(Y Vb): the power the base V draws on the unedited Ybus
+  DevBuf d_basei;  // complex [n_bus] Y Vb, summed as the sweep's mismatch sums (fused multiply-adds, row order)
 
   // branch data
   int n_branch = 0;
@@ -621,6 +622,7 @@ gs2g::SweepArgs make_args(gs2g_session* s, const gs2g_run_opts& o, int n_rows, c
   a.rescue_v0 = rescue ? (base ? s->d_basev.as<double>() : s->d_vinit.as<double>()) : nullptr;
   a.alt_v0 = base ? s->d_basev.as<double>() : nullptr;
   a.alt_s = base ? s->d_bases.as<double>() : nullptr;
+  a.alt_i = base ? s->d_basei.as<double>() : nullptr;
   a.phase_cycles = nullptr;
   if (use_rows && s->limits_on) {
     const size_t nr = (size_t)std::max(n_rows, 1);
@@ -715,6 +717,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     a.base_bwv = nullptr;
     a.alt_v0 = nullptr;
     a.alt_s = nullptr;
+    a.alt_i = nullptr;
   }
   // hand-offs with a dense tail worth sharing: a cluster of 16 (or 8) CTAs
   // per row when every row gets one (the rows are few and each of their
@@ -1320,24 +1323,34 @@ int gs2g_set_vinit(gs2g_session* s, const double* vinit) {
 
 namespace {
 // Vb conj(Y Vb) per bus for the current base V (host, once per base case),
-// so that a row's mismatch at the base V needs no sparse product
+// so that a row's mismatch norm at the base V needs no sparse product; and
+// Y Vb itself, summed with the fused multiply-adds of the sweep's mismatch
+// in the same order (IEEE fma rounds the same on host and device), so that
+// the chord sweep writes a row's F at the base V bit-identical to the sparse
+// product it replaces.
 void upload_base_power(gs2g_session* s) {
   const int n = s->n_bus;
-  std::vector<double> S(2 * n);
+  std::vector<double> S(2 * n), I(2 * n);
   for (int i = 0; i < n; ++i) {
-    double ir = 0, ii = 0;
+    double ir = 0, ii = 0, fr = 0, fi = 0;
     for (int k = s->y_ip[i]; k < s->y_ip[i + 1]; ++k) {
       const double yr = s->ybus[2 * k], yi = s->ybus[2 * k + 1];
       const double vr = s->base_v[2 * s->y_ix[k]], vi = s->base_v[2 * s->y_ix[k] + 1];
       ir += yr * vr - yi * vi;
       ii += yr * vi + yi * vr;
+      fr = std::fma(yr, vr, std::fma(-yi, vi, fr));
+      fi = std::fma(yr, vi, std::fma(yi, vr, fi));
     }
     const double vr = s->base_v[2 * i], vi = s->base_v[2 * i + 1];
     S[2 * i] = vr * ir + vi * ii;  // V conj(I)
     S[2 * i + 1] = vi * ir - vr * ii;
+    I[2 * i] = fr;
+    I[2 * i + 1] = fi;
   }
   s->d_bases.ensure(2 * n * sizeof(double));
   ck(cudaMemcpy(s->d_bases.p, S.data(), 2 * n * sizeof(double), cudaMemcpyHostToDevice), "upload base power");
+  s->d_basei.ensure(2 * n * sizeof(double));
+  ck(cudaMemcpy(s->d_basei.p, I.data(), 2 * n * sizeof(double), cudaMemcpyHostToDevice), "upload base current");
 }
 }  // namespace
 
@@ -1697,6 +1710,7 @@ int gs2g_run_multi(gs2g_session* const* sessions, int n_sessions, const gs2g_run
       b.base_inv = nullptr;
       b.alt_v0 = nullptr;
       b.alt_s = nullptr;
+      b.alt_i = nullptr;
     }
   }
   s0->d_ws.ensure(std::max((size_t)wsb * n_ctas, (size_t)cwsb * n_chord));

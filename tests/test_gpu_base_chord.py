@@ -171,3 +171,38 @@ def test_row_order_leaves_results_unchanged(kind):
     for a, b in zip(*out):
         np.testing.assert_array_equal(a, b)
     assert out[0][3].sum() > 0
+
+
+@pytest.mark.parametrize("kind", ["n1", "scenario"])
+def test_start_switch_equals_base_start(kind):
+    """A row whose own start has the larger mismatch starts from the base V
+    instead (start selection).  The chord sweep then writes the row's F at
+    the base V from the base case's Ybus product (summed as the sweep's
+    mismatch sums), corrected at the row's edited Ybus rows, instead of a
+    sparse product.  Rows that all start flat (every one switches) must give
+    the base-start results bit for bit."""
+    from gpusim2grid_b200.synthetic import grid_by_name, scenario_outages
+    g = grid_by_name("case2000_synth", 0)
+    kw = dict(init_from_n_powerflow=False, precision="mixed", nb_iter=10, scheduling="continuous", tol=1e-8,
+              start="base", strategy="base_chord")
+    if kind == "n1":
+        sw = ContingencyAnalysisGPU(g.as_tuple(), **kw)
+        sw.set_branch_data(*g.branch_data())
+        sw.add_contingencies_by_branch_id([[int(b)] for b in n1_branches(g)])
+        n = len(n1_branches(g))
+    else:
+        n = 1024
+        p, q = injection_scenarios(g, n, seed=51)
+        sw = ScenarioSweepGPU(g.as_tuple(), **kw)
+        sw.set_branch_data(*g.branch_data())
+        sw.set_injections(p, q, g.sn_mva)
+        sw.set_topology(scenario_outages(g, n, max_trips=2, seed=52))
+    sw.compute()
+    base = (sw.V_results.copy(), sw.get_row_status().copy(), sw.get_row_iterations().copy(),
+            sw.get_row_factorizations().copy())
+    sw.set_start_voltages(np.tile(np.asarray(g.vinit(), dtype=np.complex128), (n, 1)))
+    sw.compute()
+    switched = sw.V_results, sw.get_row_status(), sw.get_row_iterations(), sw.get_row_factorizations()
+    # (equal results also show that every row switched: a flat start takes other steps)
+    for a, b in zip(base, switched):
+        np.testing.assert_array_equal(a, b)
