@@ -610,8 +610,10 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
     launch_flops = f_fact * total_factors + f_iter * total_iters
     achieved_tflops = launch_flops / (kernel_ms / 1e3) / 1e12
     fma_peak = 71.4 if args.precision == "mixed" else 37.1
-    # base_chord: the chord sweep, then the single-row sweep for its hand-offs
-    sweep_launches = 2 if strat == lib.REFACTOR_BASE_CHORD else 1
+    # base_chord: the chord sweep (after the outage-compensation setup of
+    # rows that trip branches), then the single-row sweep for its hand-offs
+    has_trips = WORKLOADS[workload][1] in ("n1", "injection_n1")
+    sweep_launches = (3 if has_trips else 2) if strat == lib.REFACTOR_BASE_CHORD else 1
     per_step_launches = sweep_launches + (ls.launches_per_call(n) if learned else 0) + (1 if fallback_rows else 0)
     gname = WORKLOADS[workload][0]
 

@@ -659,8 +659,14 @@ __device__ __forceinline__ void chord_body(const DevPlan& P, const SweepArgs& a,
         __syncthreads();
         const RowEdits ed{s_ne[s], s_ek[s], s_ev[s]};
         bool c = false;
-        if (ed.n > 0 && Minv != nullptr && Vbase != nullptr && !sl[s].masked)
-          c = setup_compensation<T>(P, ed, Y, Vbase, Minv, shs(s));
+        if (ed.n > 0 && Minv != nullptr && Vbase != nullptr && !sl[s].masked) {
+          // the record set up ahead of the sweep, else here
+          const int lc = a.comp_rec != nullptr
+                             ? load_compensation(reinterpret_cast<const CompRec*>(a.comp_rec) + row, s_cr[s],
+                                                 s_cB[s], s_cLU[s], s_cpiv[s])
+                             : -1;
+          c = lc >= 0 ? lc > 0 : setup_compensation<T>(P, ed, Y, Vbase, Minv, shs(s));
+        }
         if (tid == 0) sl[s].comp = c;
         __syncthreads();
         break;

@@ -706,7 +706,8 @@ __device__ __noinline__ double alt_mismatch_norm(const DevPlan P, const RowEdits
 // session (inverse mode of the sweep) -- and W = E^T Z, Woodbury gives
 //   M^-1 F = x0 - Z B (I + W B)^-1 x0[R],   x0 = M0^-1 F.
 // Returns false (no compensation) when the row touches too many positions.
-template <typename T>
+// Run by a CTA of NT threads.
+template <typename T, int NT = BS>
 __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits ed, const double2* Y,
                                                 const double2* Vb, const T* Minv, const RowShared<T> sh) {
   const int tid = threadIdx.x;
@@ -769,7 +770,7 @@ __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits 
   if (r <= 0) return false;
   // C = I + W B, W[a][c] = Z_c[R[a]] = Minv[R[c]][R[a]], one entry per thread
   double* C = sh.s_cLU;
-  for (int q = tid; q < r * r; q += BS) {
+  for (int q = tid; q < r * r; q += NT) {
     const int i2 = q / r, j2 = q % r;
     double acc = i2 == j2 ? 1.0 : 0.0;
     for (int c = 0; c < r; ++c) acc += (double)Minv[(int64_t)R[c] * P.dim + R[i2]] * sh.s_cB[c * r + j2];
@@ -799,6 +800,98 @@ __device__ __noinline__ bool setup_compensation(const DevPlan P, const RowEdits 
   }
   __syncthreads();
   return true;
+}
+
+// A row's outage compensation as setup_compensation leaves it in shared
+// memory, kept in global memory for the chord sweep: every row's record is
+// set up by one launch ahead of the sweep (comp_setup_kernel, all rows in
+// parallel), and the sweep's refill copies the record instead of building it
+// on one thread of the CTA.  Rows touching more than COMP_REC positions
+// (r = COMP_REC_NONE) build theirs in the sweep as before.
+constexpr int COMP_REC = 8;
+constexpr int COMP_REC_NONE = -2;
+struct CompRec {
+  int r;  // compensated positions; <= 0: none; COMP_REC_NONE: set up in the sweep
+  int R[COMP_REC];
+  int piv[COMP_REC];
+  double B[COMP_REC * COMP_REC];   // row-major r x r
+  double LU[COMP_REC * COMP_REC];  // row-major r x r
+};
+
+// One 32-thread CTA per session row: the row's edits as the chord refill
+// takes them (the first MAX_EDITS), setup_compensation (the same arithmetic
+// in the same order, so the record equals what the refill would compute),
+// then the record.
+template <typename T>
+__global__ void __launch_bounds__(32) comp_setup_kernel(const DevPlan P, const SweepArgs a, CompRec* rec) {
+  __shared__ int s_ek[MAX_EDITS];
+  __shared__ double2 s_ev[MAX_EDITS];
+  __shared__ int s_cr[1 + MAX_COMP];
+  __shared__ double s_cB[MAX_COMP * MAX_COMP];
+  __shared__ double s_cLU[MAX_COMP * MAX_COMP];
+  __shared__ int s_cpiv[MAX_COMP];
+  __shared__ int s_ne;
+  const int row = blockIdx.x;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    const int e0 = a.edit_ptr[row], e1 = a.edit_ptr[row + 1];
+    const int ne = min(e1 - e0, MAX_EDITS);
+    for (int e = 0; e < ne; ++e) {
+      s_ek[e] = a.edit_k[e0 + e];
+      s_ev[e] = reinterpret_cast<const double2*>(a.edit_val)[e0 + e];
+    }
+    s_ne = ne;
+  }
+  __syncthreads();
+  CompRec* out = rec + row;
+  if (s_ne == 0) {
+    if (tid == 0) out->r = 0;
+    return;
+  }
+  const RowEdits ed{s_ne, s_ek, s_ev};
+  const RowShared<T> sh{&s_ne, s_ek, s_ev, nullptr, nullptr, nullptr, s_cr, s_cB, s_cLU, s_cpiv, nullptr};
+  const bool c = setup_compensation<T, 32>(P, ed, reinterpret_cast<const double2*>(a.ybus),
+                                           reinterpret_cast<const double2*>(a.base_v),
+                                           reinterpret_cast<const T*>(a.base_inv), sh);
+  const int r = s_cr[0];
+  if (!c) {
+    if (tid == 0) out->r = 0;
+    return;
+  }
+  if (r > COMP_REC) {
+    if (tid == 0) out->r = COMP_REC_NONE;
+    return;
+  }
+  if (tid == 0) out->r = r;
+  for (int q = tid; q < r; q += 32) {
+    out->R[q] = s_cr[1 + q];
+    out->piv[q] = s_cpiv[q];
+  }
+  for (int q = tid; q < r * r; q += 32) {
+    out->B[q] = s_cB[q];
+    out->LU[q] = s_cLU[q];
+  }
+}
+
+// The refill's copy of a record into the slot's shared arrays (every thread
+// of the CTA); returns whether the row is compensated, or -1 when the record
+// says to set it up in the sweep.
+__device__ __forceinline__ int load_compensation(const CompRec* rec, int* s_cr, double* s_cB, double* s_cLU,
+                                                 int* s_cpiv) {
+  const int r = rec->r;
+  if (r == COMP_REC_NONE) return -1;
+  if (r <= 0) return 0;
+  if (threadIdx.x == 0) s_cr[0] = r;
+  for (int q = threadIdx.x; q < r; q += BS) {
+    s_cr[1 + q] = rec->R[q];
+    s_cpiv[q] = rec->piv[q];
+  }
+  for (int q = threadIdx.x; q < r * r; q += BS) {
+    s_cB[q] = rec->B[q];
+    s_cLU[q] = rec->LU[q];
+  }
+  __syncthreads();
+  return 1;
 }
 
 // y <- y - Z B (I + W B)^-1 y[R]  (see setup_compensation)
@@ -1596,6 +1689,19 @@ int chord_ctas(const DevPlan& P, int prec, int device) {
   }
   if (per_sm < 1) per_sm = 1;
   return n_sm * per_sm;
+}
+
+int64_t comp_rec_bytes() { return (int64_t)sizeof(CompRec); }
+
+int launch_comp_setup(const DevPlan& P, const SweepArgs& a, int prec, int n_rows, void* rec, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n_rows <= 0 || rec == nullptr || a.edit_ptr == nullptr || a.base_inv == nullptr || a.base_v == nullptr)
+    return (int)cudaErrorInvalidValue;
+  if (prec == 1)
+    comp_setup_kernel<float><<<n_rows, 32, 0, st>>>(P, a, static_cast<CompRec*>(rec));
+  else
+    comp_setup_kernel<double><<<n_rows, 32, 0, st>>>(P, a, static_cast<CompRec*>(rec));
+  return (int)cudaGetLastError();
 }
 
 int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream) {

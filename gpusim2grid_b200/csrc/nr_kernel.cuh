@@ -115,6 +115,10 @@ struct SweepArgs {
   // complex [n_bus] Y V at alt_v0 on the unedited Ybus, summed over each
   // Ybus row in the order of the sweep's mismatch (nullptr: evaluate in full)
   const double* alt_i;
+  // chord sweep: per-row outage compensation records set up ahead of it by
+  // launch_comp_setup ([n_rows] of comp_rec_bytes(); nullptr: set up in the
+  // sweep)
+  const char* comp_rec;
   int* n_alt_start;
   // chord sweep: Newton steps taken on the shared base factor, summed over rows
   unsigned long long* n_chord_steps;
@@ -194,6 +198,12 @@ int64_t chord_workspace_bytes(const DevPlan& P, int prec);
 int chord_rows_per_cta();
 int chord_ctas(const DevPlan& P, int prec, int device);
 int launch_chord(const DevPlan& P, const SweepArgs& a, int prec, int n_ctas, void* stream);
+// The outage compensation of every row (a.edit_ptr rows 0..n_rows-1) on the
+// base factor (a.base_v, a.base_inv), one small CTA per row, into rec
+// ([n_rows] x comp_rec_bytes()), for the chord sweep that follows on the
+// stream (a.comp_rec).
+int64_t comp_rec_bytes();
+int launch_comp_setup(const DevPlan& P, const SweepArgs& a, int prec, int n_rows, void* rec, void* stream);
 
 // CTAs that fit at once for `prec` (for sizing the workspace).
 int sweep_ctas(int prec, int device);

@@ -92,6 +92,7 @@ struct gs2g_session {
   DevBuf d_ybus, d_vinit, d_sbus, d_basev;
   DevBuf d_bases;  // complex [n_bus] Vb conj(Y Vb): the power the base V draws on the unedited Ybus
   DevBuf d_basei;  // complex [n_bus] Y Vb, summed as the sweep's mismatch sums (fused multiply-adds, row order)
+  DevBuf d_comp;   // per-row outage compensation records of the chord sweep
 
   // branch data
   int n_branch = 0;
@@ -672,6 +673,7 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     n_chord = std::max(1, std::min(n_chord, (n_rows + per - 1) / per));
     cwsb = gs2g::chord_workspace_bytes(s->dplan, o.precision);
     s->d_handoff.ensure((size_t)n_rows * sizeof(int));
+    if (a.edit_ptr != nullptr && a.base_v != nullptr) s->d_comp.ensure((size_t)n_rows * gs2g::comp_rec_bytes());
   }
   s->d_ws.ensure(std::max((size_t)wsb * n_ctas, (size_t)cwsb * n_chord));
   a.queue = s->d_queue.as<int>();
@@ -696,6 +698,12 @@ float launch(gs2g_session* s, const gs2g_run_opts& o, int n_rows, const double* 
     c.n_handoff = s->d_queue.as<int>() + 3;
     c.n_chord_steps = s->d_chord_steps.as<unsigned long long>();
     c.broyden = s->chord == 2;
+    // every row's outage compensation, set up in parallel ahead of the sweep
+    if (a.edit_ptr != nullptr && a.base_v != nullptr) {
+      ck((cudaError_t)gs2g::launch_comp_setup(s->dplan, c, o.precision, n_rows, s->d_comp.p, s->stream),
+         "compensation setup launch");
+      c.comp_rec = s->d_comp.as<char>();
+    }
     ck((cudaError_t)gs2g::launch_chord(s->dplan, c, o.precision, n_chord, s->stream), "chord sweep launch");
     ck(cudaMemsetAsync(s->d_queue.p, 0, sizeof(int), s->stream), "queue reset");
     // how many rows were handed off decides the next launch's shape
