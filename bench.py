@@ -614,7 +614,8 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
     # rows that trip branches), then the single-row sweep for its hand-offs
     has_trips = WORKLOADS[workload][1] in ("n1", "injection_n1")
     sweep_launches = (3 if has_trips else 2) if strat == lib.REFACTOR_BASE_CHORD else 1
-    per_step_launches = sweep_launches + (ls.launches_per_call(n) if learned else 0) + (1 if fallback_rows else 0)
+    per_step_launches = sweep_launches + (ls.launches_per_call(n, sbus_rows=WORKLOADS[workload][1] != "n1")
+                                          if learned else 0) + (1 if fallback_rows else 0)
     gname = WORKLOADS[workload][0]
 
     line = {

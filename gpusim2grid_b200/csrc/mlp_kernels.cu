@@ -414,6 +414,99 @@ __global__ void features_kernel(const double2* __restrict__ sbus_rows, const dou
   }
 }
 
+// First layer of the network for rows whose inputs have no injection part
+// (sbus_rows NULL in features_kernel: outage rows at the base injections).
+// Such a row's standardised input differs from the constant row
+// xb_c = bf16((0 - mean_c) / std_c) only in the columns its tripped branches
+// reach, so X W0^T = base + sum over those columns of
+// (bf16(xs_c) - xb_c) W0[:, c], with base = xb W0^T (first_layer_base_kernel,
+// once per set of weights) and W0T = W0^T [k0 x h] (coalesced over the
+// outputs).  The column values are summed as features_kernel sums them.  A
+// row with more than FEAT_MAX_TERMS contributions computes its full input
+// row in shared memory and the whole dot product instead.  pre [rows_pad x
+// ldp] fp32 (0 in the padding rows, as the GEMM of zero rows gives).
+__global__ void sparse_first_layer_kernel(const float* __restrict__ base, const __nv_bfloat16* __restrict__ w0t,
+                                          int h, const int* __restrict__ trip_ptr, const int* __restrict__ trip_ids,
+                                          const int* __restrict__ br_col, const float* __restrict__ br_val,
+                                          const float* __restrict__ x_mean, const float* __restrict__ x_std,
+                                          int n_in, float* __restrict__ pre, int ldp, int rows) {
+  extern __shared__ float s_x[];  // [n_in]: overflow rows only
+  __shared__ int s_c[FEAT_MAX_TERMS];
+  __shared__ float s_d[FEAT_MAX_TERMS];
+  __shared__ int s_n;
+  const int r = blockIdx.x;
+  float* pr = pre + (int64_t)r * ldp;
+  if (r >= rows) {
+    for (int n = threadIdx.x; n < h; n += blockDim.x) pr[n] = 0.f;
+    return;
+  }
+  const int q0 = trip_ptr[r], q1 = trip_ptr[r + 1];
+  const bool overflow = (q1 - q0) * 4 > FEAT_MAX_TERMS;
+  if (overflow) {
+    // the row's full standardised input (features_kernel's overflow form)
+    for (int c = threadIdx.x; c < n_in; c += blockDim.x) {
+      float v = 0.f;
+      for (int q = q0; q < q1; ++q)
+        for (int k = 0; k < 4; ++k)
+          if (br_col[4 * trip_ids[q] + k] == c) v += br_val[4 * trip_ids[q] + k];
+      s_x[c] = __bfloat162float(__float2bfloat16((v - x_mean[c]) / x_std[c]));
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < h; n += blockDim.x) {
+      float acc = 0.f;
+      for (int c = 0; c < n_in; ++c) acc = fmaf(s_x[c], __bfloat162float(w0t[(int64_t)c * h + n]), acc);
+      pr[n] = acc;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int q = q0; q < q1; ++q) {
+      const int b = trip_ids[q];
+      for (int k = 0; k < 4; ++k) {
+        const int c = br_col[4 * b + k];
+        if (c < 0 || c >= n_in) continue;
+        int e = 0;
+        while (e < n && s_c[e] != c) ++e;
+        if (e == n) {
+          s_c[n] = c;
+          s_d[n] = 0.f;
+          ++n;
+        }
+        s_d[e] += br_val[4 * b + k];
+      }
+    }
+    for (int e = 0; e < n; ++e) {
+      const int c = s_c[e];
+      const float xs = __bfloat162float(__float2bfloat16((s_d[e] - x_mean[c]) / x_std[c]));
+      const float xb = __bfloat162float(__float2bfloat16((0.f - x_mean[c]) / x_std[c]));
+      s_d[e] = xs - xb;
+    }
+    s_n = n;
+  }
+  __syncthreads();
+  const int nt = s_n;
+  for (int n = threadIdx.x; n < h; n += blockDim.x) {
+    float acc = base[n];
+    for (int e = 0; e < nt; ++e) acc = fmaf(s_d[e], __bfloat162float(w0t[(int64_t)s_c[e] * h + n]), acc);
+    pr[n] = acc;
+  }
+}
+
+// base[n] = sum_c bf16((0 - mean_c) / std_c) W0T[c][n] over the n_in input
+// columns (one thread per output, fp32).
+__global__ void first_layer_base_kernel(const __nv_bfloat16* __restrict__ w0t, int h,
+                                        const float* __restrict__ x_mean, const float* __restrict__ x_std, int n_in,
+                                        float* __restrict__ base) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= h) return;
+  float acc = 0.f;
+  for (int c = 0; c < n_in; ++c)
+    acc = fmaf(__bfloat162float(__float2bfloat16((0.f - x_mean[c]) / x_std[c])),
+               __bfloat162float(w0t[(int64_t)c * h + n]), acc);
+  base[n] = acc;
+}
+
 inline int grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   if (b > 148 * 32) b = 148 * 32;
@@ -536,6 +629,34 @@ int gs2g_mlp_features(const double* sbus_rows, const double* sbus_base, const in
   gs2g::mlp::features_kernel<<<rows_pad, 256, 0, (cudaStream_t)stream>>>(
       (const double2*)sbus_rows, (const double2*)sbus_base, pvpq, n_pvpq, pq, n_pq, trip_ptr, trip_ids, br_col,
       br_val, x_mean, x_std, n_in, (__nv_bfloat16*)x_bf16, ldx, rows, n_bus);
+  return status_of(cudaGetLastError());
+}
+
+int gs2g_mlp_first_layer_base(const void* w0t_bf16, int h, const float* x_mean, const float* x_std, int n_in,
+                              float* base, void* stream) {
+  if (h <= 0 || n_in < 0 || !w0t_bf16 || !x_mean || !x_std || !base) return invalid("first_layer_base: bad arguments");
+  gs2g::mlp::first_layer_base_kernel<<<(h + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16*)w0t_bf16, h, x_mean, x_std, n_in, base);
+  return status_of(cudaGetLastError());
+}
+
+int gs2g_mlp_sparse_first_layer(const float* base, const void* w0t_bf16, int h, const int* trip_ptr,
+                                const int* trip_ids, const int* br_col, const float* br_val, const float* x_mean,
+                                const float* x_std, int n_in, float* pre, int ldp, int rows, int rows_pad,
+                                void* stream) {
+  if (h <= 0 || ldp < h || rows < 0 || rows_pad < rows || n_in < 0 || !base || !w0t_bf16 || !trip_ptr ||
+      !trip_ids || !br_col || !br_val || !x_mean || !x_std || !pre)
+    return invalid("sparse_first_layer: bad arguments");
+  if (rows_pad == 0) return 0;
+  const int smem = n_in * (int)sizeof(float);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(gs2g::mlp::sparse_first_layer_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return status_of(e);
+  }
+  gs2g::mlp::sparse_first_layer_kernel<<<rows_pad, 256, smem, (cudaStream_t)stream>>>(
+      base, (const __nv_bfloat16*)w0t_bf16, h, trip_ptr, trip_ids, br_col, br_val, x_mean, x_std, n_in, pre, ldp,
+      rows);
   return status_of(cudaGetLastError());
 }
 

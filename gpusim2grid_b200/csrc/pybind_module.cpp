@@ -561,6 +561,19 @@ void bind_mlp(py::module_& m) {
                             P<const float>(br_val), P<const float>(x_mean), P<const float>(x_std), n_in, P<void>(x),
                             ldx, rows, rows_pad, n_bus, S(stream)));
   });
+  mm.def("first_layer_base", [](uintptr_t w0t, int h, uintptr_t x_mean, uintptr_t x_std, int n_in, uintptr_t base,
+                                uintptr_t stream) {
+    check(gs2g_mlp_first_layer_base(P<const void>(w0t), h, P<const float>(x_mean), P<const float>(x_std), n_in,
+                                    P<float>(base), S(stream)));
+  });
+  mm.def("sparse_first_layer", [](uintptr_t base, uintptr_t w0t, int h, uintptr_t trip_ptr, uintptr_t trip_ids,
+                                  uintptr_t br_col, uintptr_t br_val, uintptr_t x_mean, uintptr_t x_std, int n_in,
+                                  uintptr_t pre, int ldp, int rows, int rows_pad, uintptr_t stream) {
+    check(gs2g_mlp_sparse_first_layer(P<const float>(base), P<const void>(w0t), h, P<const int>(trip_ptr),
+                                      P<const int>(trip_ids), P<const int>(br_col), P<const float>(br_val),
+                                      P<const float>(x_mean), P<const float>(x_std), n_in, P<float>(pre), ldp, rows,
+                                      rows_pad, S(stream)));
+  });
   mm.def("start_voltages", [](uintptr_t y, int ldy, uintptr_t ymean, uintptr_t ystd, uintptr_t ia, uintptr_t im,
                               uintptr_t vinit, int n_bus, uintptr_t v0, int rows, uintptr_t stream) {
     check(gs2g_mlp_start_voltages(P<float>(y), ldy, P<float>(ymean), P<float>(ystd), P<int>(ia), P<int>(im),

@@ -97,6 +97,8 @@ class WarmStartMLP:
         self.y_mean = torch.zeros(self.n_out, dtype=torch.float32, device=dev)
         self.y_std = torch.ones(self.n_out, dtype=torch.float32, device=dev)
         self._ws = {}
+        self._stats_ver = 0
+        self._sparse = (None, None)
 
     # -------------------------------------------------------------- params
     def _view(self, buf, l, bias):
@@ -123,6 +125,7 @@ class WarmStartMLP:
         f = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float32), device=self.device)
         self.x_mean, self.x_std = f(x_mean), torch.clamp(f(np.nan_to_num(x_std, nan=1.0)), min=floor)
         self.y_mean, self.y_std = f(y_mean), torch.clamp(f(np.nan_to_num(y_std, nan=1.0)), min=floor)
+        self._stats_ver += 1
 
     # ------------------------------------------------------------- buffers
     def device_inputs(self, F):
@@ -173,19 +176,66 @@ class WarmStartMLP:
         return self._view(self.wb, l, False)
 
     def _forward(self, X, w):
-        a = X
+        self._gemm(X, self._wb(0), w["pre"][0])
+        return self._forward_rest(w, X.shape[0])
+
+    def _forward_rest(self, w, B):
+        """The network from the first layer's pre-activations w['pre'][0]
+        (B rows) to its outputs w['y']."""
         L = self.layers
         for l in range(L + 1):
+            if l > 0:
+                self._gemm(w["act"][l - 1], self._wb(l), w["pre"][l] if l < L else w["y"])
             if l < L:
-                self._gemm(a, self._wb(l), w["pre"][l])
                 _M.bias_act(w["pre"][l].data_ptr(), self.h, self.b(l).data_ptr(), w["act"][l].data_ptr(), self.h,
-                            X.shape[0], self.h, True, _stream())
-                a = w["act"][l]
+                            B, self.h, True, _stream())
             else:
-                self._gemm(a, self._wb(l), w["y"])
-                _M.bias_act(w["y"].data_ptr(), self.o, self.b(l).data_ptr(), 0, self.o, X.shape[0], self.o, False,
+                _M.bias_act(w["y"].data_ptr(), self.o, self.b(l).data_ptr(), 0, self.o, B, self.o, False,
                             _stream())
         return w["y"]
+
+    def _sparse_first(self):
+        """(W0T, base) of the current first-layer weights and input
+        standardisation: W0^T [k0 x h] bf16 and the first layer's product
+        with an all-zero raw input row (gs2g_mlp_first_layer_base); rebuilt
+        after a training step or new statistics."""
+        key = (self.step, self._stats_ver)
+        if self._sparse[0] != key:
+            W0 = self._wb(0)
+            W0T = torch.empty(self.k0, self.h, dtype=torch.bfloat16, device=self.device)
+            _M.transpose_bf16(W0.data_ptr(), W0.stride(0), W0T.data_ptr(), W0T.stride(0), self.h, self.k0, _stream())
+            base = torch.empty(self.h, dtype=torch.float32, device=self.device)
+            _M.first_layer_base(W0T.data_ptr(), self.h, self.x_mean.data_ptr(), self.x_std.data_ptr(), self.n_in,
+                                base.data_ptr(), _stream())
+            self._sparse = (key, (W0T, base))
+        return self._sparse[1]
+
+    def predict_trips(self, trip_ptr, trip_ids, br_cols, br_vals, n_rows, chunk=16384):
+        """Standardised outputs (rows padded to 128, o) fp32 of rows whose raw
+        inputs are only their tripped branches' contributions (no injection
+        part; device int32 CSR trip_ptr / trip_ids, the per-branch columns
+        and values of ``LearnedStart``): the first layer from those few
+        columns (gs2g_mlp_sparse_first_layer), the other layers on the GEMM.
+        Equals ``predict`` of the same rows' inputs up to the fp32 summation
+        order of the first layer."""
+        W0T, base = self._sparse_first()
+        rp = _ceil(max(int(n_rows), 1), 128)
+        out = None
+        for r0 in range(0, rp, chunk):
+            B = min(chunk, rp - r0)
+            w = self._buffers(B, False)
+            rows = max(0, min(B, int(n_rows) - r0))
+            _M.sparse_first_layer(base.data_ptr(), W0T.data_ptr(), self.h, trip_ptr.data_ptr() + 4 * r0,
+                                  trip_ids.data_ptr(), br_cols.data_ptr(), br_vals.data_ptr(), self.x_mean.data_ptr(),
+                                  self.x_std.data_ptr(), self.n_in, w["pre"][0].data_ptr(), self.h, rows, B,
+                                  _stream())
+            y = self._forward_rest(w, B)
+            if rp <= chunk:
+                return y
+            if out is None:
+                out = torch.empty(rp, self.o, dtype=torch.float32, device=self.device)
+            out[r0:r0 + B].copy_(y)
+        return out
 
     def _backward(self, X, T, w, scale):
         """Gradients of 0.5 * scale * ||y - T||^2 over the valid columns into
@@ -376,10 +426,14 @@ class LearnedStart:
     ``grid`` is the synthetic ``Grid`` (array tuple + branch data).  ``train``
     generates and solves training rows on the GPU and fits the network;
     ``start_voltages`` turns row definitions (injections, tripped branches)
-    into V0 on the device."""
+    into V0 on the device.  ``sparse_first_layer`` (default on): rows
+    without injection part take the network's first layer from the few input
+    columns their tripped branches reach (``WarmStartMLP.predict_trips``)
+    instead of the dense input block and its GEMM."""
 
     def __init__(self, grid, hidden=1024, layers=2, device=None, seed=0):
         self.grid = grid
+        self.sparse_first_layer = True
         d = grid_arrays(grid.as_tuple())
         self._d = d
         n = d["n_bus"]
@@ -551,8 +605,16 @@ class LearnedStart:
         torch's current stream.  With ``out_ptr`` (a device address of rows x
         n_bus complex128, e.g. a session's ``start_rows_buffer``) V0 is
         written there and None is returned."""
-        X, R = self.inputs(sbus_rows, trips, n_rows)
-        y = self.net.predict(X)
+        if sbus_rows is None and trips is not None and self.sparse_first_layer:
+            # outage rows at the base injections: the first layer from the
+            # few input columns their tripped branches reach
+            R = int(n_rows) if n_rows is not None else (
+                len(trips[0]) - 1 if isinstance(trips, tuple) else len(trips))
+            tp, ti = self._device_trips(trips)
+            y = self.net.predict_trips(tp, ti, self._br_cols32, self._br_vals32, R)
+        else:
+            X, R = self.inputs(sbus_rows, trips, n_rows)
+            y = self.net.predict(X)
         V0 = None
         if out_ptr is None:
             V0 = torch.empty(R, self._d["n_bus"], dtype=torch.complex128, device=self.device)
@@ -562,9 +624,13 @@ class LearnedStart:
                           int(out_ptr), R, _stream())
         return V0
 
-    def launches_per_call(self, n_rows):
+    def launches_per_call(self, n_rows, sbus_rows=True):
         """Kernels of this library one ``start_voltages`` call launches: the
         fused inputs, a GEMM and a bias/activation per layer and chunk, the
-        start voltages."""
+        start voltages; without injection rows (``sbus_rows`` False) the
+        first layer's sparse product replaces the inputs and the first GEMM
+        (per chunk)."""
         chunks = max(1, -(-_ceil(max(n_rows, 1), 128) // 16384))
+        if not sbus_rows and self.sparse_first_layer:
+            return (2 * self.net.layers + 1) * chunks + 1
         return 2 * (self.net.layers + 1) * chunks + 2

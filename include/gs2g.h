@@ -421,6 +421,23 @@ int gs2g_mlp_features(const double* sbus_rows, const double* sbus_base, const in
                       int n_pq, const int* trip_ptr, const int* trip_ids, const int* br_col, const float* br_val,
                       const float* x_mean, const float* x_std, int n_in, void* x_bf16, int ldx, int rows,
                       int rows_pad, int n_bus, void* stream);
+/* The first layer's pre-activations for rows without injection part
+ * (gs2g_mlp_features with sbus_rows NULL), from the few input columns their
+ * tripped branches reach: pre[r] = base + sum over those columns c of
+ * (bf16(xs_c) - bf16(-x_mean_c / x_std_c)) * W0T[c], the column values
+ * summed as gs2g_mlp_features sums them; pre [rows_pad x ldp] fp32, 0 in
+ * the padding rows.  W0T = W0^T (bf16, [n_in x h] row-major; W0 is the
+ * first layer's [h x k0] weight) and base = gs2g_mlp_first_layer_base of the
+ * same weights.  Equals X W0^T of the standardised inputs up to fp32
+ * summation order.  (The reference has no network; no counterpart.) */
+int gs2g_mlp_sparse_first_layer(const float* base, const void* w0t_bf16, int h, const int* trip_ptr,
+                                const int* trip_ids, const int* br_col, const float* br_val, const float* x_mean,
+                                const float* x_std, int n_in, float* pre, int ldp, int rows, int rows_pad,
+                                void* stream);
+/* base[h] = sum over the n_in input columns of bf16(-x_mean_c / x_std_c) *
+ * W0T[c] (the first layer's product with an all-zero raw input row). */
+int gs2g_mlp_first_layer_base(const void* w0t_bf16, int h, const float* x_mean, const float* x_std, int n_in,
+                              float* base, void* stream);
 /* Start voltages from the network's standardised outputs y[rows x ldy]:
  * bus b takes Va = y[va_index[b]] * y_std + y_mean when va_index[b] >= 0
  * (pv and pq buses), else the angle of vinit[b]; Vm likewise through

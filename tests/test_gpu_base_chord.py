@@ -206,3 +206,31 @@ def test_start_switch_equals_base_start(kind):
     # (equal results also show that every row switched: a flat start takes other steps)
     for a, b in zip(base, switched):
         np.testing.assert_array_equal(a, b)
+
+
+def test_compensation_records_and_in_sweep_setup_reach_fp64_solutions():
+    """Rows tripping up to four branches: a row touching at most 8 Jacobian
+    positions takes its outage compensation from the records set up ahead of
+    the chord sweep, a larger one sets it up in the sweep, and beyond 16
+    positions a row steps uncompensated until it leaves the chord.  Every
+    row must reach the plain FP64 flat-start solution."""
+    from gpusim2grid_b200.synthetic import grid_by_name, scenario_outages
+    g = grid_by_name("case2000_synth", 0)
+    n = 512
+    p, q = injection_scenarios(g, n, seed=61)
+    trips = scenario_outages(g, n, max_trips=4, seed=62)
+    assert max(len(t) for t in trips) == 4
+    out = []
+    for precision, strategy, start in (("fp64", "refactor_every", "flat"), ("mixed", "base_chord", "base")):
+        sw = ScenarioSweepGPU(g.as_tuple(), init_from_n_powerflow=False, precision=precision, nb_iter=10,
+                              scheduling="continuous", tol=1e-8, start=start, strategy=strategy)
+        sw.set_branch_data(*g.branch_data())
+        sw.set_injections(p, q, g.sn_mva)
+        sw.set_topology(trips)
+        sw.compute()
+        out.append(sw)
+    ref, bc = out
+    np.testing.assert_array_equal(bc.get_row_status(), ref.get_row_status())
+    ok = ref.get_row_status() == RowStatus.CONVERGED
+    assert ok.sum() > 0.9 * n
+    assert np.abs(bc.V_results[ok] - ref.V_results[ok]).max() < TOL_V_MIXED

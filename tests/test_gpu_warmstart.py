@@ -141,3 +141,32 @@ def test_given_start_worse_than_base_begins_from_base(g118):
     np.testing.assert_array_equal(sw.get_row_iterations()[::2], base.get_row_iterations()[::2])
     assert np.all(sw.get_row_iterations()[1::2] <= 1)
     assert np.abs(sw.V_results - base.V_results).max() < TOL_V_MIXED
+
+
+def test_sparse_first_layer_equals_the_gemm(g118, learned118):
+    """Rows without injection part (outage rows at the base injections) take
+    the network's first layer from the few input columns their tripped
+    branches reach.  Its pre-activations must equal the GEMM of the full
+    standardised inputs up to fp32 summation order: rows with one trip,
+    rows with three, an empty row, and a row with more contributions than
+    the kernel's shared list holds (the full dot product in the CTA).  The
+    start voltages then agree to the bf16 activations' precision."""
+    ls = learned118
+    net = ls.net
+    rng = np.random.default_rng(7)
+    trips = ([[int(b)] for b in n1_branches(g118)[:40]]
+             + [sorted(int(b) for b in rng.choice(g118.n_branch, 3, replace=False)) for _ in range(20)]
+             + [list(range(70)), []])
+    n = len(trips)
+    X, _ = ls.inputs(None, trips, n)
+    net.predict(X)
+    dense = net._buffers(X.shape[0], False)["pre"][0][:n].clone()
+    tp, ti = ls._device_trips(trips)
+    net.predict_trips(tp, ti, ls._br_cols32, ls._br_vals32, n)
+    sparse = net._buffers(X.shape[0], False)["pre"][0][:n].clone()
+    assert float((sparse - dense).abs().max()) <= 1e-3 * float(dense.abs().max())
+    ls.sparse_first_layer = False
+    v_dense = ls.start_voltages(None, trips, n).cpu().numpy()
+    ls.sparse_first_layer = True
+    v_sparse = ls.start_voltages(None, trips, n).cpu().numpy()
+    assert np.abs(v_sparse - v_dense).max() < 1e-2
