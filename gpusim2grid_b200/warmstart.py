@@ -628,9 +628,9 @@ class LearnedStart:
         """Kernels of this library one ``start_voltages`` call launches: the
         fused inputs, a GEMM and a bias/activation per layer and chunk, the
         start voltages; without injection rows (``sbus_rows`` False) the
-        first layer's sparse product replaces the inputs and the first GEMM
-        (per chunk)."""
+        first layer's sparse product (per chunk) replaces the inputs and the
+        first GEMM."""
         chunks = max(1, -(-_ceil(max(n_rows, 1), 128) // 16384))
         if not sbus_rows and self.sparse_first_layer:
-            return (2 * self.net.layers + 1) * chunks + 1
+            return (2 * self.net.layers + 2) * chunks + 1
         return 2 * (self.net.layers + 1) * chunks + 2
