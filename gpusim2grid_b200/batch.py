@@ -43,7 +43,8 @@ _STRATEGY = {"refactor_every": lib.REFACTOR_EVERY, "adaptive": lib.REFACTOR_ADAP
 def _rows_csr(branch_ids_per_row):
     """(rows, ptr, ids) of branch-id lists, each row's duplicates dropped
     (first occurrence kept).  Rows of one id each (the N-1 case), given as
-    lists or as an integer array, take a vectorised path."""
+    lists or as an integer array, take a vectorised path (rows None: the
+    CSR is the only copy)."""
     if isinstance(branch_ids_per_row, np.ndarray) and branch_ids_per_row.ndim == 2 and \
             branch_ids_per_row.shape[1] == 1:
         flat = np.ascontiguousarray(branch_ids_per_row[:, 0], dtype=np.int32)
@@ -54,7 +55,7 @@ def _rows_csr(branch_ids_per_row):
         ptr, ids = _ids_csr(rows)
         return rows, ptr, ids
     ptr = np.arange(flat.size + 1, dtype=np.int32)
-    return flat[:, None].tolist(), ptr, flat
+    return None, ptr, flat
 
 
 def _ids_csr(rows):
@@ -249,8 +250,9 @@ class _BatchSweep:
 
     @property
     def warm_report(self):
-        """Timings of the last learned start: predict_ms (features, network
-        and V0 on the device, wall), n_rescued (rows restarted), n_base_start
+        """Timings of the last learned start: predict_ms (host time to
+        enqueue the network and V0; the device runs them ahead of the sweep
+        on the same stream order), n_rescued (rows restarted), n_base_start
         (rows that began from the base case: its mismatch was the smaller)."""
         return dict(self._warm)
 
@@ -377,16 +379,17 @@ class _BatchSweep:
             import torch
             sbus, trips, n = self._device_row_defs()
             # V0 is written in place into the session's start-row buffer on
-            # torch's stream, which must be done before the session's launch
+            # torch's stream; the session stream waits for it on the device
+            # (no host synchronisation between the network and the sweep)
             self._learned.start_voltages(sbus, trips, n, out_ptr=self._s.start_rows_buffer(n))
-            torch.cuda.current_stream().synchronize()
-            self._learned.net.check()
+            self._s.wait_stream(torch.cuda.current_stream().cuda_stream)
             self._warm = dict(predict_ms=(time.perf_counter() - t0) * 1e3)
             ratio, reuse = self._learned_opts
         self._s.run(self.nb_iter, self.tol, fixed, self._prec, _START[self._start], 0.0, n_ctas, False,
                     _STRATEGY[self._strategy], ratio, reuse, rescue, self.nb_iter_per_round, **self._scaling_kw())
         tm = self._s.timings()
         if self._start == "learned":
+            self._learned.net.check()  # the network's GEMMs finished before the sweep (stream order)
             self._warm["n_rescued"] = int(tm["n_rescued"])
             self._warm["n_base_start"] = int(tm["n_base_start"])
         kernel_ms = tm["kernel_ms"]
@@ -537,6 +540,7 @@ class ContingencyAnalysisGPU(_BatchSweep):
     def __init__(self, grid, **kw):
         super().__init__(grid, **kw)
         self._ctg = []
+        self._ctg_csr = (np.zeros(1, dtype=np.int32), np.zeros(0, dtype=np.int32))
 
     def add_contingencies_by_branch_id(self, branch_ids_per_ctg):
         """One inner list per contingency (branch indices; a branch named twice
@@ -545,21 +549,24 @@ class ContingencyAnalysisGPU(_BatchSweep):
             raise RuntimeError("set_branch_data() must be called before add_contingencies_by_branch_id()")
         rows, ptr, ids = _rows_csr(branch_ids_per_ctg)
         self._s.set_contingencies(ptr, ids)
-        self._ctg = rows
+        self._ctg = rows  # None for single-branch rows: built from the CSR when asked for
         self._ctg_csr = (ptr, ids)
 
     def get_contingencies(self):
+        if self._ctg is None:
+            ptr, ids = self._ctg_csr
+            return [ids[ptr[r]:ptr[r + 1]].tolist() for r in range(len(ptr) - 1)]
         return [list(r) for r in self._ctg]
 
     def _row_defs(self):
-        return None, self._ctg_csr, len(self._ctg)
+        return None, self._ctg_csr, len(self._ctg_csr[0]) - 1
 
     def _rows_have_trips(self):
         return True
 
     @property
     def n_contingencies(self):
-        return len(self._ctg)
+        return len(self._ctg_csr[0]) - 1
 
 
 class InjectionSweepGPU(_BatchSweep):
@@ -607,24 +614,31 @@ class ScenarioSweepGPU(InjectionSweepGPU):
 
     def __init__(self, grid, **kw):
         super().__init__(grid, **kw)
-        self._topo = None
+        self._topo_csr = None
 
     def set_topology(self, branch_ids_per_scenario):
         if self._n_branches is None:
             raise RuntimeError("set_branch_data() must be called before set_topology()")
-        rows, ptr, ids = _rows_csr(branch_ids_per_scenario)
+        _, ptr, ids = _rows_csr(branch_ids_per_scenario)
         self._s.set_contingencies(ptr, ids)
-        self._topo = rows
         self._topo_csr = (ptr, ids)
 
     def _row_defs(self):
         if self._inj is None:
             raise RuntimeError("set_injections() must be called before compute()")
         p, q, sn = self._inj
-        return (p + 1j * q) / sn, (self._topo_csr if self._topo is not None else None), self._n_scen
+        return (p + 1j * q) / sn, self._topo_csr, self._n_scen
+
+    def get_topology(self):
+        """The tripped branch ids of every scenario row (``set_topology``,
+        duplicates dropped), or None without a topology."""
+        if self._topo_csr is None:
+            return None
+        ptr, ids = self._topo_csr
+        return [ids[ptr[r]:ptr[r + 1]].tolist() for r in range(len(ptr) - 1)]
 
     def _rows_have_trips(self):
-        return self._topo is not None
+        return self._topo_csr is not None
 
     def get_disconnected(self):
         """(n_rows,) int: 1 for a row whose topology islands the grid and was
@@ -662,14 +676,17 @@ def compute_many(sweeps, batch_size=0):
         for f in sweeps:
             sbus, trips, n = f._device_row_defs()
             f._learned.start_voltages(sbus, trips, n, out_ptr=f._s.start_rows_buffer(n))
-        torch.cuda.current_stream().synchronize()
+        # every session stream waits for the networks on the device
         for f in sweeps:
-            f._learned.net.check()
+            f._s.wait_stream(torch.cuda.current_stream().cuda_stream)
         ratio, reuse = f0._learned_opts
     lib.run_multi([f._s for f in sweeps], f0.nb_iter, f0.tol, f0.scheduling == "chunked", f0._prec, _START[start],
                   0.0, max(int(batch_size), 0), False, _STRATEGY[f0._strategy], ratio, reuse,
                   start in ("rows", "learned"), f0.nb_iter_per_round, **f0._scaling_kw())
     kernel_ms = sweeps[0]._s.timings()["kernel_ms"]
+    if start == "learned":
+        for f in sweeps:
+            f._learned.net.check()
     for f in sweeps:
         f._ran = True
         kernel_ms += f.fp64_fallback()

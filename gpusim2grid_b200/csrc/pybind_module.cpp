@@ -435,6 +435,7 @@ class Session {
   }
 
   void sync() { check(gs2g_sync(h())); }
+  void wait_stream(uintptr_t stream) { check(gs2g_session_wait_stream(h(), reinterpret_cast<void*>(stream))); }
 
  private:
   gs2g_session* s_ = nullptr;
@@ -652,5 +653,6 @@ PYBIND11_MODULE(_gs2g, m) {
       .def("dlpack", &Session::dlpack)
       .def("device_rows", &Session::device_rows)
       .def("timings", &Session::timings)
-      .def("sync", &Session::sync);
+      .def("sync", &Session::sync)
+      .def("wait_stream", &Session::wait_stream, py::arg("stream"));
 }

@@ -81,6 +81,7 @@ struct gs2g_session {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_ext = nullptr;  // work of another stream the session stream waits for
   gs2g::Plan plan;
   gs2g::DevPlan dplan{};
   std::vector<int> y_ip, y_ix, pv, pq;  // canonical pattern and bus sets, for re-planning
@@ -957,6 +958,7 @@ int gs2g_session_destroy(gs2g_session* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->ev_ext) cudaEventDestroy(s->ev_ext);
     for (cudaEvent_t e : s->ev_stage)
       if (e) cudaEventDestroy(e);
     if (s->h_stage) cudaFreeHost(s->h_stage);
@@ -1966,6 +1968,16 @@ int gs2g_sync(gs2g_session* s) {
   if (!s) throw std::invalid_argument("NULL session");
   DeviceGuard g(s->device);
   ck(cudaStreamSynchronize(s->stream), "sync");
+  GS2G_CATCH
+}
+
+int gs2g_session_wait_stream(gs2g_session* s, void* stream) {
+  GS2G_TRY
+  if (!s) throw std::invalid_argument("NULL session");
+  DeviceGuard g(s->device);
+  if (!s->ev_ext) ck(cudaEventCreateWithFlags(&s->ev_ext, cudaEventDisableTiming), "event");
+  ck(cudaEventRecord(s->ev_ext, static_cast<cudaStream_t>(stream)), "record the other stream");
+  ck(cudaStreamWaitEvent(s->stream, s->ev_ext, 0), "wait for the other stream");
   GS2G_CATCH
 }
 

@@ -245,7 +245,8 @@ int gs2g_set_start_rows_device(gs2g_session* s, int n_rows, const double* v0_dev
  * device, for callers that compute start voltages on the GPU and write them
  * in place (no copy).  Sizes the buffer and records n_rows start rows; its
  * contents are used by the next GS2G_START_ROWS run, so the caller's writes
- * must be complete (its stream synchronised) before gs2g_run.  Valid until
+ * must be complete (its stream synchronised, or ordered before the session
+ * stream by gs2g_session_wait_stream) before gs2g_run.  Valid until
  * the next call that sets start rows or destroy. */
 int gs2g_start_rows_buffer(gs2g_session* s, int n_rows, double** v0_dev);
 /* Replace the base injections (single-solve resolve). */
@@ -336,6 +337,12 @@ int gs2g_get_device_rows(gs2g_session* s, int* n_rows, const double** sbus_rows,
 int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
 /* Synchronise the session stream. */
 int gs2g_sync(gs2g_session* s);
+/* Order the session stream after the work enqueued so far on `stream` (NULL:
+ * the legacy default stream) on the device, without a host
+ * synchronisation: e.g. start voltages written into gs2g_start_rows_buffer
+ * by a network on the caller's stream, then gs2g_run.  (The reference
+ * synchronises instead; no counterpart.) */
+int gs2g_session_wait_stream(gs2g_session* s, void* stream);
 
 /* Allocation-free batch solve.  No counterpart in the reference: this entry
  * point exists for callers that must not allocate device memory while they
