@@ -665,8 +665,8 @@ def measure(args, workload, steps, warmup, train_rows, rows_limit=0, e2e=True):
     return line, (g, trips, p, q)
 
 
-# the driver-visible second configuration of the default line: the 6500-bus
-# injection sweep (the north star's ">= 3x" names it beside the N-1 sweep)
+# the second workload of the default line: the 6500-bus injection sweep
+# (its speed-up over plain FP64 is reported beside the N-1 sweep's)
 CFG2 = "injection_sweep_case6500_synth"
 CFG2_KEYS = ("value", "ms_per_step", "rows_converged", "rows_counted", "newton_iters_total", "lu_factorizations_total",
              "rows_fp64_fallback", "ms_split", "fp64_flat_value", "speedup_vs_fp64_flat", "mixed_flat_value",

@@ -79,7 +79,7 @@ def grid_arrays(grid):
     slack_weights, pv, pq)``.  Returns a dict of canonical arrays."""
     if not isinstance(grid, (tuple, list)) or len(grid) != 7:
         raise ValueError("grid must be the array tuple (Ybus, Vinit, Sbus, slack_ids, slack_weights, pv, pq); "
-                         "lightsim2grid grids are not supported by this build")
+                         "lightsim2grid grid objects are not accepted (pass their array tuple)")
     Ybus, Vinit, Sbus, slack_ids, slack_weights, pv, pq = grid
     Y = sp.csr_matrix(Ybus, dtype=np.complex128)
     Y.sum_duplicates()

@@ -393,7 +393,7 @@ class _BatchSweep:
             self._warm["n_rescued"] = int(tm["n_rescued"])
             self._warm["n_base_start"] = int(tm["n_base_start"])
         kernel_ms = tm["kernel_ms"]
-        kernel_ms += self.fp64_fallback(n_ctas)
+        kernel_ms += self.fp64_fallback(n_ctas, tm["n_failed"])
         tm = dict(tm, kernel_ms=kernel_ms)
         self._timings = BatchTimings(n_rows=self._s.n_rows(), total_iters=int(tm["total_iters"]),
                                      t_plan_ms=tm["plan_ms"], t_upload_ms=tm["upload_ms"],
@@ -401,12 +401,15 @@ class _BatchSweep:
         self._ran = True
         self._host = None
 
-    def fp64_fallback(self, n_ctas=0):
+    def fp64_fallback(self, n_ctas=0, n_failed=None):
         """Re-solve, in plain FP64 from Vinit, the rows a mixed-precision
-        continuous run left MAX_ITER or DIVERGED (the north star's "flat-start
-        FP64 NR remains the fallback").  Returns its kernel ms."""
+        continuous run left MAX_ITER or DIVERGED (the flat-start FP64 NR
+        remains the fallback).  ``n_failed``: those rows' count when the
+        caller has read the timings already.  Returns its kernel ms."""
         self._fallback_rows = 0
         if self.fallback != "fp64" or self._prec != lib.PREC_MIXED or self.scheduling != "continuous":
+            return 0.0
+        if (self._s.timings()["n_failed"] if n_failed is None else n_failed) == 0:
             return 0.0
         import torch
         st = torch.from_dlpack(self._s.dlpack("status"))

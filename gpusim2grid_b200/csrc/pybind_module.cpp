@@ -431,6 +431,7 @@ class Session {
     d["chord_steps"] = t.chord_steps;
     d["base_setup_ms"] = t.base_setup_ms;
     d["base_setup_bytes"] = t.base_setup_bytes;
+    d["n_failed"] = t.n_failed;
     return d;
   }
 

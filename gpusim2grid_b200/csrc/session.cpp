@@ -18,7 +18,6 @@
 #include <condition_variable>
 #include <cstring>
 #include <functional>
-#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -441,6 +440,7 @@ void assemble_rows(gs2g_session* s) {
     bool any_skip = false;
     std::vector<int> mptr(nr + 1, 0), mbus;  // masked buses per row (handle_disconnected)
     std::vector<int> comp_size, comp_min;
+    std::vector<std::pair<int, std::complex<double>>> acc;
     for (int r = 0; r < nr; ++r) {
       uniq.assign(s->ctg_ids.begin() + s->ctg_ptr[r], s->ctg_ids.begin() + s->ctg_ptr[r + 1]);
       std::sort(uniq.begin(), uniq.end());
@@ -507,15 +507,24 @@ void assemble_rows(gs2g_session* s) {
         }
       }
       mptr[r + 1] = (int)mbus.size();
-      std::map<int, std::complex<double>> acc;
+      // one edit per Ybus position the trips touch, in position order, the
+      // trips' terms summed in trip and term order (from zero)
+      acc.clear();
       for (int l : uniq) {
         const double* v[4] = {&s->yff[2 * l], &s->ytt[2 * l], &s->yft[2 * l], &s->ytf[2 * l]};
         const int kk[4] = {s->k_ff[l], s->k_tt[l], s->k_ft[l], s->k_tf[l]};
         // an open endpoint has no Ybus row or column: its terms are skipped
         // (contingency_analysis_helper.cpp:53-75)
-        for (int q = 0; q < 4; ++q)
-          if (kk[q] >= 0) acc[kk[q]] += std::complex<double>(v[q][0], v[q][1]);
+        for (int q = 0; q < 4; ++q) {
+          if (kk[q] < 0) continue;
+          const std::complex<double> t(v[q][0], v[q][1]);
+          size_t e = 0;
+          while (e < acc.size() && acc[e].first != kk[q]) ++e;
+          if (e == acc.size()) acc.emplace_back(kk[q], std::complex<double>(0.0, 0.0) + t);
+          else acc[e].second += t;
+        }
       }
+      std::sort(acc.begin(), acc.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
       if ((int)acc.size() > kMaxEdits)
         throw std::invalid_argument("row " + std::to_string(r) + " trips too many branches (" +
                                     std::to_string(acc.size()) + " Ybus edits > " + std::to_string(kMaxEdits) + ")");
@@ -1952,13 +1961,17 @@ int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out) {
   GS2G_TRY
   if (!s || !out) throw std::invalid_argument("NULL argument");
   *out = s->tm;
+  out->n_failed = 0;
   if (s->last_rows_run > 0) {
     DeviceGuard g(s->device);
-    std::vector<int> it(s->last_rows_run);
+    std::vector<int> it(s->last_rows_run), st(s->last_rows_run);
     ck(cudaMemcpy(it.data(), s->d_iters.p, it.size() * sizeof(int), cudaMemcpyDeviceToHost), "read iters");
-    int64_t tot = 0;
+    ck(cudaMemcpy(st.data(), s->d_status.p, st.size() * sizeof(int), cudaMemcpyDeviceToHost), "read statuses");
+    int64_t tot = 0, failed = 0;
     for (int v : it) tot += v;
+    for (int v : st) failed += v == GS2G_ROW_MAX_ITER || v == GS2G_ROW_DIVERGED;
     out->total_iters = tot;
+    out->n_failed = failed;
   }
   GS2G_CATCH
 }

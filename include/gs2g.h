@@ -159,6 +159,9 @@ typedef struct gs2g_timings {
    * wall ms and the device bytes it holds */
   double base_setup_ms;
   int64_t base_setup_bytes;
+  /* rows of the last run (gs2g_run_subset re-solves included) whose status
+   * is MAX_ITER or DIVERGED, counted when the timings are read */
+  int64_t n_failed;
 } gs2g_timings;
 
 const char* gs2g_last_error(void);

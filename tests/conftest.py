@@ -58,6 +58,6 @@ def g6500():
 # tolerances: FP64 engine vs FP64 oracle (same algorithm, different sparse LU
 # and summation order); mixed precision converges to the same 1e-8 mismatch,
 # so its voltages differ from the FP64 oracle by at most the Newton error
-# left at that mismatch.  The north-star bar is |dV| <= 1e-6 pu.
+# left at that mismatch.  The agreement bar is |dV| <= 1e-6 pu.
 TOL_V_FP64 = 1e-9
 TOL_V_MIXED = 1e-6
