@@ -121,6 +121,7 @@ struct gs2g_session {
   int n_start = 0;
   DevBuf d_v0rows;
   bool rows_dirty = true;
+  bool edits_dirty = true;  // the rows' Ybus edits, masks, skips and order still to build
 
   // assembled rows on the device
   int n_rows = 0;
@@ -409,30 +410,42 @@ void order_rows(gs2g_session* s, int nr) {
   s->rows_have_order = true;
 }
 
-void assemble_rows(gs2g_session* s) {
-  if (!s->rows_dirty) return;
-  const int n = s->n_bus;
-  int nr = 0;
-  if (s->n_ctg > 0 && s->n_inj > 0 && s->n_ctg != s->n_inj)
-    throw std::invalid_argument("topology rows (" + std::to_string(s->n_ctg) + ") and injection rows (" +
-                                std::to_string(s->n_inj) + ") differ in number");
-  nr = std::max(s->n_ctg, s->n_inj);
-  s->n_rows = nr;
-  s->rows_have_sbus = s->n_inj > 0;
-  s->rows_have_edits = s->n_ctg > 0;
-  s->rows_have_skip = false;
-  s->rows_have_mask = false;
-  if (nr == 0) {
+// Rows in two stages.  The first (row count, trip CSR on the device) is all
+// gs2g_get_device_rows needs, so a caller's network can run on the rows
+// while the host builds the second (every row's Ybus edits, islanding
+// verdict, masks and the row order), which a run needs.
+void assemble_rows(gs2g_session* s, bool full = true) {
+  if (s->rows_dirty) {
+    if (s->n_ctg > 0 && s->n_inj > 0 && s->n_ctg != s->n_inj)
+      throw std::invalid_argument("topology rows (" + std::to_string(s->n_ctg) + ") and injection rows (" +
+                                  std::to_string(s->n_inj) + ") differ in number");
+    const int nr = std::max(s->n_ctg, s->n_inj);
+    s->n_rows = nr;
+    s->rows_have_sbus = s->n_inj > 0;
+    s->rows_have_edits = s->n_ctg > 0;
+    s->rows_have_skip = false;
+    s->rows_have_mask = false;
+    s->rows_have_order = false;
+    if (nr > 0 && s->rows_have_edits) {
+      s->d_trip_ptr.ensure((nr + 1) * sizeof(int));
+      s->d_trip_ids.ensure(std::max<size_t>(s->ctg_ids.size(), 1) * sizeof(int));
+      ck(cudaMemcpy(s->d_trip_ptr.p, s->ctg_ptr.data(), (nr + 1) * sizeof(int), cudaMemcpyHostToDevice),
+         "upload trips");
+      if (!s->ctg_ids.empty())
+        ck(cudaMemcpy(s->d_trip_ids.p, s->ctg_ids.data(), s->ctg_ids.size() * sizeof(int), cudaMemcpyHostToDevice),
+           "upload trips");
+    }
     s->rows_dirty = false;
+    s->edits_dirty = true;
+  }
+  if (!full || !s->edits_dirty) return;
+  const int n = s->n_bus;
+  const int nr = s->n_rows;
+  if (nr == 0) {
+    s->edits_dirty = false;
     return;
   }
   if (s->rows_have_edits) {
-    s->d_trip_ptr.ensure((nr + 1) * sizeof(int));
-    s->d_trip_ids.ensure(std::max<size_t>(s->ctg_ids.size(), 1) * sizeof(int));
-    ck(cudaMemcpy(s->d_trip_ptr.p, s->ctg_ptr.data(), (nr + 1) * sizeof(int), cudaMemcpyHostToDevice), "upload trips");
-    if (!s->ctg_ids.empty())
-      ck(cudaMemcpy(s->d_trip_ids.p, s->ctg_ids.data(), s->ctg_ids.size() * sizeof(int), cudaMemcpyHostToDevice),
-         "upload trips");
     std::vector<int> eptr(nr + 1, 0), ek;
     std::vector<double> ev;
     std::vector<uint8_t> skip(nr, 0);
@@ -558,7 +571,7 @@ void assemble_rows(gs2g_session* s) {
     }
   }
   order_rows(s, nr);
-  s->rows_dirty = false;
+  s->edits_dirty = false;
 }
 
 struct OutBufs {
@@ -1948,7 +1961,7 @@ int gs2g_get_device_rows(gs2g_session* s, int* n_rows, const double** sbus_rows,
   GS2G_TRY
   if (!s) throw std::invalid_argument("NULL session");
   DeviceGuard g(s->device);
-  assemble_rows(s);
+  assemble_rows(s, false);
   if (n_rows) *n_rows = s->n_rows;
   if (sbus_rows) *sbus_rows = s->rows_have_sbus ? s->d_sbus_rows.as<double>() : nullptr;
   if (trip_ptr) *trip_ptr = s->rows_have_edits ? s->d_trip_ptr.as<int>() : nullptr;

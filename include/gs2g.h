@@ -334,7 +334,9 @@ int gs2g_get_device_results(const gs2g_session* s, double** v, double** residual
  * the base injections), trip_ptr [n_rows + 1] / trip_ids [n_trip_ids] CSR of
  * tripped branches (NULL: no trips).  Valid until the rows change.  A
  * device-resident caller (e.g. a learned start) reads them instead of
- * shipping the rows again. */
+ * shipping the rows again.  The rows' Ybus edits, islanding verdicts and
+ * order are built by the next run, so a caller's network on these rows and
+ * that host work overlap. */
 int gs2g_get_device_rows(gs2g_session* s, int* n_rows, const double** sbus_rows, const int** trip_ptr,
                          const int** trip_ids, int64_t* n_trip_ids);
 int gs2g_get_timings(const gs2g_session* s, gs2g_timings* out);
