@@ -25,6 +25,7 @@ inside the same launch.
 
 from __future__ import annotations
 
+import itertools
 import time
 
 import numpy as np
@@ -51,11 +52,36 @@ def _rows_csr(branch_ids_per_row):
     elif len(branch_ids_per_row) and all(len(r) == 1 for r in branch_ids_per_row):
         flat = np.fromiter((int(r[0]) for r in branch_ids_per_row), dtype=np.int32, count=len(branch_ids_per_row))
     else:
-        rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_row]
-        ptr, ids = _ids_csr(rows)
-        return rows, ptr, ids
+        try:
+            ptr, ids = _dedup_csr(branch_ids_per_row)
+        except (TypeError, ValueError, OverflowError):
+            rows = [list(dict.fromkeys(int(v) for v in ids)) for ids in branch_ids_per_row]
+            ptr, ids = _ids_csr(rows)
+            return rows, ptr, ids
+        return None, ptr, ids
     ptr = np.arange(flat.size + 1, dtype=np.int32)
     return None, ptr, flat
+
+
+def _dedup_csr(branch_ids_per_row):
+    """(ptr, ids) int32 of lists of integer ids, each row's repeated ids
+    dropped (first occurrence kept, order kept), without a Python loop per
+    id: the rows are flattened, (row, id) keys that repeat are removed by
+    their first index."""
+    n = len(branch_ids_per_row)
+    lens = np.fromiter(map(len, branch_ids_per_row), dtype=np.int64, count=n)
+    flat = np.fromiter(itertools.chain.from_iterable(branch_ids_per_row), dtype=np.int64, count=int(lens.sum()))
+    if flat.size and (flat.min() < np.iinfo(np.int32).min or flat.max() > np.iinfo(np.int32).max):
+        raise OverflowError("branch id out of the int32 range")
+    rid = np.repeat(np.arange(n, dtype=np.int64), lens)
+    if flat.size:
+        span = int(flat.max()) - int(flat.min()) + 1
+        _, first = np.unique(rid * span + (flat - flat.min()), return_index=True)
+        keep = np.sort(first)
+        flat, rid = flat[keep], rid[keep]
+    ptr = np.zeros(n + 1, dtype=np.int32)
+    ptr[1:] = np.cumsum(np.bincount(rid, minlength=n))
+    return ptr, flat.astype(np.int32)
 
 
 def _ids_csr(rows):

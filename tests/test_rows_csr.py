@@ -1,6 +1,6 @@
 """Host-side row definitions: branch-id lists to the trip CSR the session
-takes (duplicates dropped, first occurrence kept; single-branch rows take a
-vectorised path that keeps the CSR as the only copy)."""
+takes (duplicates dropped, first occurrence kept), on vectorised paths that
+keep the CSR as the only copy."""
 
 import numpy as np
 
@@ -18,5 +18,22 @@ def test_single_branch_rows_keep_only_the_csr():
 
 def test_other_rows_drop_duplicates_in_order():
     rows, ptr, ids = _rows_csr([[4, 2, 4], [], [1]])
-    assert rows == [[4, 2], [], [1]]
+    assert rows is None
     assert ptr.tolist() == [0, 2, 2, 3] and ids.tolist() == [4, 2, 1]
+
+
+def test_vectorised_rows_equal_the_per_row_reference():
+    """The flattened conversion of general rows (any count per row,
+    repeats, negative ids left for the library to reject) equals the
+    per-row one: first occurrences in row order."""
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        rows = [[int(x) for x in rng.integers(-3, 20, int(rng.integers(0, 6)))]
+                for _ in range(int(rng.integers(2, 40)))]
+        rows[0] = rows[0] + [7, 7]  # not every row of one id
+        ref = [list(dict.fromkeys(r)) for r in rows]
+        _, ptr, ids = _rows_csr(rows)
+        assert ptr.tolist() == np.cumsum([0] + [len(r) for r in ref]).tolist()
+        assert ids.tolist() == [v for r in ref for v in r]
+    _, ptr, ids = _rows_csr(np.array([[1, 2], [2, 2]]))
+    assert ptr.tolist() == [0, 2, 3] and ids.tolist() == [1, 2, 2]
